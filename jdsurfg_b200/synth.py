@@ -1,0 +1,147 @@
+"""Seeded synthetic layered-earth models for the benchmark configurations.
+
+There is no public dataset for this path: every configuration is generated
+here from a fixed seed, with the shapes, depth grids, velocity ranges and
+period sets of the benchmark configurations.  The same generator feeds the
+GPU runs and the CPU oracle.
+
+Layout of a case (all numpy, matching the reference's Eigen column-major
+containers): ``vs`` is (nz, ncol) float32 C-order, i.e. an Eigen
+``fmat3(nx, ny, nz)`` in memory with column index n = ix + nx*iy; ``vp``/``rho``
+are either None (vp/rho from the Brocher relations, as
+SurfTime::get_1d_kernel does, SurfaceWave.cpp:476-480) or explicit arrays of
+the same shape; each period table ``tables[w]`` (w = Rc, Rg, Lc, Lg) is an
+(ntmax, nmode) float64 array with -1 padding like SurfTime::tRc, or None.
+"""
+import numpy as np
+
+WAVES = ("Rc", "Rg", "Lc", "Lg")
+
+
+def brocher(vs):
+    """Brocher (2005) vp(vs), rho(vp) in float32 (empirical.cpp:9-18)."""
+    v = vs.astype(np.float64)
+    vp = (0.9409 + 2.0947 * v - 0.8206 * v ** 2 + 0.2683 * v ** 3 - 0.0251 * v ** 4).astype(np.float32)
+    p = vp.astype(np.float64)
+    rho = (1.6612 * p - 0.4721 * p ** 2 + 0.0671 * p ** 3 - 0.0043 * p ** 4 + 0.000106 * p ** 5).astype(np.float32)
+    return vp, rho
+
+
+def _corr_field(rng, nx, ny, nz, lh, lv):
+    from scipy.ndimage import gaussian_filter
+    w = rng.standard_normal((nz, ny, nx))
+    f = gaussian_filter(w, sigma=(lv, lh, lh), mode="wrap")
+    f /= max(np.abs(f).max(), 1e-30)
+    return f
+
+
+def _table(periods, nmode):
+    periods = np.asarray(periods, np.float64)
+    return np.ascontiguousarray(np.repeat(periods[:, None], nmode, axis=1))
+
+
+def make_case(nx, ny, depth, vs_top, vs_bot, amp, periods, waves, nmode, seed, lvz_frac=0.0, water_frac=0.0,
+              explicit_vp=None, lh=4.0, lv=3.0):
+    rng = np.random.default_rng(seed)
+    depth = np.asarray(depth, np.float32)
+    nz = len(depth)
+    frac = (depth - depth[0]) / (depth[-1] - depth[0])
+    base = vs_top + (vs_bot - vs_top) * frac
+    field = _corr_field(rng, nx, ny, nz, lh, lv)
+    vs = (base[:, None, None] * (1.0 + amp * field)).astype(np.float32)
+    ncol = nx * ny
+    vs = vs.reshape(nz, ncol)
+    if lvz_frac > 0:
+        cols = rng.random(ncol) < lvz_frac
+        zmask = (depth >= 15.0) & (depth <= 25.0)
+        vs[np.ix_(zmask, cols)] *= np.float32(0.9)
+    vp = rho = None
+    if explicit_vp is not None or water_frac > 0:
+        if explicit_vp is not None:
+            vp = (np.float32(explicit_vp) * vs).astype(np.float32)
+            _, rho = brocher(vs)
+            rho = brocher_rho(vp)
+        else:
+            vp, rho = brocher(vs)
+    if water_frac > 0:
+        wcols = np.nonzero(rng.random(ncol) < water_frac)[0]
+        nw = rng.integers(1, 4, size=len(wcols))
+        for c, k in zip(wcols, nw):
+            vs[:k, c] = 0.0
+            vp[:k, c] = 1.5
+            rho[:k, c] = 1.03
+    tables = [None] * 4
+    for w in waves:
+        tables[WAVES.index(w)] = _table(periods, nmode)
+    return dict(nx=nx, ny=ny, nz=nz, depth=depth, vs=np.ascontiguousarray(vs),
+                vp=None if vp is None else np.ascontiguousarray(vp),
+                rho=None if rho is None else np.ascontiguousarray(rho), tables=tables)
+
+
+def brocher_rho(vp):
+    p = vp.astype(np.float64)
+    return (1.6612 * p - 0.4721 * p ** 2 + 0.0671 * p ** 3 - 0.0043 * p ** 4 + 0.000106 * p ** 5).astype(np.float32)
+
+
+def depth_grid(nz_fine, dz_fine, nz_total, dz_coarse):
+    fine = np.arange(nz_fine) * dz_fine
+    coarse = fine[-1] + dz_coarse * np.arange(1, nz_total - nz_fine + 1)
+    return np.concatenate([fine, coarse]).astype(np.float32)
+
+
+def make_config(name, seed=2024, nx=None, ny=None):
+    """Named configurations.
+
+    tiny  : 4x3 columns, nz=12 (2 km), Rc/Rg/Lc/Lg mode 0, 6 periods -- unit tests
+    small : 16x16, nz=20 nodes every 2 km (0..38 km), vs 2.8->4.6 +-5 %
+            (correlation 4 columns / 3 nodes), vp = 1.732 vs, rho = Brocher(vp),
+            25 log-spaced periods 2-40 s, Rayleigh mode 0 phase + group
+    production : 128x128, nz=48 (1 km to 20 km, then 2.5 km), vs 2.5->4.7
+            +-8 %, LVZ -10 % at 15-25 km in 20 % of columns, 1-3 fluid nodes
+            (vp 1.5, vs 0, rho 1.03) in 10 % of columns, 40 log-spaced
+            periods 1-60 s, Rayleigh and Love, modes 0-1, phase and group
+    large : 256x256, nz=64 (1 km to 20 km, then 2.5 km), vs 2.5->4.7 +-8 %,
+            LVZ in 20 % of columns, 60 log-spaced periods 1-80 s, Rayleigh and
+            Love mode 0 phase
+    """
+    if name == "tiny":
+        depth = np.arange(12, dtype=np.float32) * 2.0
+        return make_case(nx or 4, ny or 3, depth, 2.6, 4.4, 0.05, np.geomspace(3.0, 30.0, 6), WAVES, 1, seed)
+    if name == "small":
+        depth = np.arange(20, dtype=np.float32) * 2.0
+        return make_case(nx or 16, ny or 16, depth, 2.8, 4.6, 0.05, np.geomspace(2.0, 40.0, 25), ("Rc", "Rg"), 1,
+                         seed, explicit_vp=1.732)
+    if name == "production":
+        depth = depth_grid(21, 1.0, 48, 2.5)
+        return make_case(nx or 128, ny or 128, depth, 2.5, 4.7, 0.08, np.geomspace(1.0, 60.0, 40), WAVES, 2, seed,
+                         lvz_frac=0.2, water_frac=0.1)
+    if name == "large":
+        depth = depth_grid(21, 1.0, 64, 2.5)
+        return make_case(nx or 256, ny or 256, depth, 2.5, 4.7, 0.08, np.geomspace(1.0, 80.0, 60), ("Rc", "Lc"), 1,
+                         seed, lvz_frac=0.2)
+    raise ValueError(name)
+
+
+def kmax_of(tables):
+    k = 0
+    for t in tables:
+        if t is None:
+            continue
+        for m in range(t.shape[1]):
+            col = t[:, m]
+            n = 0
+            while n < len(col) and col[n] != -1:
+                n += 1
+            k += n
+    return k
+
+
+def subset_columns(case, cols):
+    """A case restricted to the given column indices (nx = len(cols), ny = 1)."""
+    cols = np.asarray(cols)
+    out = dict(case)
+    out["nx"], out["ny"] = len(cols), 1
+    out["vs"] = np.ascontiguousarray(case["vs"][:, cols])
+    out["vp"] = None if case["vp"] is None else np.ascontiguousarray(case["vp"][:, cols])
+    out["rho"] = None if case["rho"] is None else np.ascontiguousarray(case["rho"][:, cols])
+    return out

@@ -1,0 +1,205 @@
+"""ctypes access to the CPU oracle (oracle/libswd_oracle.so).
+
+Test infrastructure only: tests use it as the checker; bench.py uses it for
+the timed CPU baseline.  Nothing in the product path imports this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+_LIB = None
+_REF = None
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(ORACLE_DIR, "libswd_oracle.so")
+        if not os.path.exists(so):
+            build()
+        _LIB = C.CDLL(so)
+        _LIB.swdo_dltar.restype = C.c_double
+        _LIB.swdo_frechet_rows.restype = C.c_long
+    return _LIB
+
+
+def ref_cxx():
+    """The reference's own surfdisp.cpp/empirical.cpp (oracle/_ref), or None."""
+    global _REF
+    if _REF is None:
+        so = os.path.join(ORACLE_DIR, "_ref", "libswd_refcxx.so")
+        if not os.path.exists(so):
+            return None
+        _REF = C.CDLL(so)
+    return _REF
+
+
+def load_swd_model():
+    d = np.loadtxt(os.path.join(ROOT, "tests", "golden", "swd_model.txt"), skiprows=1).astype(np.float32)
+    return [np.ascontiguousarray(d[:, i]) for i in range(4)]  # z, vs, vp, rho
+
+
+def f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def surfdisp96(thk, vp, vs, rho, iflsph, iwave, mode, igr, t, refine=0, rtol=1e-10, sngl=1):
+    thk, vp, vs, rho = f32(thk), f32(vp), f32(vs), f32(rho)
+    t = np.ascontiguousarray(t, np.float64)
+    cg = np.zeros(len(t))
+    ierr, nev, itl = C.c_int(0), C.c_long(0), C.c_int(0)
+    lib().swdo_surfdisp96_ex(_ptr(thk), _ptr(vp), _ptr(vs), _ptr(rho), len(thk), iflsph, iwave, mode, igr, len(t),
+                             _ptr(t), _ptr(cg), C.byref(ierr), refine, C.c_double(rtol), sngl, C.byref(nev),
+                             C.byref(itl))
+    return cg, ierr.value, nev.value
+
+
+def surfdisp(thk, vp, vs, rho, t, wtype, mode=0, sphere=1, keep_flat=1, refine=0, rtol=1e-10, sngl=1):
+    thk, vp, vs, rho = f32(thk), f32(vp), f32(vs), f32(rho)
+    t = np.ascontiguousarray(t, np.float64)
+    cg = np.zeros(len(t))
+    st = np.zeros(len(t), np.int32)
+    lib().swdo_surfdisp(_ptr(thk), _ptr(vp), _ptr(vs), _ptr(rho), len(thk), _ptr(t), _ptr(cg), len(t), wtype, mode,
+                        sphere, keep_flat, refine, C.c_double(rtol), sngl, _ptr(st))
+    return cg, st
+
+
+def dltar(thk, vp, vs, rho, iflsph, iwave, t, c):
+    thk, vp, vs, rho = f32(thk), f32(vp), f32(vs), f32(rho)
+    return lib().swdo_dltar(_ptr(thk), _ptr(vp), _ptr(vs), _ptr(rho), len(thk), iflsph, iwave, C.c_double(t),
+                            C.c_double(c))
+
+
+def sregn96(thk, vp, vs, rho, t, cp, iflsph=1):
+    thk, vp, vs, rho = f32(thk), f32(vp), f32(vs), f32(rho)
+    n = len(thk)
+    b = [np.zeros(n) for _ in range(8)]
+    tt, cpv, cg = C.c_double(t), C.c_double(cp), C.c_double(0)
+    lib().sregn96_(_ptr(thk), _ptr(vp), _ptr(vs), _ptr(rho), n, C.byref(tt), C.byref(cpv), C.byref(cg),
+                   *[_ptr(x) for x in b], iflsph)
+    keys = ["ur", "uz", "tr", "tz", "dcda", "dcdb", "dcdh", "dcdr"]
+    out = dict(zip(keys, b))
+    out["c"] = cpv.value
+    out["u"] = cg.value
+    return out
+
+
+def slegn96(thk, vs, rho, t, cp, iflsph=1):
+    thk, vs, rho = f32(thk), f32(vs), f32(rho)
+    n = len(thk)
+    b = [np.zeros(n) for _ in range(5)]
+    tt, cpv, cg = C.c_double(t), C.c_double(cp), C.c_double(0)
+    lib().slegn96_(_ptr(thk), _ptr(vs), _ptr(rho), n, C.byref(tt), C.byref(cpv), C.byref(cg),
+                   *[_ptr(x) for x in b], iflsph)
+    keys = ["uu", "tt", "dcdb", "dcdh", "dcdr"]
+    out = dict(zip(keys, b))
+    out["c"] = cpv.value
+    out["u"] = cg.value
+    return out
+
+
+def grid2layer(z, vp, vs, rho, sublayers=3):
+    nz = len(z)
+    L = nz + (nz - 1) * sublayers
+    th, a, b, r = [np.zeros(L, np.float32) for _ in range(4)]
+    L = lib().swdo_grid2layer(_ptr(f32(z)), _ptr(f32(vp)), _ptr(f32(vs)), _ptr(f32(rho)), nz, sublayers, _ptr(th),
+                              _ptr(a), _ptr(b), _ptr(r))
+    return th[:L], a[:L], b[:L], r[:L]
+
+
+def _table_args(tables):
+    args, keep = [], []
+    for w in range(4):
+        t = tables[w]
+        if t is None:
+            args += [None, 0, 0]
+        else:
+            t = np.asfortranarray(np.asarray(t, np.float64))
+            keep.append(t)
+            args += [_ptr(t), t.shape[0], t.shape[1]]
+    return args, keep
+
+
+def _kmax(tables):
+    from jdsurfg_b200.synth import kmax_of
+    return kmax_of([None if t is None else np.asarray(t) for t in tables])
+
+
+def kernel1d(vs, vp, rho, dep, tables, refine=1, rtol=1e-12, sngl=0, sphere=1):
+    """One column through kernel1D; returns node kernels before the chain rule."""
+    nz = len(dep)
+    targs, keep = _table_args(tables)
+    kmax = _kmax(tables)
+    vc, vo = np.zeros(kmax), np.zeros(kmax)
+    kvs, kvp, kr = np.zeros(kmax * nz), np.zeros(kmax * nz), np.zeros(kmax * nz)
+    st = np.zeros(kmax, np.int32)
+    lib().swdo_kernel1d(_ptr(f32(vs)), _ptr(f32(vp)), _ptr(f32(rho)), _ptr(f32(dep)), nz, *targs, _ptr(vc), _ptr(vo),
+                        _ptr(kvs), _ptr(kvp), _ptr(kr), _ptr(st), refine, C.c_double(rtol), sngl, sphere)
+    sh = (kmax, nz)
+    return dict(vc=vc, vout=vo, kvs=kvs.reshape(sh), kvp=kvp.reshape(sh), krho=kr.reshape(sh), status=st)
+
+
+def get_1d_kernel(case, refine=1, rtol=1e-10, sngl=1, sphere=1, nthreads=0, cols=None):
+    from jdsurfg_b200.synth import subset_columns
+    if cols is not None:
+        case = subset_columns(case, cols)
+    vs = case["vs"]
+    nz, ncol = vs.shape
+    targs, keep = _table_args(case["tables"])
+    kmax = _kmax(case["tables"])
+    vc, vo = np.zeros((kmax, ncol)), np.zeros((kmax, ncol))
+    ker = np.zeros((kmax, nz, ncol))
+    st = np.zeros((kmax, ncol), np.int32)
+    nev = C.c_long(0)
+    lib().swdo_get_1d_kernel(ncol, nz, _ptr(vs), _ptr(case["vp"]), _ptr(case["rho"]), _ptr(case["depth"]), *targs,
+                             _ptr(vc), _ptr(vo), _ptr(ker), _ptr(st), refine, C.c_double(rtol), sngl, sphere,
+                             nthreads, C.byref(nev))
+    return dict(vc=vc, vout=vo, kernel=ker, status=st, nevals=nev.value)
+
+
+def get_2d_map(case, refine=1, rtol=1e-10, sngl=1, sphere=1, nthreads=0, cols=None):
+    from jdsurfg_b200.synth import subset_columns
+    if cols is not None:
+        case = subset_columns(case, cols)
+    vs = case["vs"]
+    nz, ncol = vs.shape
+    targs, keep = _table_args(case["tables"])
+    kmax = _kmax(case["tables"])
+    vc, vo = np.zeros((kmax, ncol)), np.zeros((kmax, ncol))
+    st = np.zeros((kmax, ncol), np.int32)
+    nev = C.c_long(0)
+    lib().swdo_get_2d_map(ncol, nz, _ptr(vs), _ptr(case["vp"]), _ptr(case["rho"]), _ptr(case["depth"]), *targs,
+                          _ptr(vc), _ptr(vo), _ptr(st), refine, C.c_double(rtol), sngl, sphere, nthreads,
+                          C.byref(nev))
+    return dict(vc=vc, vout=vo, status=st, nevals=nev.value)
+
+
+def frechet_rows(nx, ny, nz, kernel, row_slot, fdm):
+    """Frechet rows (SurfaceWave.cpp:590-676): list of (indices, values)."""
+    kmax = kernel.shape[0]
+    kernel = np.ascontiguousarray(kernel, np.float64)
+    row_slot = np.ascontiguousarray(row_slot, np.int32)
+    fdm = np.ascontiguousarray(fdm, np.float32)
+    nrows = len(row_slot)
+    n = (nx - 2) * (ny - 2) * (nz - 1)
+    nnz = np.zeros(nrows, np.int32)
+    idx = np.zeros(nrows * n, np.int32)
+    val = np.zeros(nrows * n, np.float32)
+    lib().swdo_frechet_rows(nx, ny, nz, kmax, _ptr(kernel), nrows, _ptr(row_slot), _ptr(fdm), _ptr(nnz), _ptr(idx),
+                            _ptr(val))
+    rows = []
+    for r in range(nrows):
+        rows.append((idx[r * n:r * n + nnz[r]].copy(), val[r * n:r * n + nnz[r]].copy()))
+    return rows
