@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Throughput of SurfTime::get_1d_kernel (dispersion + depth kernels for every
+column, period and mode of a 3-D model) on B200.
+
+A step is one get_1d_kernel call over the whole workload (the "production"
+grid: 128x128 columns, 48 nodes, 40 periods 1-60 s, Rayleigh and Love, modes
+0-1, phase and group, LVZ in 20 % and fluid layers in 10 % of the columns;
+seeded synthetic models).  value = column-period-mode slots per second with
+inputs resident in HBM; e2e = the same through the host-memory C-ABI call
+with pinned host buffers, host<->device copies inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl swdk|reference]
+
+Under torchrun each rank computes its own grid (different seed): weak
+scaling, no collective on the data path.  --impl reference times the CPU
+oracle (a line-by-line restatement of the reference's Fortran/C++ path; the
+reference's Fortran cannot be compiled here) on the host cores, on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "dispersion+kernel column-periods/s, learned vs plain GPU at |Δc|≤1e-6 km/s"
+UNIT = "column-period-modes/s"
+# Algorithmic FP64 flops per layer per secular evaluation (FMA = 2), hand count
+# of surfdisp96.f dltar4/var/dnka/normc (798-1095) and dltar1 (734-794);
+# divisions, square roots and exp/sin/cos are not counted.
+F_SEC_RAYLEIGH = 161
+F_SEC_LOVE = 19
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="swdk", choices=["swdk", "reference"])
+    ap.add_argument("--workload", default="production", choices=["production", "large", "small", "tiny"])
+    ap.add_argument("--ncols", type=int, default=0, help="use only the first N columns (profiling)")
+    ap.add_argument("--refine", default="tight", choices=["tight", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def workload(args, rank):
+    from jdsurfg_b200 import synth
+    case = synth.make_config(args.workload, seed=2024 + rank)
+    if args.ncols:
+        n = min(args.ncols, case["nx"] * case["ny"])
+        case = synth.subset_columns(case, np.arange(n))
+    return case
+
+
+def case_desc(args, case, kmax):
+    return {"workload": args.workload, "nx": case["nx"], "ny": case["ny"], "nz": case["nz"], "kmax": kmax,
+            "columns": case["nx"] * case["ny"], "refine": args.refine, "root_tolerance_km_s": 1e-6,
+            "l2": "flushed between steps (256 MiB write)", "sphere": True}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.p = None
+        if shutil.which("nvidia-smi"):
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 throughput of this GPU: cuBLAS float64 GEMM, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def build_oracle_native():
+    """The CPU baseline: the oracle built for this host (-march=native)."""
+    d = tempfile.mkdtemp(prefix="swdo_")
+    so = os.path.join(d, "libswd_oracle_native.so")
+    src = os.path.join(ROOT, "oracle", "swd_oracle.cpp")
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    try:
+        subprocess.run([cxx, "-O3", "-march=native", "-fopenmp", "-fPIC", "-std=c++17", "-ffp-contract=off", "-shared",
+                        "-o", so, src], check=True, capture_output=True)
+        return so, "g++ -O3 -march=native -fopenmp"
+    except Exception:
+        return os.path.join(ROOT, "oracle", "libswd_oracle.so"), "g++ -O3 -fopenmp (portable build)"
+
+
+def cpu_baseline(case, args, target_s):
+    """The oracle port on all host threads over a bounded column sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ctypes as C
+    import oracle_lib as O
+    so, how = build_oracle_native()
+    O._LIB = C.CDLL(so)
+    O._LIB.swdo_dltar.restype = C.c_double
+    O._LIB.swdo_frechet_rows.restype = C.c_long
+    cores = os.cpu_count() or 1
+    ncol = case["nx"] * case["ny"]
+    refine = 1 if args.refine == "tight" else 0
+    n = min(ncol, max(cores, 8))
+    t0 = time.perf_counter()
+    r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n))
+    dt = time.perf_counter() - t0
+    kmax = r["vc"].shape[0]
+    per_col = dt / n
+    n2 = int(min(ncol, max(n, target_s / max(per_col, 1e-9))))
+    n2 = max(cores, (n2 // cores) * cores) if n2 >= cores else n2
+    n2 = min(n2, ncol)
+    t0 = time.perf_counter()
+    r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n2))
+    dt = time.perf_counter() - t0
+    return {"value": n2 * kmax / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n2} of {ncol} columns x {kmax} slots ({dt:.1f} s, {how}, OpenMP over columns)"}, n2, dt
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    case = workload(args, 0)
+    from jdsurfg_b200 import synth
+    kmax = synth.kmax_of(case["tables"])
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    for _ in range(max(0, args.warmup)):
+        pass
+    per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    cb, n2, _ = cpu_baseline(case, args, per_step_s)
+    import oracle_lib as O
+    refine = 1 if args.refine == "tight" else 0
+    cols = np.arange(n2)
+    for _ in range(args.warmup):
+        O.get_1d_kernel(case, refine=refine, nthreads=cb["cores"], cols=cols[:max(1, n2 // 4)])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.get_1d_kernel(case, refine=refine, nthreads=cb["cores"], cols=cols)
+    dt = time.perf_counter() - t0
+    value = args.steps * n2 * kmax / dt
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, jdsurfg_b200/synth.py)", "config": case_desc(args, case, kmax),
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    from jdsurfg_b200 import Engine
+    case = workload(args, rank)
+    eng = Engine(device=local, refine=args.refine)
+    eng.setup(case)
+    nx, ny, nz = case["nx"], case["ny"], case["nz"]
+    ncol, kmax = nx * ny, eng.kmax
+    units = ncol * kmax
+    vs = torch.from_numpy(case["vs"]).to(dev)
+    vp = None if case["vp"] is None else torch.from_numpy(case["vp"]).to(dev)
+    rho = None if case["rho"] is None else torch.from_numpy(case["rho"]).to(dev)
+    vc = torch.empty((kmax, ncol), dtype=torch.float64, device=dev)
+    vout = torch.empty_like(vc)
+    ker = torch.empty((kmax, nz, ncol), dtype=torch.float64, device=dev)
+    st = torch.empty((kmax, ncol), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        flush.fill_(1)
+        eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    roots_ms, evals, lr, ll = 0.0, 0, 0, 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        s = eng.stats()  # synchronises on the engine's work; collects per-stage events
+        roots_ms += s["ms_roots"]
+        evals += s["secular_evals"]
+        lr += s["layer_evals_rayleigh"]
+        ll += s["layer_evals_love"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * units / (ms_per_step * 1e-3)
+    stats = eng.stats()
+    status = np.bincount(st.cpu().numpy().ravel(), minlength=5).tolist()
+
+    # e2e: host-memory C-ABI call, pinned buffers, copies in the timed region
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+        h_vs = pin(case["vs"].shape, torch.float32)
+        h_vs[...] = case["vs"]
+        h_vp = h_rho = None
+        if case["vp"] is not None:
+            h_vp = pin(case["vp"].shape, torch.float32)
+            h_vp[...] = case["vp"]
+            h_rho = pin(case["rho"].shape, torch.float32)
+            h_rho[...] = case["rho"]
+        h_vc, h_vout = pin((kmax, ncol), torch.float64), pin((kmax, ncol), torch.float64)
+        h_ker = pin((kmax, nz, ncol), torch.float64)
+        h_st = pin((kmax, ncol), torch.int32)
+        import ctypes as C
+        from jdsurfg_b200.engine import lib, _p
+
+        def host_step():
+            rc = lib().swdk_get_1d_kernel(eng._h, nx, ny, nz, _p(h_vs), _p(h_vp), _p(h_rho), _p(h_vc), _p(h_vout),
+                                          _p(h_ker), _p(h_st))
+            assert rc == 0, rc
+
+        host_step()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            host_step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([dt], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            dt = float(t.item())
+        h2d = h_vs.nbytes + (0 if h_vp is None else h_vp.nbytes + h_rho.nbytes)
+        d2h = h_vc.nbytes + h_vout.nbytes + h_ker.nbytes + h_st.nbytes
+        e2e = {"value": world * units * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+
+    # roofline of the dominant kernel (k_roots: secular functions, FP64 pipe)
+    peak = fp64_peak_tflops(torch, dev)
+    flops = lr * F_SEC_RAYLEIGH + ll * F_SEC_LOVE
+    achieved = flops / (roots_ms * 1e-3) / 1e12 if roots_ms > 0 else 0.0
+    roofline = {"kernel": "k_roots", "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": "measured in this run: cuBLAS float64 GEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
+                "flops_per_layer_eval": {"rayleigh": F_SEC_RAYLEIGH, "love": F_SEC_LOVE},
+                "share_of_step": roots_ms / ms if ms else None}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb, _, _ = cpu_baseline(case, args, args.cpu_seconds)
+        except Exception as ex:  # the baseline is reported, never required
+            cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator, jdsurfg_b200/synth.py); no public dataset exists for this path",
+                "config": case_desc(args, case, kmax), "clocks": clk, "e2e": e2e,
+                "gpu_launches": 3 * args.steps, "roofline": roofline, "cpu_baseline": cb,
+                "detail": {"secular_evals_per_step": evals / args.steps,
+                           "evals_per_slot": evals / args.steps / units,
+                           "ms_roots": roots_ms / args.steps, "ms_prep": stats["ms_prep"],
+                           "ms_eigen": stats["ms_eigen"], "status_counts": status}}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

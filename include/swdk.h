@@ -1,0 +1,161 @@
+/*
+ * swdk.h -- C-ABI of the B200 surface-wave dispersion and depth-kernel
+ * engine (libswdk.so).  Plain pointers and sizes only.
+ *
+ * It replaces, for one call over a whole 3-D model, the per-column OpenMP
+ * loops of JDSurfG's SurfTime class and the Fortran calls they make:
+ *
+ *   swdk_get_1d_kernel   <- SurfTime::get_1d_kernel
+ *                           (src/SWD/SurfaceWave.hpp:103,
+ *                            src/SWD/SurfaceWave.cpp:458-502), i.e. kernel1D
+ *                           (SurfaceWave.cpp:266-412) per column with
+ *                           surfdisp96_/sregn96_/sregnpu_/slegn96_/slegnpu_
+ *                           (src/SWD/swd.hpp:5-96)
+ *   swdk_get_2d_map      <- SurfTime::get_2d_map
+ *                           (SurfaceWave.hpp:102, SurfaceWave.cpp:420-450),
+ *                           i.e. disp1D (SurfaceWave.cpp:177-255)
+ *   swdk_set_periods     <- the SurfTime members tRc/tRg/tLc/tLg
+ *                           (SurfaceWave.hpp:86-88), (ntmax, nmode)
+ *                           column-major with -1 padding as io.cpp fills them
+ *   swdk_set_depth       <- SurfTime::set_model's depth (SurfaceWave.cpp:678-686)
+ *   swdk_surfdisp96_batch<- surfdisp96_ (swd.hpp:78-81) over many layered
+ *                           models with one period list
+ *   swdk_frechet_rows    <- the row assembly of SurfTime::frechet_matrix
+ *                           (SurfaceWave.cpp:630-660)
+ *
+ * Array layouts are Eigen's column-major ones used by the reference:
+ *   vs, vp, rho      : (nx, ny, nz)       float,  element (ix,iy,iz) at ix + nx*(iy + ny*iz)
+ *   vc, vout, status : (nx*ny, kmax)      double/int32, column n = ix + nx*iy
+ *   kernel           : (nx*ny, nz, kmax)  double
+ * kmax = total number of periods over Rc, Rg, Lc, Lg and their modes, in
+ * the reference's slot order (SurfaceWave.cpp:14-48).
+ *
+ * Return value: 0 on success, a negative SWDK_E* code otherwise.  Per-slot
+ * outcomes are in `status` (SWDK_ST_*).  A context is used from one host
+ * thread at a time; calls on different contexts are independent.
+ */
+#ifndef SWDK_H_
+#define SWDK_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define SWDK_OK 0
+#define SWDK_E_ARG (-1)       /* bad argument (NULL, size out of range)      */
+#define SWDK_E_CUDA (-2)      /* a CUDA runtime call failed                  */
+#define SWDK_E_NOPERIODS (-3) /* swdk_set_periods not called / no periods    */
+#define SWDK_E_NODEPTH (-4)   /* swdk_set_depth not called or nz mismatch    */
+#define SWDK_E_LIMIT (-5)     /* model beyond the compiled limits            */
+
+/* per-slot status */
+#define SWDK_ST_OK 0
+#define SWDK_ST_NO_ROOT 1    /* no root after the single-period retry; the
+                                reference calls exit(1) (surfdisp.cpp:100-108) */
+#define SWDK_ST_RETRIED 2    /* found by that retry (surfdisp.cpp:94-99)     */
+#define SWDK_ST_NAN_INPUT 3  /* column has non-finite or invalid values     */
+#define SWDK_ST_ITER_LIMIT 4 /* refinement hit its iteration cap            */
+
+/* root refinement */
+#define SWDK_REFINE_REFERENCE 0 /* surfdisp96 nevill: |c1-c2| <= 1e-6*c1     */
+#define SWDK_REFINE_TIGHT 1     /* Brent on the same bracket, width <= rtol*c */
+
+/* compiled limits */
+#define SWDK_MAX_NZ 80          /* grid nodes per column                   */
+#define SWDK_MAX_LAYERS 320     /* sublayers per column (4*nz-3)           */
+#define SWDK_MAX_PERIODS 128    /* periods per (wave type, mode) list      */
+
+typedef struct swdk_config {
+  int device;      /* CUDA device ordinal (default 0)                         */
+  int refine;      /* SWDK_REFINE_* (default SWDK_REFINE_TIGHT)                */
+  double rtol;     /* bracket width for SWDK_REFINE_TIGHT (default 1e-10)     */
+  int sngl;        /* 1: roots rounded to REAL*4 as surfdisp96 does (default) */
+  int sphere;      /* 1: spherical earth as SurfTime (default); 0: flat       */
+  int block_roots; /* threads per block of the root kernel, 0 = default       */
+} swdk_config;
+
+typedef struct swdk_stats {
+  int64_t secular_evals; /* secular-function evaluations of the last call    */
+  int64_t layer_evals_rayleigh; /* sum over Rayleigh evaluations of the layers
+                                   propagated (dltar4, surfdisp96.f:798-898) */
+  int64_t layer_evals_love;     /* same for Love (dltar1, surfdisp96.f:734-794) */
+  int32_t nchains;       /* distinct (wave, period list) root chains per column */
+  int32_t nslots;        /* kmax of the last call                            */
+  float ms_prep, ms_roots, ms_eigen; /* device time of the last call's stages */
+} swdk_stats;
+
+typedef struct swdk_ctx swdk_ctx;
+
+/* Fills *cfg with the defaults listed above. */
+int swdk_config_default(swdk_config* cfg);
+
+/* Creates a context on cfg->device (cfg may be NULL for defaults). */
+int swdk_create(swdk_ctx** ctx, const swdk_config* cfg);
+void swdk_destroy(swdk_ctx* ctx);
+
+/* Period tables of SurfTime (tRc, tRg, tLc, tLg); a table may be NULL with
+ * ntmax = nmode = 0.  Each is (ntmax, nmode) column-major, -1 padded. */
+int swdk_set_periods(swdk_ctx* ctx, const double* tRc, int ntRc, int nmRc, const double* tRg, int ntRg, int nmRg,
+                     const double* tLc, int ntLc, int nmLc, const double* tLg, int ntLg, int nmLg);
+
+/* Node depths (km) of the model grid, as SurfTime::depth. */
+int swdk_set_depth(swdk_ctx* ctx, const float* depth, int nz);
+
+/* kmax of the current period tables (number of slots per column). */
+int swdk_kmax(const swdk_ctx* ctx);
+
+/* SurfTime::get_1d_kernel over an (nx, ny, nz) model in HOST memory.
+ * vp and rho may be NULL: then they follow from vs by the Brocher relations
+ * like the reference; when given, they are used as node values (fluid
+ * nodes: vs = 0) and the chain rule still uses the Brocher derivatives as
+ * SurfaceWave.cpp:491-500 does.  status may be NULL. */
+int swdk_get_1d_kernel(swdk_ctx* ctx, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
+                       double* vc, double* vout, double* kernel, int32_t* status);
+
+/* SurfTime::get_2d_map: dispersion only (phase; group from the energy
+ * integrals for Rg/Lg as groupvel_r/_l do). */
+int swdk_get_2d_map(swdk_ctx* ctx, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
+                    double* vc, double* vout, int32_t* status);
+
+/* The same two calls on DEVICE pointers (current device of the context),
+ * enqueued on `stream` (a cudaStream_t, NULL = the context's stream); they
+ * return once the work is enqueued. */
+int swdk_get_1d_kernel_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                              const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
+                              void* stream);
+int swdk_get_2d_map_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                           const float* d_rho, double* d_vc, double* d_vout, int32_t* d_status, void* stream);
+
+/* surfdisp96_ over nmodel layered models of nlayer layers each (HOST
+ * memory).  thk/vp/vs/rho are (nlayer, nmodel) column-major (model m's
+ * layers contiguous), t has kmax periods, cg is (kmax, nmodel), ierr has
+ * nmodel entries.  iflsph/iwave/mode/igr have surfdisp96's meaning
+ * (iwave 1 Love 2 Rayleigh, mode 1 = fundamental, igr 0 phase). */
+int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* thk, const float* vp, const float* vs,
+                          const float* rho, int iflsph, int iwave, int mode, int igr, int kmax, const double* t,
+                          double* cg, int32_t* ierr);
+
+/* Frechet rows of SurfTime::frechet_matrix from a DEVICE kernel
+ * (nx*ny, nz, kmax) double: for each of nrows receivers r with period slot
+ * row_slot[r] and ray weights fdm[r] ((nx, ny) float column-major), row r
+ * is float(fdm(ix+1,iy+1) * kernel(ii, iz, slot)) over the interior cells
+ * j = iz*(nx-2)*(ny-2) + iy*(nx-2) + ix, iz < nz-1, nonzeros kept in
+ * ascending j.  Device outputs: nnz[nrows], and indices/values with row r
+ * at r*(nx-2)*(ny-2)*(nz-1) (capacity per row).  Enqueued on `stream`. */
+int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, const double* d_kernel, int nrows,
+                             const int32_t* d_row_slot, const float* d_fdm, int32_t* d_nnz, int32_t* d_indices,
+                             float* d_values, void* stream);
+
+/* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
+int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
+
+/* Human-readable text of the last error on this context. */
+const char* swdk_last_error(const swdk_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWDK_H_ */

@@ -1,0 +1,1087 @@
+// swdk.cu -- kernels and C-ABI of the B200 surface-wave engine (libswdk.so).
+//
+// Pipeline of one SurfTime::get_1d_kernel call (SurfaceWave.cpp:458-502):
+//   k_prep   : one thread per column: Brocher vp/rho (empirical.cpp:9-18),
+//              grid2LayerModel (SurfaceWave.cpp:113-155), surfdisp96's
+//              sphere() flattening (surfdisp96.f:499-571) and start value
+//              (surfdisp96.f:154-226); writes the REAL*4 layer model
+//              layer-major and bottom-aligned so a warp of columns reads each
+//              layer in one coalesced request.
+//   k_roots  : one thread per (column, root chain); a chain is one
+//              surfdisp96 call (wave, period list, modes 1..M) with the
+//              reference's retry (surfdisp.cpp:94-109); identical chains of
+//              different slot types are computed once.
+//   k_eigen  : one block per column, one thread per output slot: sregn96 /
+//              sregnpu / slegn96 / slegnpu passes, sphericity, _ParamConvert
+//              and the empirical chain rule (SurfaceWave.cpp:491-500).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "swdk.h"
+#include "swdk_core.cuh"
+#include "swdk_eigen.cuh"
+
+using namespace swdk;
+
+namespace {
+
+struct ColInfo {
+  double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
+  float betmx;  // largest flattened shear velocity
+  int L;        // sublayers incl. half-space
+  int llw;      // 2 if the top layer is fluid
+  int nw;       // leading fluid grid nodes
+  int valid;
+};
+
+struct ChainDesc {
+  int t_off;    // first period in the period array
+  int np;       // periods
+  int nmode;    // modes 1..nmode
+  int iwave;    // 1 Love, 2 Rayleigh
+  int igr;      // surfdisp96 igr
+  int out_off;  // root slot of (mode 1, period 0)
+};
+
+struct SlotDesc {
+  int wtype;        // 0 Rc, 1 Rg, 2 Lc, 3 Lg
+  int oslot;        // output slot (0..kmax-1)
+  int r0, r1, r2;   // root slots of T, T(1+0.005), T(1-0.005)
+  double t, t1, t2;
+};
+
+// ---------------------------------------------------------------------------
+// exact-order arithmetic for the model preparation (matches the CPU order)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// correctly rounded x^5 for x exactly representable in float (x^2 is exact)
+__device__ __forceinline__ double pow5_cr(double x) {
+  const double x2 = dmul(x, x);
+  const double hi = dmul(x2, x2);
+  const double lo = fma(x2, x2, -hi);
+  return fma(hi, x, dmul(lo, x));
+}
+
+// empirical_relation (empirical.cpp:9-18); std::pow(float,int) is evaluated
+// in double and, for float arguments, the exact-then-rounded products below
+// equal glibc's correctly rounded pow.
+__device__ void brocher(float vsz, float& vpz, float& rhoz) {
+  const double v = vsz, v2 = dmul(v, v), v3 = dmul(v2, v), v4 = dmul(v2, v2);
+  vpz = (float)dsub(dadd(dsub(dadd(0.9409, dmul(2.0947, v)), dmul(0.8206, v2)), dmul(0.2683, v3)),
+                    dmul(0.0251, v4));
+  const double p = vpz, p2 = dmul(p, p), p3 = dmul(p2, p), p4 = dmul(p2, p2), p5 = pow5_cr(p);
+  rhoz = (float)dadd(dsub(dadd(dsub(dmul(1.6612, p), dmul(0.4721, p2)), dmul(0.0671, p3)), dmul(0.0043, p4)),
+                     dmul(0.000106, p5));
+}
+
+// empirical_deriv (empirical.cpp:26-34)
+__device__ void brocher_deriv(float vp, float vs, float& drda, float& dadb) {
+  const double p = vp, p2 = dmul(p, p), p3 = dmul(p2, p), p4 = dmul(p2, p2);
+  drda = (float)dadd(dsub(dadd(dsub(1.6612, dmul(0.4721 * 2, p)), dmul(0.0671 * 3, p2)), dmul(0.0043 * 4, p3)),
+                     dmul(0.000106 * 5, p4));
+  const double s = vs, s2 = dmul(s, s), s3 = dmul(s2, s);
+  dadb = (float)dsub(dadd(dsub(2.0947, dmul(0.8206 * 2, s)), dmul(0.2683 * 3, s2)), dmul(0.0251 * 4, s3));
+}
+
+// gtsolh (surfdisp96.f:377-398), REAL*4
+__device__ float gtsolh(float a, float b) {
+  float c = fmul(0.95f, b);
+  for (int i = 0; i < 5; ++i) {
+    const float gamma = fdiv(b, a);
+    const float kappa = fdiv(c, b);
+    const float k2 = fmul(kappa, kappa);
+    const float gk = fmul(gamma, kappa);
+    const float gk2 = fmul(gk, gk);
+    const float fac1 = __fsqrt_rn(fsub(1.0f, gk2));
+    const float fac2 = __fsqrt_rn(fsub(1.0f, k2));
+    const float tk = fsub(2.0f, k2);
+    const float fr = fsub(fmul(tk, tk), fmul(fmul(4.0f, fac1), fac2));
+    float frp = fadd(fadd(-fmul(fmul(4.0f, fsub(2.0f, k2)), kappa),
+                          fdiv(fmul(fmul(fmul(fmul(4.0f, fac2), gamma), gamma), kappa), fac1)),
+                     fdiv(fmul(fmul(4.0f, fac1), kappa), fac2));
+    frp = fdiv(frp, b);
+    c = fsub(c, fdiv(fr, frp));
+  }
+  return c;
+}
+
+// surfdisp96 model set-up for one column: sphere() (ar = 6370) when
+// sphere != 0, extremal velocities and the start value.  d/a/b/r are the
+// layer arrays (top-down, length L) and are flattened in place; rhoR/rhoL
+// receive the Rayleigh/Love density mappings.
+__device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, const float* r, float* rhoR, float* rhoL,
+                           ColInfo& ci) {
+  if (sphere) {
+    const double ar = 6370.0;
+    double dr = 0.0, r0 = ar;
+    d[L - 1] = 1.0f;
+    for (int i = 0; i < L; ++i) {
+      dr = dadd(dr, (double)d[i]);
+      const double r1 = dsub(ar, dr);
+      const double z0 = dmul(ar, log(ddiv(ar, r0)));
+      const double z1 = dmul(ar, log(ddiv(ar, r1)));
+      d[i] = (float)dsub(z1, z0);
+      const double tmp = ddiv(dadd(ar, ar), dadd(r0, r1));
+      a[i] = (float)dmul((double)a[i], tmp);
+      b[i] = (float)dmul((double)b[i], tmp);
+      const float btp = (float)tmp;
+      rhoR[i] = fmul(r[i], (float)pow((double)btp, (double)(-2.275f)));
+      const float b2 = fmul(btp, btp), b4 = fmul(b2, b2), b5 = fmul(b4, btp);
+      rhoL[i] = fmul(r[i], fdiv(1.0f, b5));
+      r0 = r1;
+    }
+    d[L - 1] = 0.0f;
+  } else {
+    for (int i = 0; i < L; ++i) { rhoR[i] = r[i]; rhoL[i] = r[i]; }
+  }
+  ci.llw = (b[0] <= 0.0f) ? 2 : 1;
+  int jmn = 0, jsol = 1;
+  float betmx = -1.e20f, betmn = 1.e20f;
+  for (int i = 0; i < L; ++i) {
+    if (b[i] > 0.01f && b[i] < betmn) { betmn = b[i]; jmn = i; jsol = 1; }
+    else if (b[i] <= 0.01f && a[i] < betmn) { betmn = a[i]; jmn = i; jsol = 0; }
+    if (b[i] > betmx) betmx = b[i];
+  }
+  float cc1 = (jsol == 0) ? betmn : gtsolh(a[jmn], b[jmn]);
+  cc1 = fmul(0.95f, cc1);
+  cc1 = fmul(0.90f, cc1);
+  ci.cc = (double)cc1;
+  ci.betmx = betmx;
+}
+
+__device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
+
+// ---------------------------------------------------------------------------
+// k_prep: node model -> layer models (one thread per column)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __restrict__ vs_in,
+                                              const float* __restrict__ vp_in, const float* __restrict__ rho_in,
+                                              const float* __restrict__ depth, int sphere, int Lmax,
+                                              float4* __restrict__ layR, float4* __restrict__ layL,
+                                              float4* __restrict__ lay0, ColInfo* __restrict__ info,
+                                              float2* __restrict__ chainrule) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  float v[NZMAX], vp[NZMAX], rho[NZMAX], dep[NZMAX];
+  bool valid = true;
+  for (int k = 0; k < nz; ++k) {
+    v[k] = vs_in[col + (size_t)ncol * k];
+    dep[k] = depth[k];
+    if (vp_in) {
+      vp[k] = vp_in[col + (size_t)ncol * k];
+      rho[k] = rho_in[col + (size_t)ncol * k];
+    } else {
+      brocher(v[k], vp[k], rho[k]);
+    }
+    if (!finitef(v[k]) || !finitef(vp[k]) || !finitef(rho[k]) || v[k] < 0.0f || !(vp[k] > 0.0f) || !(rho[k] > 0.0f))
+      valid = false;
+  }
+  int nw = 0;
+  while (nw < nz - 1 && v[nw] == 0.0f) ++nw;
+  for (int k = nw; k < nz; ++k)
+    if (!(v[k] > 0.0f)) valid = false;
+  for (int k = 0; k < nz; ++k) {
+    float drda = 0.0f, dadb = 0.0f;
+    brocher_deriv(vp[k], v[k], drda, dadb);
+    chainrule[(size_t)k * ncol + col] = make_float2(dadb, drda);
+  }
+  // grid2LayerModel (SurfaceWave.cpp:113-155), fluid nodes merged into one layer
+  float th[LMAX], a[LMAX], b[LMAX], r[LMAX], rR[LMAX], rL[LMAX];
+  const int n = 4;
+  int L, istart, k = 0;
+  if (nw > 0) {
+    L = (nz - nw) + (nz - nw - 1) * 3 + 1;
+    istart = nw;
+    th[0] = fsub(dep[nw], dep[0]);
+    r[0] = rho[0];
+    b[0] = 0.0f;
+    a[0] = vp[0];
+    k = 1;
+  } else {
+    L = nz + (nz - 1) * 3;
+    istart = 0;
+  }
+  for (int i = istart; i < nz - 1; ++i) {
+    const float thk = fdiv(fsub(dep[i + 1], dep[i]), (float)n);
+    const float dvp = fsub(vp[i + 1], vp[i]), dvs = fsub(v[i + 1], v[i]), drh = fsub(rho[i + 1], rho[i]);
+    for (int j = 0; j < n; ++j) {
+      const float w = (float)(2 * j + 1);
+      th[k] = thk;
+      a[k] = (float)dadd((double)vp[i], ddiv((double)fmul(w, dvp), 2.0 * n));
+      b[k] = (float)dadd((double)v[i], ddiv((double)fmul(w, dvs), 2.0 * n));
+      r[k] = (float)dadd((double)rho[i], ddiv((double)fmul(w, drh), 2.0 * n));
+      ++k;
+    }
+  }
+  th[L - 1] = 0.0f;
+  a[L - 1] = vp[nz - 1];
+  b[L - 1] = v[nz - 1];
+  r[L - 1] = rho[nz - 1];
+  for (int m = 0; m < L; ++m) lay0[(size_t)col * Lmax + m] = make_float4(th[m], a[m], b[m], r[m]);
+  ColInfo ci;
+  ci.L = L;
+  ci.nw = nw;
+  ci.valid = valid ? 1 : 0;
+  sd96_setup(L, sphere, th, a, b, r, rR, rL, ci);
+  for (int m = 0; m < L; ++m) {
+    const size_t o = (size_t)(L - 1 - m) * ncol + col;
+    layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
+    layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
+  }
+  info[col] = ci;
+}
+
+// k_prep_layers: layered models (surfdisp96_ input) -> layer models
+__global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ thk, const float* __restrict__ vp,
+                              const float* __restrict__ vs, const float* __restrict__ rho, int sphere,
+                              float4* __restrict__ layR, float4* __restrict__ layL, ColInfo* __restrict__ info) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= nmodel) return;
+  float th[LMAX], a[LMAX], b[LMAX], r[LMAX], rR[LMAX], rL[LMAX];
+  bool valid = true;
+  for (int m = 0; m < nlayer; ++m) {
+    const size_t o = (size_t)col * nlayer + m;
+    th[m] = thk[o]; a[m] = vp[o]; b[m] = vs[o]; r[m] = rho[o];
+    if (!finitef(th[m]) || !finitef(a[m]) || !finitef(b[m]) || !finitef(r[m])) valid = false;
+  }
+  ColInfo ci;
+  ci.L = nlayer;
+  ci.nw = (b[0] <= 0.0f) ? 1 : 0;
+  ci.valid = valid ? 1 : 0;
+  sd96_setup(nlayer, sphere, th, a, b, r, rR, rL, ci);
+  for (int m = 0; m < nlayer; ++m) {
+    const size_t o = (size_t)(nlayer - 1 - m) * nmodel + col;
+    layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
+    layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
+  }
+  info[col] = ci;
+}
+
+// ---------------------------------------------------------------------------
+// k_roots: one thread per (column, chain)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __restrict__ chains,
+                                               const double* __restrict__ periods, const float4* __restrict__ layR,
+                                               const float4* __restrict__ layL, const ColInfo* __restrict__ info,
+                                               int refine, double rtol, int sngl, int retry, double* __restrict__ croot,
+                                               int32_t* __restrict__ cstat, int32_t* __restrict__ ierr_out,
+                                               unsigned long long* __restrict__ nevals) {
+  // nevals[0]: evaluations, nevals[1]: Rayleigh layer-evaluations,
+  // nevals[2]: Love layer-evaluations
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const ChainDesc cd = chains[blockIdx.y];
+  unsigned long long my_evals = 0;
+  // every lane runs run_chain (its warp vote needs the full warp); lanes
+  // past the last column or with an invalid model take part inactive
+  const bool inrange = col < ncol;
+  const int ccol = inrange ? col : 0;
+  const ColInfo ci = info[ccol];
+  const bool active = inrange && ci.valid;
+  double* outp = croot + (size_t)cd.out_off * ncol + ccol;
+  int32_t* stp = cstat + (size_t)cd.out_off * ncol + ccol;
+  if (inrange && !ci.valid) {
+    for (int i = 0; i < cd.nmode * cd.np; ++i) { outp[(size_t)i * ncol] = 0.0; stp[(size_t)i * ncol] = ST_NAN_INPUT; }
+    if (ierr_out) ierr_out[col] = 1;
+  }
+  LayerView V;
+  V.lay = (cd.iwave == 2) ? layR : layL;
+  V.ncol = ncol;
+  V.col = ccol;
+  V.L = ci.L;
+  V.llw = ci.llw;
+  ChainParams P;
+  P.t = periods + cd.t_off;
+  P.kmax = cd.np;
+  P.nmode = cd.nmode;
+  P.igr = cd.igr;
+  P.iwave = cd.iwave;
+  P.refine = refine;
+  P.rtol = rtol;
+  P.sngl = sngl;
+  P.cc = ci.cc;
+  P.betmx = ci.betmx;
+  P.retry = retry;
+  double cbuf[KMAX_CHAIN];
+  double cbbuf[KMAX_CHAIN + 24];
+  ChainIO io;
+  io.c = cbuf;
+  io.cb = cbbuf;
+  io.out = outp;
+  io.st = stp;
+  io.stride = cd.np * ncol;
+  io.ostride = ncol;
+  ChainState s;
+  run_chain(V, P, io, s, active);
+  if (active) {
+    if (s.iterlim)
+      for (int i = 0; i < cd.nmode * cd.np; ++i)
+        if (stp[(size_t)i * ncol] == ST_OK) stp[(size_t)i * ncol] = ST_ITER_LIMIT;
+    if (ierr_out) ierr_out[col] = s.ierr;
+    my_evals = (unsigned long long)s.nevals;
+  }
+  // layers per evaluation: the half-space, L-2-(llw-1)+1 propagated layers
+  // and the fluid top when llw = 2 -- i.e. L for every evaluation
+  unsigned long long my_layers = my_evals * (unsigned long long)(active ? ci.L : 0);
+  for (int o = 16; o > 0; o >>= 1) {
+    my_evals += __shfl_down_sync(0xffffffffu, my_evals, o);
+    my_layers += __shfl_down_sync(0xffffffffu, my_layers, o);
+  }
+  if ((threadIdx.x & 31) == 0 && my_evals) {
+    atomicAdd(nevals, my_evals);
+    atomicAdd(nevals + (cd.iwave == 2 ? 1 : 2), my_layers);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_eigen: one block per column, threads over output slots
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int worst_status(int a, int b) {
+  // NO_ROOT / NAN dominate, then ITER_LIMIT, then RETRIED
+  auto rank = [](int s) { return s == ST_NAN_INPUT ? 4 : s == ST_NO_ROOT ? 3 : s == ST_ITER_LIMIT ? 2 : s == ST_RETRIED ? 1 : 0; };
+  return rank(a) >= rank(b) ? a : b;
+}
+
+// _flat2sphere (surfdisp.cpp:17-51)
+__device__ __forceinline__ double flat2sphere(double t, double c, int love, int group) {
+  const double ar = 6371.0;
+  const double omega = 2.0 * 3.141592653589793 / t;
+  const double x = (love ? 1.5 : 0.5) * c / (ar * omega);
+  const double tm = sqrt(1. + x * x);
+  return group ? c * tm : c / tm;
+}
+
+// node contribution x_b + x_a*dadb + x_r*drda*dadb of one pass, scaled by s
+__device__ __forceinline__ void accumulate_nodes(double* kacc, const double* na, const double* nb, const double* nr,
+                                                 const float2* cr, int nz, double s, bool has_a) {
+  for (int i = 0; i < nz; ++i) {
+    const double dadb = cr[i].x, drda = cr[i].y;
+    double v = nb[i];
+    if (has_a) v = v + na[i] * dadb;
+    v = v + nr[i] * drda * dadb;
+    kacc[i] += s * v;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+                                               const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
+                                               const SlotDesc* __restrict__ slots, int nslots,
+                                               const double* __restrict__ croot, const int32_t* __restrict__ cstat,
+                                               int sphere, int path, double* __restrict__ vc, double* __restrict__ vout,
+                                               double* __restrict__ kernel, int32_t* __restrict__ status) {
+  extern __shared__ double sm[];
+  const int col = blockIdx.x;
+  const ColInfo ci = info[col];
+  const int L = ci.L;
+  double* drs = sm;
+  double* zd = drs + L;
+  double* za = zd + L;
+  double* zb = za + L;
+  double* zrR = zb + L;
+  double* zrL = zrR + L;
+  double* vtp = zrL + L;
+  double* rtR = vtp + L;
+  double* rtL = rtR + L;
+  float2* crs = (float2*)(rtL + L);  // nz chain-rule factors
+  const float4* lc = lay0 + (size_t)col * Lmax;
+  // bldsph (sregn96.f90:130-184 / slegn96.f90:107-167), ar = 6371
+  if (threadIdx.x == 0) {
+    double dr = 0.0;
+    for (int i = 0; i < L; ++i) {
+      dr = dr + ((i == L - 1) ? 1.0 : (double)lc[i].x);
+      drs[i] = dr;
+    }
+  }
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) crs[i] = chainrule[(size_t)i * ncol + col];
+  __syncthreads();
+  const double ar = 6371.0;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    const float4 l = lc[i];
+    if (sphere) {
+      const double r0 = (i == 0) ? ar : ar - drs[i - 1];
+      const double r1 = ar - drs[i];
+      const double z0 = ar * log(ar / r0), z1 = ar * log(ar / r1);
+      const double tmp = (2.0 * ar) / (r0 + r1);
+      vtp[i] = tmp;
+      rtR[i] = pow(tmp, (double)(-2.275f));
+      const double t2 = tmp * tmp, t4 = t2 * t2, t5 = t4 * tmp;
+      rtL[i] = 1.0 / t5;
+      za[i] = (double)l.y * tmp;
+      zb[i] = (double)l.z * tmp;
+      zrR[i] = (double)l.w * rtR[i];
+      zrL[i] = (double)l.w * rtL[i];
+      zd[i] = (i == L - 1) ? 0.0 : z1 - z0;
+    } else {
+      vtp[i] = 1.0; rtR[i] = 1.0; rtL[i] = 1.0;
+      za[i] = l.y; zb[i] = l.z; zrR[i] = l.w; zrL[i] = l.w;
+      zd[i] = l.x;
+    }
+  }
+  __syncthreads();
+  EigModel MR, ML;
+  MR.zd = zd; MR.za = za; MR.zb = zb; MR.zrho = zrR; MR.vtp = vtp; MR.rtp = rtR; MR.L = L;
+  ML.zd = zd; ML.za = za; ML.zb = zb; ML.zrho = zrL; ML.vtp = vtp; ML.rtp = rtL; ML.L = L;
+
+  double scr[LMAX * 6];
+  double kacc[NZMAX], na[NZMAX], nb[NZMAX], nr[NZMAX];
+  for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
+    const SlotDesc sd = slots[s];
+    const bool love = sd.wtype >= 2;
+    const bool group = (sd.wtype == 1 || sd.wtype == 3);
+    const double c0 = croot[(size_t)sd.r0 * ncol + col];
+    int st = cstat[(size_t)sd.r0 * ncol + col];
+    double c1 = 0.0, c2 = 0.0;
+    const bool three = (path == 0) && group;
+    if (three) {
+      c1 = croot[(size_t)sd.r1 * ncol + col];
+      c2 = croot[(size_t)sd.r2 * ncol + col];
+      st = worst_status(st, cstat[(size_t)sd.r1 * ncol + col]);
+      st = worst_status(st, cstat[(size_t)sd.r2 * ncol + col]);
+    }
+    const size_t oo = (size_t)sd.oslot * ncol + col;
+    bool dead = !ci.valid || c0 == 0.0 || (three && (c1 == 0.0 || c2 == 0.0));
+    if (!ci.valid) st = ST_NAN_INPUT;
+    else if (dead) st = ST_NO_ROOT;
+    if (status) status[oo] = st;
+    if (dead) {
+      vc[oo] = 0.0;
+      vout[oo] = 0.0;
+      if (path == 0)
+        for (int i = 0; i < nz; ++i) kernel[((size_t)sd.oslot * nz + i) * ncol + col] = 0.0;
+      continue;
+    }
+    const EigModel& M = love ? ML : MR;
+    if (path == 1) {  // get_2d_map: disp1D (SurfaceWave.cpp:177-255)
+      if (!group) {
+        const double v = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
+        vc[oo] = v;
+        vout[oo] = v;
+      } else {
+        vc[oo] = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
+        const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
+        double ugr, norm;
+        if (love) love_pass(M, omega, wvno, scr, ugr, norm);
+        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
+        double tm = 1.0;
+        if (sphere) {
+          const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
+          tm = sqrt(1. + x * x);
+        }
+        vout[oo] = ugr * tm;
+      }
+      continue;
+    }
+    // ---- get_1d_kernel: kernel1D (SurfaceWave.cpp:266-412) ----
+    for (int i = 0; i < nz; ++i) kacc[i] = 0.0;
+    const int stride = love ? 3 : 6;
+    const double* fac_a = M.vtp;
+    const double* fac_r = M.rtp;
+    if (!group) {
+      const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
+      double ugr, norm;
+      if (love) love_pass(M, omega, wvno, scr, ugr, norm);
+      else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
+      double tm = 1.0;
+      if (sphere) {
+        const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
+        tm = sqrt(1. + x * x);
+      }
+      const double tm3 = tm * tm * tm;
+      if (love) {
+        param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, nb);
+        param_convert_dev(scr, stride, 1, norm, fac_r, L, nz, ci.nw, nr);
+      } else {
+        param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, na);
+        param_convert_dev(scr, stride, 1, norm, fac_a, L, nz, ci.nw, nb);
+        param_convert_dev(scr, stride, 2, norm, fac_r, L, nz, ci.nw, nr);
+      }
+      accumulate_nodes(kacc, na, nb, nr, crs, nz, 1.0 / tm3, !love);
+      const double cs = c0 / tm;
+      vc[oo] = cs;
+      vout[oo] = cs;
+    } else {
+      // sregnpu / slegnpu (sregn96.f90:1737-1878, slegn96.f90:785-918)
+      const double twopi = 2.0 * PI_F;
+      const double cp = c0;
+      double cg = 0.0, f1 = 0.0, f2 = 0.0, dtt = 1.0, tm = 1.0, tm1 = 0.0;
+      for (int pass = 0; pass < 3; ++pass) {
+        const double tt = (pass == 0) ? sd.t : (pass == 1) ? sd.t1 : sd.t2;
+        const double cc = (pass == 0) ? c0 : (pass == 1) ? c1 : c2;
+        const double omega = twopi / tt, wvno = omega / cc;
+        double ugr, norm;
+        if (love) love_pass(M, omega, wvno, scr, ugr, norm);
+        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
+        if (love) {
+          param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, nb);
+          param_convert_dev(scr, stride, 1, norm, fac_r, L, nz, ci.nw, nr);
+        } else {
+          param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, na);
+          param_convert_dev(scr, stride, 1, norm, fac_a, L, nz, ci.nw, nb);
+          param_convert_dev(scr, stride, 2, norm, fac_r, L, nz, ci.nw, nr);
+        }
+        double coef;
+        if (pass == 0) {
+          cg = ugr;
+          const double uc1 = cg / cp;
+          dtt = sd.t2 - sd.t1;
+          f1 = uc1 * (2.0 - uc1);
+          f2 = uc1 * uc1 * sd.t;
+          if (sphere) {
+            const double om0 = twopi / sd.t;
+            const double k = love ? 1.5 : 0.5;
+            const double x = (love ? 3.0 : 1.0) * cp / (2. * ar * om0);
+            tm = sqrt(1. + x * x);
+            const double y = k / (ar * om0);
+            tm1 = (y * y) / tm;
+            coef = cg * cp * tm1;
+          } else {
+            coef = 0.0;
+          }
+        } else if (pass == 1) {
+          coef = tm * (f2 / dtt);
+        } else {
+          coef = tm * (f1 - f2 / dtt);
+        }
+        if (coef != 0.0) accumulate_nodes(kacc, na, nb, nr, crs, nz, coef, !love);
+      }
+      vc[oo] = cp / tm;
+      vout[oo] = cg * tm;
+    }
+    // water / merged fluid nodes carry no kernel (SurfaceWave.cpp:495)
+    for (int i = 0; i < nz; ++i) {
+      const double v = (i < ci.nw) ? 0.0 : kacc[i];
+      kernel[((size_t)sd.oslot * nz + i) * ncol + col] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Frechet rows (SurfaceWave.cpp:630-659): one block per row
+// ---------------------------------------------------------------------------
+__global__ void k_frechet(int nx, int ny, int nz, int kmax, const double* __restrict__ kernel, const int32_t* __restrict__ slot,
+                          const float* __restrict__ fdm, int32_t* __restrict__ nnz, int32_t* __restrict__ idx,
+                          float* __restrict__ val) {
+  const int r = blockIdx.x;
+  const int nxi = nx - 2, nyi = ny - 2;
+  const int n = nxi * nyi * (nz - 1);
+  const size_t ncol = (size_t)nx * ny;
+  const int s = slot[r];
+  if (s < 0 || s >= kmax) {  // invalid period slot: empty row
+    if (threadIdx.x == 0) nnz[r] = 0;
+    return;
+  }
+  const float* f = fdm + (size_t)r * ncol;
+  int32_t* oi = idx + (size_t)r * n;
+  float* ov = val + (size_t)r * n;
+  __shared__ int base;
+  __shared__ int wsum[32];
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < n; j0 += blockDim.x) {
+    const int j = j0 + threadIdx.x;
+    float v = 0.0f;
+    bool keep = false;
+    if (j < n) {
+      const int ix = j % nxi, iy = (j / nxi) % nyi, iz = j / (nxi * nyi);
+      const size_t ii = (size_t)(iy + 1) * nx + ix + 1;
+      v = (float)((double)f[(ix + 1) + (size_t)nx * (iy + 1)] * kernel[ii + ncol * (iz + (size_t)nz * s)]);
+      keep = fabsf(v) > 0.0f;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    const int wpre = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) wsum[wid] = __popc(bal);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) { if (w < wid) off += wsum[w]; tot += wsum[w]; }
+    if (keep) { oi[base + off + wpre] = j; ov[base + off + wpre] = v; }
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) nnz[r] = base;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+  template <class T> T* as() const { return (T*)p; }
+};
+
+struct Plan {
+  std::vector<ChainDesc> chains;
+  std::vector<double> periods;
+  std::vector<SlotDesc> slots;
+  int kmax = 0, nroot = 0;
+  DevBuf d_chains, d_periods, d_slots;
+};
+
+int nt_of(const double* col, int ntmax) {
+  int n = 0;
+  while (n < ntmax && col[n] != -1) ++n;
+  return n;
+}
+
+}  // namespace
+
+struct swdk_ctx {
+  swdk_config cfg;
+  cudaStream_t stream = nullptr;
+  std::vector<double> tab[4];
+  int ntmax[4] = {0, 0, 0, 0}, nmode[4] = {0, 0, 0, 0};
+  std::vector<float> depth;
+  bool have_periods = false;
+  bool dirty = true;
+  Plan plan[2];  // 0: get_1d_kernel, 1: get_2d_map
+  DevBuf layR, layL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr;
+  DevBuf in_vs, in_vp, in_rho, out_vc, out_vout, out_kernel, out_status, in_misc;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // stage marks; ev[4]: call done
+  unsigned long long* h_nevals = nullptr;
+  swdk_stats stats;
+  bool stats_pending = false;
+  std::string err;
+};
+
+namespace {
+
+int fail(swdk_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(ctx, SWDK_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int find_chain(Plan& P, std::vector<std::vector<double>>& lists, int iwave, const std::vector<double>& lst, int nmode) {
+  for (size_t i = 0; i < P.chains.size(); ++i) {
+    if (P.chains[i].iwave == iwave && lists[i] == lst) {
+      P.chains[i].nmode = std::max(P.chains[i].nmode, nmode);
+      return (int)i;
+    }
+  }
+  ChainDesc d;
+  d.t_off = 0;
+  d.np = (int)lst.size();
+  d.nmode = nmode;
+  d.iwave = iwave;
+  d.igr = 0;
+  d.out_off = 0;
+  P.chains.push_back(d);
+  lists.push_back(lst);
+  return (int)P.chains.size() - 1;
+}
+
+int build_plan(swdk_ctx* ctx, int path) {
+  Plan& P = ctx->plan[path];
+  P.chains.clear();
+  P.periods.clear();
+  P.slots.clear();
+  std::vector<std::vector<double>> lists;
+  struct Pending { int w, oslot, ch0, ch1, ch2, mode, k; double t, t1, t2; };
+  std::vector<Pending> pend;
+  int idx = 0;
+  for (int w = 0; w < 4; ++w) {
+    if (ctx->ntmax[w] * ctx->nmode[w] <= 0) continue;
+    for (int mode = 0; mode < ctx->nmode[w]; ++mode) {
+      const double* col = ctx->tab[w].data() + (size_t)mode * ctx->ntmax[w];
+      const int nt = nt_of(col, ctx->ntmax[w]);
+      if (nt == 0) continue;
+      if (nt > SWDK_MAX_PERIODS) return fail(ctx, SWDK_E_LIMIT, "more than SWDK_MAX_PERIODS periods in one list");
+      const int iwave = (w < 2) ? 2 : 1;
+      std::vector<double> lst(col, col + nt), l1(nt), l2(nt);
+      const double dt = 0.01;
+      for (int i = 0; i < nt; ++i) { l1[i] = col[i] * (1.0 + 0.5 * dt); l2[i] = col[i] * (1.0 - 0.5 * dt); }
+      const int ch0 = find_chain(P, lists, iwave, lst, mode + 1);
+      int ch1 = -1, ch2 = -1;
+      const bool group = (w == 1 || w == 3);
+      if (path == 0 && group) {
+        ch1 = find_chain(P, lists, iwave, l1, mode + 1);
+        ch2 = find_chain(P, lists, iwave, l2, mode + 1);
+      }
+      for (int k = 0; k < nt; ++k) pend.push_back({w, idx + k, ch0, ch1, ch2, mode, k, lst[k], l1[k], l2[k]});
+      idx += nt;
+    }
+  }
+  P.kmax = idx;
+  int off = 0;
+  for (size_t i = 0; i < P.chains.size(); ++i) {
+    P.chains[i].t_off = (int)P.periods.size();
+    P.periods.insert(P.periods.end(), lists[i].begin(), lists[i].end());
+    P.chains[i].out_off = off;
+    off += P.chains[i].nmode * P.chains[i].np;
+  }
+  P.nroot = off;
+  auto rslot = [&](int ch, int mode, int k) { return ch < 0 ? -1 : P.chains[ch].out_off + mode * P.chains[ch].np + k; };
+  for (const Pending& q : pend) {
+    SlotDesc s;
+    s.wtype = q.w;
+    s.oslot = q.oslot;
+    s.r0 = rslot(q.ch0, q.mode, q.k);
+    s.r1 = rslot(q.ch1, q.mode, q.k);
+    s.r2 = rslot(q.ch2, q.mode, q.k);
+    s.t = q.t;
+    s.t1 = q.t1;
+    s.t2 = q.t2;
+    P.slots.push_back(s);
+  }
+  if (P.chains.empty()) return fail(ctx, SWDK_E_NOPERIODS, "no periods");
+  CK(P.d_chains.ensure(P.chains.size() * sizeof(ChainDesc)));
+  CK(P.d_periods.ensure(P.periods.size() * sizeof(double)));
+  CK(P.d_slots.ensure(P.slots.size() * sizeof(SlotDesc)));
+  CK(cudaMemcpy(P.d_chains.p, P.chains.data(), P.chains.size() * sizeof(ChainDesc), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.d_periods.p, P.periods.data(), P.periods.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.d_slots.p, P.slots.data(), P.slots.size() * sizeof(SlotDesc), cudaMemcpyHostToDevice));
+  return SWDK_OK;
+}
+
+int ensure_plans(swdk_ctx* ctx) {
+  if (!ctx->have_periods) return fail(ctx, SWDK_E_NOPERIODS, "swdk_set_periods not called");
+  if (!ctx->dirty) return SWDK_OK;
+  for (int p = 0; p < 2; ++p) {
+    int r = build_plan(ctx, p);
+    if (r) return r;
+  }
+  ctx->dirty = false;
+  return SWDK_OK;
+}
+
+// model preparation + roots + eigen for one call on device pointers
+int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+               const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
+               cudaStream_t st) {
+  if (nx <= 0 || ny <= 0 || !d_vs || !d_vc || !d_vout || (path == 0 && !d_kernel))
+    return fail(ctx, SWDK_E_ARG, "bad arguments");
+  if ((d_vp == nullptr) != (d_rho == nullptr)) return fail(ctx, SWDK_E_ARG, "vp and rho must both be given or both NULL");
+  if ((int)ctx->depth.size() != nz) return fail(ctx, SWDK_E_NODEPTH, "nz does not match swdk_set_depth");
+  if (nz < 2 || nz > SWDK_MAX_NZ || 4 * nz - 3 > SWDK_MAX_LAYERS) return fail(ctx, SWDK_E_LIMIT, "nz out of range");
+  int r = ensure_plans(ctx);
+  if (r) return r;
+  Plan& P = ctx->plan[path];
+  const int ncol = nx * ny;
+  const int Lmax = 4 * nz - 3;
+  CK(ctx->layR.ensure((size_t)Lmax * ncol * sizeof(float4)));
+  CK(ctx->layL.ensure((size_t)Lmax * ncol * sizeof(float4)));
+  CK(ctx->lay0.ensure((size_t)Lmax * ncol * sizeof(float4)));
+  CK(ctx->info.ensure((size_t)ncol * sizeof(ColInfo)));
+  CK(ctx->chainrule.ensure((size_t)nz * ncol * sizeof(float2)));
+  CK(ctx->croot.ensure((size_t)P.nroot * ncol * sizeof(double)));
+  CK(ctx->cstat.ensure((size_t)P.nroot * ncol * sizeof(int32_t)));
+  CK(ctx->nevals.ensure(3 * sizeof(unsigned long long)));
+  CK(ctx->depth_d.ensure((size_t)nz * sizeof(float)));
+  CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, 3 * sizeof(unsigned long long), st));
+  CK(cudaEventRecord(ctx->ev[0], st));
+  k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
+                                             Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
+                                             ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                             ctx->chainrule.as<float2>());
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[1], st));
+  const int bt = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : 128;
+  dim3 gr((ncol + bt - 1) / bt, (unsigned)P.chains.size());
+  k_roots<<<gr, bt, 0, st>>>(ncol, P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
+                             ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol,
+                             ctx->cfg.sngl, 1, ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), nullptr,
+                             ctx->nevals.as<unsigned long long>());
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[2], st));
+  const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
+  const int nslots = (int)P.slots.size();
+  const int et = std::min(128, ((nslots + 31) / 32) * 32);
+  k_eigen<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                  ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), nslots,
+                                  ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
+                                  d_vout, d_kernel, d_status);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[3], st));
+  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(ctx->ev[4], st));
+  ctx->stats_pending = true;
+  ctx->stats.nchains = (int)P.chains.size();
+  ctx->stats.nslots = P.kmax;
+  return SWDK_OK;
+}
+
+void collect_stats(swdk_ctx* ctx) {
+  if (!ctx->stats_pending) return;
+  cudaEventSynchronize(ctx->ev[4]);
+  ctx->stats_pending = false;
+  ctx->stats.secular_evals = (int64_t)ctx->h_nevals[0];
+  ctx->stats.layer_evals_rayleigh = (int64_t)ctx->h_nevals[1];
+  ctx->stats.layer_evals_love = (int64_t)ctx->h_nevals[2];
+  cudaEventElapsedTime(&ctx->stats.ms_prep, ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&ctx->stats.ms_roots, ctx->ev[1], ctx->ev[2]);
+  cudaEventElapsedTime(&ctx->stats.ms_eigen, ctx->ev[2], ctx->ev[3]);
+}
+
+int run_host(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
+             double* vc, double* vout, double* kernel, int32_t* status) {
+  if (!ctx || nx <= 0 || ny <= 0 || !vs || !vc || !vout || (path == 0 && !kernel)) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  CK(cudaSetDevice(ctx->cfg.device));
+  int r = ensure_plans(ctx);
+  if (r) return r;
+  const size_t ncol = (size_t)nx * ny;
+  const int kmax = ctx->plan[path].kmax;
+  cudaStream_t st = ctx->stream;
+  CK(ctx->in_vs.ensure(ncol * nz * sizeof(float)));
+  if (vp) {
+    CK(ctx->in_vp.ensure(ncol * nz * sizeof(float)));
+    CK(ctx->in_rho.ensure(ncol * nz * sizeof(float)));
+  }
+  CK(ctx->out_vc.ensure(ncol * kmax * sizeof(double)));
+  CK(ctx->out_vout.ensure(ncol * kmax * sizeof(double)));
+  CK(ctx->out_status.ensure(ncol * kmax * sizeof(int32_t)));
+  if (path == 0) CK(ctx->out_kernel.ensure(ncol * nz * kmax * sizeof(double)));
+  CK(cudaMemcpyAsync(ctx->in_vs.p, vs, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (vp) {
+    CK(cudaMemcpyAsync(ctx->in_vp.p, vp, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->in_rho.p, rho, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
+  }
+  r = run_device(ctx, path, nx, ny, nz, ctx->in_vs.as<float>(), vp ? ctx->in_vp.as<float>() : nullptr,
+                 vp ? ctx->in_rho.as<float>() : nullptr, ctx->out_vc.as<double>(), ctx->out_vout.as<double>(),
+                 path == 0 ? ctx->out_kernel.as<double>() : nullptr, ctx->out_status.as<int32_t>(), st);
+  if (r) return r;
+  CK(cudaMemcpyAsync(vc, ctx->out_vc.p, ncol * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(vout, ctx->out_vout.p, ncol * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (status) CK(cudaMemcpyAsync(status, ctx->out_status.p, ncol * kmax * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  if (path == 0)
+    CK(cudaMemcpyAsync(kernel, ctx->out_kernel.p, ncol * nz * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  collect_stats(ctx);
+  return SWDK_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int swdk_config_default(swdk_config* cfg) {
+  if (!cfg) return SWDK_E_ARG;
+  cfg->device = 0;
+  cfg->refine = SWDK_REFINE_TIGHT;
+  cfg->rtol = 1e-10;
+  cfg->sngl = 1;
+  cfg->sphere = 1;
+  cfg->block_roots = 0;
+  return SWDK_OK;
+}
+
+int swdk_create(swdk_ctx** out, const swdk_config* cfg) {
+  if (!out) return SWDK_E_ARG;
+  *out = nullptr;
+  swdk_ctx* ctx = new swdk_ctx();
+  if (cfg) ctx->cfg = *cfg;
+  else swdk_config_default(&ctx->cfg);
+  if (ctx->cfg.rtol <= 0.0) ctx->cfg.rtol = 1e-10;
+  memset(&ctx->stats, 0, sizeof(ctx->stats));
+  cudaError_t e = cudaSetDevice(ctx->cfg.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_nevals, 3 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    fprintf(stderr, "swdk_create: %s\n", cudaGetErrorString(e));
+    swdk_destroy(ctx);
+    return SWDK_E_CUDA;
+  }
+  ctx->h_nevals[0] = ctx->h_nevals[1] = ctx->h_nevals[2] = 0;
+  *out = ctx;
+  return SWDK_OK;
+}
+
+void swdk_destroy(swdk_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[] = {&ctx->layR, &ctx->layL, &ctx->lay0, &ctx->info, &ctx->chainrule, &ctx->croot, &ctx->cstat,
+                    &ctx->nevals, &ctx->depth_d, &ctx->ierr, &ctx->in_vs, &ctx->in_vp, &ctx->in_rho,
+                    &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc};
+  for (DevBuf* b : bufs) b->release();
+  for (int p = 0; p < 2; ++p) {
+    ctx->plan[p].d_chains.release();
+    ctx->plan[p].d_periods.release();
+    ctx->plan[p].d_slots.release();
+  }
+  for (int i = 0; i < 5; ++i)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int swdk_set_periods(swdk_ctx* ctx, const double* tRc, int ntRc, int nmRc, const double* tRg, int ntRg, int nmRg,
+                     const double* tLc, int ntLc, int nmLc, const double* tLg, int ntLg, int nmLg) {
+  if (!ctx) return SWDK_E_ARG;
+  const double* t[4] = {tRc, tRg, tLc, tLg};
+  const int nt[4] = {ntRc, ntRg, ntLc, ntLg}, nm[4] = {nmRc, nmRg, nmLc, nmLg};
+  for (int w = 0; w < 4; ++w) {
+    if (nt[w] < 0 || nm[w] < 0 || (nt[w] * nm[w] > 0 && !t[w])) return fail(ctx, SWDK_E_ARG, "bad period table");
+    if (nt[w] > SWDK_MAX_PERIODS) return fail(ctx, SWDK_E_LIMIT, "period table longer than SWDK_MAX_PERIODS");
+    ctx->ntmax[w] = nt[w];
+    ctx->nmode[w] = nm[w];
+    ctx->tab[w].assign(t[w] ? t[w] : nullptr, t[w] ? t[w] + (size_t)nt[w] * nm[w] : nullptr);
+    for (double v : ctx->tab[w])
+      if (v != -1 && !(v > 0.0)) return fail(ctx, SWDK_E_ARG, "periods must be positive (or -1 padding)");
+  }
+  ctx->have_periods = true;
+  ctx->dirty = true;
+  cudaSetDevice(ctx->cfg.device);
+  return ensure_plans(ctx);
+}
+
+int swdk_set_depth(swdk_ctx* ctx, const float* depth, int nz) {
+  if (!ctx || !depth || nz < 2) return SWDK_E_ARG;
+  if (nz > SWDK_MAX_NZ) return fail(ctx, SWDK_E_LIMIT, "nz > SWDK_MAX_NZ");
+  ctx->depth.assign(depth, depth + nz);
+  return SWDK_OK;
+}
+
+int swdk_kmax(const swdk_ctx* ctx) {
+  if (!ctx || !ctx->have_periods) return 0;
+  int k = 0;
+  for (int w = 0; w < 4; ++w)
+    for (int m = 0; m < ctx->nmode[w]; ++m) k += nt_of(ctx->tab[w].data() + (size_t)m * ctx->ntmax[w], ctx->ntmax[w]);
+  return k;
+}
+
+int swdk_get_1d_kernel(swdk_ctx* ctx, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
+                       double* vc, double* vout, double* kernel, int32_t* status) {
+  return run_host(ctx, 0, nx, ny, nz, vs, vp, rho, vc, vout, kernel, status);
+}
+
+int swdk_get_2d_map(swdk_ctx* ctx, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
+                    double* vc, double* vout, int32_t* status) {
+  return run_host(ctx, 1, nx, ny, nz, vs, vp, rho, vc, vout, nullptr, status);
+}
+
+int swdk_get_1d_kernel_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                              const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
+                              void* stream) {
+  if (!ctx) return SWDK_E_ARG;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  return run_device(ctx, 0, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+}
+
+int swdk_get_2d_map_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                           const float* d_rho, double* d_vc, double* d_vout, int32_t* d_status, void* stream) {
+  if (!ctx) return SWDK_E_ARG;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  return run_device(ctx, 1, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, nullptr, d_status, st);
+}
+
+int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* thk, const float* vp, const float* vs,
+                          const float* rho, int iflsph, int iwave, int mode, int igr, int kmax, const double* t,
+                          double* cg, int32_t* ierr) {
+  if (!ctx || nmodel <= 0 || nlayer < 2 || !thk || !vp || !vs || !rho || !t || !cg || kmax <= 0 || mode < 1 ||
+      (iwave != 1 && iwave != 2))
+    return fail(ctx, SWDK_E_ARG, "bad arguments");
+  if (nlayer > SWDK_MAX_LAYERS || kmax > SWDK_MAX_PERIODS) return fail(ctx, SWDK_E_LIMIT, "size beyond limits");
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = ctx->stream;
+  const size_t nm = nmodel, nin = nm * nlayer;
+  CK(ctx->in_misc.ensure(4 * nin * sizeof(float) + kmax * sizeof(double) + sizeof(ChainDesc)));
+  float* d_in = ctx->in_misc.as<float>();
+  double* d_t = (double*)(d_in + 4 * nin);
+  ChainDesc* d_ch = (ChainDesc*)(d_t + kmax);
+  CK(cudaMemcpyAsync(d_in, thk, nin * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_in + nin, vp, nin * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_in + 2 * nin, vs, nin * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_in + 3 * nin, rho, nin * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_t, t, kmax * sizeof(double), cudaMemcpyHostToDevice, st));
+  ChainDesc cd;
+  cd.t_off = 0; cd.np = kmax; cd.nmode = mode; cd.iwave = iwave; cd.igr = igr; cd.out_off = 0;
+  CK(cudaMemcpyAsync(d_ch, &cd, sizeof(cd), cudaMemcpyHostToDevice, st));
+  CK(ctx->layR.ensure(nin * sizeof(float4)));
+  CK(ctx->layL.ensure(nin * sizeof(float4)));
+  CK(ctx->info.ensure(nm * sizeof(ColInfo)));
+  CK(ctx->croot.ensure((size_t)mode * kmax * nm * sizeof(double)));
+  CK(ctx->cstat.ensure((size_t)mode * kmax * nm * sizeof(int32_t)));
+  CK(ctx->ierr.ensure(nm * sizeof(int32_t)));
+  CK(ctx->nevals.ensure(3 * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, 3 * sizeof(unsigned long long), st));
+  CK(cudaEventRecord(ctx->ev[0], st));
+  k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_in, d_in + nin, d_in + 2 * nin,
+                                                       d_in + 3 * nin, iflsph, ctx->layR.as<float4>(),
+                                                       ctx->layL.as<float4>(), ctx->info.as<ColInfo>());
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[1], st));
+  k_roots<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(nmodel, d_ch, d_t, ctx->layR.as<float4>(),
+                                                         ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
+                                                         ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, 0,
+                                                         ctx->croot.as<double>(), ctx->cstat.as<int32_t>(),
+                                                         ctx->ierr.as<int32_t>(),
+                                                         ctx->nevals.as<unsigned long long>());
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[2], st));
+  CK(cudaEventRecord(ctx->ev[3], st));
+  // the reference's cg holds the last mode: rows (mode-1)*kmax .. of croot
+  std::vector<double> tmp((size_t)kmax * nm);
+  CK(cudaMemcpyAsync(tmp.data(), ctx->croot.as<double>() + (size_t)(mode - 1) * kmax * nm,
+                     (size_t)kmax * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (ierr) CK(cudaMemcpyAsync(ierr, ctx->ierr.p, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(ctx->ev[4], st));
+  ctx->stats_pending = true;
+  CK(cudaStreamSynchronize(st));
+  for (size_t m = 0; m < nm; ++m)
+    for (int k = 0; k < kmax; ++k) cg[m * kmax + k] = tmp[(size_t)k * nm + m];
+  collect_stats(ctx);
+  return SWDK_OK;
+}
+
+int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, const double* d_kernel, int nrows,
+                             const int32_t* d_row_slot, const float* d_fdm, int32_t* d_nnz, int32_t* d_indices,
+                             float* d_values, void* stream) {
+  if (!ctx || nx < 3 || ny < 3 || nz < 2 || kmax <= 0 || nrows < 0 || !d_kernel || !d_row_slot || !d_fdm || !d_nnz ||
+      !d_indices || !d_values)
+    return fail(ctx, SWDK_E_ARG, "bad arguments");
+  if (nrows == 0) return SWDK_OK;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, d_nnz, d_indices, d_values);
+  CK(cudaGetLastError());
+  return SWDK_OK;
+}
+
+int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out) {
+  if (!ctx || !out) return SWDK_E_ARG;
+  collect_stats(ctx);  // waits for the last call's completion event
+  *out = ctx->stats;
+  return SWDK_OK;
+}
+
+const char* swdk_last_error(const swdk_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+}  // extern "C"

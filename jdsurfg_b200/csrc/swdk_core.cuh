@@ -1,0 +1,695 @@
+// swdk_core.cuh -- device numerics of the surface-wave forward model.
+//
+// Everything here is __host__ __device__ so the same arithmetic can be
+// exercised on the CPU by developer probes; the product runs it only inside
+// the CUDA kernels of swdk_kernels.cu.
+//
+// Reference semantics (JDSurfG, src/SWD):
+//   * secular functions dltar4 (Rayleigh, Dunkin delta matrix) and dltar1
+//     (Love, Haskell) follow surfdisp96.f:712-1095;
+//   * the period/mode continuation, bracket scan and refinement follow
+//     surfdisp96.f:57-370 (surfdisp96) and :400-708 (getsol/nevill/half);
+//   * eigenfunctions and energy integrals follow sregn96.f90:193-1629 and
+//     slegn96.f90:179-670.
+// Restructuring relative to the Fortran (same mathematics):
+//   * per-layer divisions by rho, ra, rb become one reciprocal each;
+//   * E/E^-1 and the f/g/h layer integrals are formed once per layer and
+//     shared by the six intijr integrals (the reference rebuilds them per
+//     integral);
+//   * the up/down compound-matrix vectors in the eigenfunction pass are
+//     normalised by powers of two with an integer exponent instead of
+//     max-division + log (exact scaling, no log per layer);
+//   * the Rayleigh down pass, svfunc and energy are fused in one top-down
+//     sweep; node kernels are formed by _ParamConvert on the fly.
+#pragma once
+#include <cstdint>
+#include <cmath>
+
+#ifdef __CUDACC__
+#define SWDK_HD __host__ __device__ __forceinline__
+#define SWDK_HDI __host__ __device__
+#else
+#define SWDK_HD inline
+#define SWDK_HDI inline
+#endif
+
+namespace swdk {
+
+// ---------------------------------------------------------------------------
+// status codes (per output slot)
+// ---------------------------------------------------------------------------
+enum : int32_t {
+  ST_OK = 0,
+  ST_NO_ROOT = 1,      // no root after the per-period retry (the reference exits)
+  ST_RETRIED = 2,      // found by the reference's single-period retry
+  ST_NAN_INPUT = 3,    // non-finite or non-positive model values
+  ST_ITER_LIMIT = 4,   // refinement hit its iteration cap (reference: 100 in nevill)
+};
+
+constexpr int KMAX_CHAIN = 128;   // periods per chain (host checks)
+constexpr double TWOPI = 2.0 * 3.141592653589793;
+constexpr double PI_F = 3.1415927410125732;  // REAL*4 pi of sregn96/slegn96
+
+// ---------------------------------------------------------------------------
+// small double complex with Fortran (Smith) division
+// ---------------------------------------------------------------------------
+struct cx {
+  double re, im;
+};
+SWDK_HD cx mkc(double r, double i = 0.0) { cx z; z.re = r; z.im = i; return z; }
+SWDK_HD cx operator+(cx a, cx b) { return mkc(a.re + b.re, a.im + b.im); }
+SWDK_HD cx operator-(cx a, cx b) { return mkc(a.re - b.re, a.im - b.im); }
+SWDK_HD cx operator-(cx a) { return mkc(-a.re, -a.im); }
+SWDK_HD cx operator*(cx a, cx b) { return mkc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+SWDK_HD cx operator*(double s, cx a) { return mkc(s * a.re, s * a.im); }
+SWDK_HD cx operator*(cx a, double s) { return mkc(a.re * s, a.im * s); }
+SWDK_HD cx operator/(cx a, double s) { return mkc(a.re / s, a.im / s); }
+SWDK_HD cx operator+(cx a, double s) { return mkc(a.re + s, a.im); }
+SWDK_HD cx operator-(double s, cx a) { return mkc(s - a.re, -a.im); }
+SWDK_HD cx operator/(cx a, cx b) {
+  if (fabs(b.re) >= fabs(b.im)) {
+    double r = b.im / b.re, den = b.re + b.im * r;
+    return mkc((a.re + a.im * r) / den, (a.im - a.re * r) / den);
+  } else {
+    double r = b.re / b.im, den = b.im + b.re * r;
+    return mkc((a.re * r + a.im) / den, (a.im * r - a.re) / den);
+  }
+}
+SWDK_HD cx operator/(double s, cx b) { return mkc(s) / b; }
+SWDK_HD cx csqrt_real(double x) { return x >= 0.0 ? mkc(sqrt(x), 0.0) : mkc(0.0, sqrt(-x)); }
+SWDK_HD cx cexpc(cx z) {
+  double e = exp(z.re);
+  if (z.im == 0.0) return mkc(e, 0.0);
+  double s, c;
+  sincos(z.im, &s, &c);
+  return mkc(e * c, e * s);
+}
+SWDK_HD double cabsc(cx z) { return hypot(z.re, z.im); }
+SWDK_HD double dsign1(double x) { return copysign(1.0, x); }
+
+// exact power-of-two normalisation: v *= 2^-e where 2^e ~ max|v|
+SWDK_HD int pow2_exponent(double t) {
+  int e;
+  frexp(t, &e);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// secular functions on the flattened REAL*4 layer model
+//   lay[mp*ncol + col] = (d, a, b, rho), mp = 0 is the half-space and mp
+//   counts layers upward (bottom-aligned, layer-major)
+// ---------------------------------------------------------------------------
+struct LayerView {
+  const float4* lay;
+  int ncol, col;
+  int L;    // layers including the half-space
+  int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
+  SWDK_HD float4 get(int m) const {  // m: reference (top-down, 0-based) index
+    return lay[(size_t)(L - 1 - m) * ncol + col];
+  }
+};
+
+// dltar4 (surfdisp96.f:798-898)
+SWDK_HDI double dltar4(const LayerView& V, double wvno, double omga) {
+  double omega = omga;
+  if (omega < 1.0e-4) omega = 1.0e-4;
+  const double wvno2 = wvno * wvno;
+  const double iom = 1.0 / omega;
+  float4 h = V.get(V.L - 1);
+  double a = h.y, b = h.z, rho1 = h.w;
+  double xka = omega / a, xkb = omega / b;
+  double ra = sqrt((wvno + xka) * fabs(wvno - xka));
+  double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+  double t = b * iom;
+  double gammk = 2.0 * t * t;
+  double gam = gammk * wvno2;
+  double gamm1 = gam - 1.0;
+  double e0 = rho1 * rho1 * (gamm1 * gamm1 - gam * gammk * ra * rb);
+  double e1 = -rho1 * ra;
+  double e2 = rho1 * (gamm1 - gammk * ra * rb);
+  double e3 = rho1 * rb;
+  double e4 = wvno2 - ra * rb;
+  for (int m = V.L - 2; m >= V.llw - 1; --m) {
+    float4 ly = V.get(m);
+    const double dpth = ly.x;
+    a = ly.y;
+    b = ly.z;
+    const double rho = ly.w;
+    xka = omega / a;
+    xkb = omega / b;
+    t = b * iom;
+    gammk = 2.0 * t * t;
+    gam = gammk * wvno2;
+    ra = sqrt((wvno + xka) * fabs(wvno - xka));
+    rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    const double p = ra * dpth, q = rb * dpth;
+    // var (surfdisp96.f:901-1018)
+    double w, x, cosp, y, z, cosq, pex = 0.0, sex = 0.0;
+    if (wvno < xka) {
+      double sp, cp;
+      sincos(p, &sp, &cp);
+      w = sp / ra; x = -ra * sp; cosp = cp;
+    } else if (wvno == xka) {
+      cosp = 1.0; w = dpth; x = 0.0;
+    } else {
+      pex = p;
+      double fac = (p < 16.0) ? exp(-2.0 * p) : 0.0;
+      cosp = (1.0 + fac) * 0.5;
+      double sp = (1.0 - fac) * 0.5;
+      w = sp / ra; x = ra * sp;
+    }
+    if (wvno < xkb) {
+      double sq, cq;
+      sincos(q, &sq, &cq);
+      y = sq / rb; z = -rb * sq; cosq = cq;
+    } else if (wvno == xkb) {
+      cosq = 1.0; y = dpth; z = 0.0;
+    } else {
+      sex = q;
+      double fac = (q < 16.0) ? exp(-2.0 * q) : 0.0;
+      cosq = (1.0 + fac) * 0.5;
+      double sq = (1.0 - fac) * 0.5;
+      y = sq / rb; z = rb * sq;
+    }
+    const double exa = pex + sex;
+    const double a0 = (exa < 60.0) ? exp(-exa) : 0.0;
+    const double cpcq = cosp * cosq, cpy = cosp * y, cpz = cosp * z, cqw = cosq * w, cqx = cosq * x;
+    const double xy = x * y, xz = x * z, wy = w * y, wz = w * z;
+    // dnka (surfdisp96.f:1051-1095)
+    const double irho = 1.0 / rho;
+    gamm1 = gam - 1.0;
+    const double twgm1 = gam + gamm1, gmgmk = gam * gammk, gmgm1 = gam * gamm1, gm1sq = gamm1 * gamm1;
+    const double rho2 = rho * rho, irho2 = irho * irho;
+    const double a0pq = a0 - cpcq;
+    const double c11 = cpcq - 2.0 * gmgm1 * a0pq - gmgmk * xz - wvno2 * gm1sq * wy;
+    const double c12 = (wvno2 * cpy - cqx) * irho;
+    const double c13 = -(twgm1 * a0pq + gammk * xz + wvno2 * gamm1 * wy) * irho;
+    const double c14 = (cpz - wvno2 * cqw) * irho;
+    const double c15 = -(2.0 * wvno2 * a0pq + xz + wvno2 * wvno2 * wy) * irho2;
+    const double c21 = (gmgmk * cpz - gm1sq * cqw) * rho;
+    const double c22 = cpcq;
+    const double c23 = gammk * cpz - gamm1 * cqw;
+    const double c24 = -wz;
+    const double c41 = (gm1sq * cpy - gmgmk * cqx) * rho;
+    const double c42 = -xy;
+    const double c43 = gamm1 * cpy - gammk * cqx;
+    const double c51 = -(2.0 * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+    const double c53 = -(gammk * gamm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gamm1 * gm1sq * wy) * rho;
+    const double tt = -2.0 * wvno2;
+    const double c31 = tt * c53, c32 = tt * c43, c33 = a0 + 2.0 * (cpcq - c11), c34 = tt * c23, c35 = tt * c13;
+    // ee(i) = sum_j e(j) ca(j,i); ca rows: 1:(c11..c15) 2:(c21,c22,c23,c24,c14)
+    // 3:(c31..c35) 4:(c41,c42,c43,c22,c12) 5:(c51,c41,c53,c21,c11)
+    double f0 = e0 * c11 + e1 * c21 + e2 * c31 + e3 * c41 + e4 * c51;
+    double f1 = e0 * c12 + e1 * c22 + e2 * c32 + e3 * c42 + e4 * c41;
+    double f2 = e0 * c13 + e1 * c23 + e2 * c33 + e3 * c43 + e4 * c53;
+    double f3 = e0 * c14 + e1 * c24 + e2 * c34 + e3 * c22 + e4 * c21;
+    double f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
+    // normc (surfdisp96.f:1022-1047): divide by the largest magnitude
+    double t1 = fmax(fmax(fmax(fabs(f0), fabs(f1)), fmax(fabs(f2), fabs(f3))), fabs(f4));
+    if (t1 < 1.e-40) t1 = 1.0;
+    const double it1 = 1.0 / t1;
+    e0 = f0 * it1; e1 = f1 * it1; e2 = f2 * it1; e3 = f3 * it1; e4 = f4 * it1;
+  }
+  if (V.llw != 1) {
+    float4 ly = V.get(0);
+    const double a0l = ly.y, dpth = ly.x, rho = ly.w;
+    xka = omega / a0l;
+    ra = sqrt((wvno + xka) * fabs(wvno - xka));
+    const double p = ra * dpth;
+    double w, cosp;
+    if (wvno < xka) {
+      double sp, cp;
+      sincos(p, &sp, &cp);
+      w = sp / ra; cosp = cp;
+    } else if (wvno == xka) {
+      cosp = 1.0; w = dpth;
+    } else {
+      double fac = (p < 16.0) ? exp(-2.0 * p) : 0.0;
+      cosp = (1.0 + fac) * 0.5;
+      w = ((1.0 - fac) * 0.5) / ra;
+    }
+    const double w0 = -rho * w;
+    return cosp * e0 + w0 * e1;
+  }
+  return e0;
+}
+
+// dltar1 (surfdisp96.f:734-794)
+SWDK_HDI double dltar1(const LayerView& V, double wvno, double omega) {
+  float4 h = V.get(V.L - 1);
+  double beta1 = h.z, rho1 = h.w;
+  double xkb = omega / beta1;
+  double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+  double e1 = rho1 * rb;
+  double e2 = 1.0 / (beta1 * beta1);
+  for (int m = V.L - 2; m >= V.llw - 1; --m) {
+    float4 ly = V.get(m);
+    beta1 = ly.z;
+    rho1 = ly.w;
+    const double dpth = ly.x;
+    const double xmu = rho1 * beta1 * beta1;
+    xkb = omega / beta1;
+    rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    const double q = dpth * rb;
+    double cosq, y, z;
+    if (wvno < xkb) {
+      double sq, cq;
+      sincos(q, &sq, &cq);
+      y = sq / rb; z = -rb * sq; cosq = cq;
+    } else if (wvno == xkb) {
+      cosq = 1.0; y = dpth; z = 0.0;
+    } else {
+      double fac = (q < 16.0) ? exp(-2.0 * q) : 0.0;
+      cosq = (1.0 + fac) * 0.5;
+      double sq = (1.0 - fac) * 0.5;
+      y = sq / rb; z = rb * sq;
+    }
+    const double e10 = e1 * cosq + e2 * xmu * z;
+    const double e20 = e1 * y / xmu + e2 * cosq;
+    double xnor = fmax(fabs(e10), fabs(e20));
+    if (xnor < 1.e-40) xnor = 1.0;
+    const double ix = 1.0 / xnor;
+    e1 = e10 * ix;
+    e2 = e20 * ix;
+  }
+  return e1;
+}
+
+SWDK_HD double secular(const LayerView& V, int iwave, double wvno, double omega) {
+  return (iwave == 1) ? dltar1(V, wvno, omega) : dltar4(V, wvno, omega);
+}
+
+// ---------------------------------------------------------------------------
+// surfdisp96 period/mode continuation as a flat state machine.  Each call of
+// chain_advance() runs control logic until it needs one secular-function
+// value (returns true with s.creq set) or the chain is finished (false).
+// ---------------------------------------------------------------------------
+enum Phase : int {
+  PH_CHAIN_START, PH_PERIOD_START, PH_GS_START, PH_GS_FIRST, PH_SCAN, PH_SCAN_GOT, PH_REFINE_START,
+  PH_NEV_A, PH_NEV_TOP, PH_NEV_BODY_GOT, PH_NEV_BODY, PH_NEV_HALF_GOT, PH_NEV_NEV_GOT, PH_BRENT_STEP,
+  PH_BRENT_GOT, PH_REFINE_DONE, PH_GS_OK, PH_GS_FAIL, PH_PERIOD_OUT, PH_FAIL, PH_MODE_END, PH_CHAIN_END,
+  PH_RETRY_NEXT, PH_DONE
+};
+
+struct ChainParams {
+  const double* t;  // periods of the chain
+  int kmax;         // periods
+  int nmode;        // modes 1..nmode (surfdisp96 "mode")
+  int igr;          // 0 phase; >0 numerical group velocity (surfdisp96.f:241-248)
+  int iwave;        // 1 Love, 2 Rayleigh
+  int refine;       // 0 reference nevill, 1 Brent
+  double rtol;      // Brent bracket tolerance (relative)
+  int sngl;         // REAL*4 output like the reference
+  double cc;        // start value 0.95*0.90*c_R(slowest layer), surfdisp96.f:206-226
+  float betmx;      // largest shear velocity of the flattened model
+  int retry;        // 1: surfdisp()'s single-period retry (surfdisp.cpp:94-109)
+};
+
+struct ChainState {
+  int phase, next;
+  double last;    // value of the last requested secular evaluation
+  double creq;    // requested phase velocity
+  double omega;   // 2 pi / t1 of the current root
+  // surfdisp96 locals
+  int iq, k, ift, ierr;
+  double t1;
+  float t1a, t1b;
+  double c1, c2, clow, cm, del1, del2, del1st;
+  int ifirst, idir, gpass;
+  // refinement
+  double c3, del3, ra_, fa, rb_, fb, rc_, fc, rd, re;
+  int nev, nctrl, m;
+  int nscan;
+  // retries
+  int sub, rq_m, rq_k, sub_ierr;
+  double sub_out;
+  int iterlim;
+  long long nevals;
+};
+
+// Output callback: slot (mode iq, period k) gets value v; the caller owns
+// storage.  out(mode-1, k-1) addressing is done by the kernel.
+struct ChainIO {
+  double* c;    // [KMAX_CHAIN] continuation array (surfdisp96 c())
+  double* cb;   // [KMAX_CHAIN] group continuation (surfdisp96 cb())
+  double* out;  // out[(iq-1)*stride + (k-1)*ostride]
+  int stride, ostride;
+  int32_t* st;  // status, same addressing as out
+};
+
+constexpr double ONE_DC = 1.0e-2;  // surfdisp96 "one"
+constexpr double ONEA = 1.5;       // dble(sone0)
+constexpr double DC = (double)0.005f;
+constexpr float HGR = 0.005f;
+constexpr int SCAN_CAP = 20000;    // guard against non-finite inputs (legit scans need < 2000)
+
+SWDK_HD double& out_at(const ChainIO& io, int iq, int k) {
+  return io.out[(size_t)(iq - 1) * io.stride + (size_t)(k - 1) * io.ostride];
+}
+SWDK_HD int32_t& st_at(const ChainIO& io, int iq, int k) {
+  return io.st[(size_t)(iq - 1) * io.stride + (size_t)(k - 1) * io.ostride];
+}
+
+SWDK_HD void chain_init(ChainState& s) {
+  s.phase = PH_CHAIN_START;
+  s.sub = 0;
+  s.iterlim = 0;
+  s.nevals = 0;
+  s.last = 0.0;
+  s.del1st = 0.0;
+}
+
+// request a secular-function value at c; continue with phase nxt
+#define SWDK_REQ(cv, nxt) do { s.creq = (cv); s.next = (nxt); return true; } while (0)
+
+SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& io) {
+  for (;;) {
+    // parameters of the active chain: the main chain or a single-period retry
+    const double* tp = s.sub ? (P.t + (s.rq_k - 1)) : P.t;
+    const int kmax = s.sub ? 1 : P.kmax;
+    const int nmode = s.sub ? s.rq_m : P.nmode;
+    switch (s.phase) {
+      case PH_CHAIN_START: {
+        s.ift = 999;
+        s.ierr = 0;
+        s.iq = 1;
+        s.k = 1;
+        s.cm = P.cc;
+        s.c1 = P.cc;
+        s.clow = P.cc;
+        for (int i = 0; i < kmax; ++i) { io.c[i] = 0.0; io.cb[i] = 0.0; }
+        s.phase = PH_PERIOD_START;
+        break;
+      }
+      case PH_PERIOD_START: {
+        if (s.k > kmax) { s.phase = PH_MODE_END; break; }
+        if (s.k >= s.ift) { s.phase = PH_FAIL; break; }
+        double t1 = tp[s.k - 1];
+        if (P.igr > 0) {
+          s.t1a = (float)(t1 / (double)(1.0f + HGR));
+          s.t1b = (float)(t1 / (double)(1.0f - HGR));
+          t1 = (double)s.t1a;
+        } else {
+          s.t1a = (float)t1;
+        }
+        s.t1 = t1;
+        const int k = s.k, iq = s.iq;
+        if (k == 1 && iq == 1) { s.c1 = P.cc; s.clow = P.cc; s.ifirst = 1; }
+        else if (k == 1 && iq > 1) { s.c1 = io.c[0] + ONE_DC * DC; s.clow = s.c1; s.ifirst = 1; }
+        else if (k > 1 && iq > 1) {
+          s.ifirst = 0;
+          s.clow = io.c[k - 1] + ONE_DC * DC;
+          s.c1 = io.c[k - 2];
+          if (s.c1 < s.clow) s.c1 = s.clow;
+        } else {
+          s.ifirst = 0;
+          s.c1 = io.c[k - 2] - ONEA * DC;
+          s.clow = s.cm;
+        }
+        s.gpass = 0;
+        s.phase = PH_GS_START;
+        break;
+      }
+      case PH_GS_START: {  // getsol entry (surfdisp96.f:439-451)
+        s.omega = TWOPI / s.t1;
+        s.nscan = 0;
+        SWDK_REQ(s.c1, PH_GS_FIRST);
+      }
+      case PH_GS_FIRST: {
+        s.del1 = s.last;
+        if (s.ifirst == 1) s.del1st = s.del1;
+        const double plmn = dsign1(s.del1st) * dsign1(s.del1);
+        if (s.ifirst == 1) s.idir = 1;
+        else if (plmn >= 0.0) s.idir = 1;
+        else s.idir = -1;
+        s.phase = PH_SCAN;
+        break;
+      }
+      case PH_SCAN: {  // label 1000
+        s.c2 = (s.idir > 0) ? s.c1 + DC : s.c1 - DC;
+        if (s.c2 <= s.clow) { s.idir = 1; s.c1 = s.clow; break; }
+        if (++s.nscan > SCAN_CAP) { s.phase = PH_GS_FAIL; break; }
+        SWDK_REQ(s.c2, PH_SCAN_GOT);
+      }
+      case PH_SCAN_GOT: {
+        s.del2 = s.last;
+        if (dsign1(s.del1) != dsign1(s.del2)) { s.phase = PH_REFINE_START; break; }
+        s.c1 = s.c2;
+        s.del1 = s.del2;
+        if (s.c1 < s.cm || s.c1 >= ((double)P.betmx + DC) || !(s.c1 == s.c1)) { s.phase = PH_GS_FAIL; break; }
+        s.phase = PH_SCAN;
+        break;
+      }
+      case PH_REFINE_START: {
+        if (P.refine == 0) {
+          s.c3 = 0.5 * (s.c1 + s.c2);
+          SWDK_REQ(s.c3, PH_NEV_A);
+        }
+        s.ra_ = s.c1; s.fa = s.del1; s.rb_ = s.c2; s.fb = s.del2;
+        s.rc_ = s.ra_; s.fc = s.fa; s.rd = s.rb_ - s.ra_; s.re = s.rd;
+        s.nctrl = 0;
+        s.phase = PH_BRENT_STEP;
+        break;
+      }
+      // ---- nevill (surfdisp96.f:575-694), bracket kept in c1/c2 ----
+      case PH_NEV_A: {
+        s.del3 = s.last;
+        s.nev = 1; s.nctrl = 1; s.m = 1;
+        s.phase = PH_NEV_TOP;
+        break;
+      }
+      case PH_NEV_TOP: {
+        s.nctrl = s.nctrl + 1;
+        if (s.nctrl >= 100) { s.iterlim++; s.phase = PH_REFINE_DONE; break; }
+        if (s.c3 < fmin(s.c1, s.c2) || s.c3 > fmax(s.c1, s.c2)) {
+          s.nev = 0;
+          s.c3 = 0.5 * (s.c1 + s.c2);
+          SWDK_REQ(s.c3, PH_NEV_BODY_GOT);
+        }
+        s.phase = PH_NEV_BODY;
+        break;
+      }
+      case PH_NEV_BODY_GOT: {
+        s.del3 = s.last;
+        s.phase = PH_NEV_BODY;
+        break;
+      }
+      case PH_NEV_BODY: {
+        const double s13 = s.del1 - s.del3;
+        const double s32 = s.del3 - s.del2;
+        if (dsign1(s.del3) * dsign1(s.del1) < 0.0) { s.c2 = s.c3; s.del2 = s.del3; }
+        else { s.c1 = s.c3; s.del1 = s.del3; }
+        if (fabs(s.c1 - s.c2) <= 1.e-6 * s.c1) { s.phase = PH_REFINE_DONE; break; }
+        if (dsign1(s13) != dsign1(s32)) s.nev = 0;
+        const double ss1 = fabs(s.del1), s1 = (double)0.01f * ss1;
+        const double ss2 = fabs(s.del2), s2 = (double)0.01f * ss2;
+        if (s1 > ss2 || s2 > ss1 || s.nev == 0) {
+          s.c3 = 0.5 * (s.c1 + s.c2);
+          SWDK_REQ(s.c3, PH_NEV_HALF_GOT);
+        }
+        // Neville on x(y) (surfdisp96.f:654-682); x/y held in io.cb tail
+        double* x = io.cb + KMAX_CHAIN;
+        double* y = x + 12;
+        int m = s.m;
+        if (s.nev == 2) { x[m] = s.c3; y[m] = s.del3; }
+        else { x[0] = s.c1; y[0] = s.del1; x[1] = s.c2; y[1] = s.del2; m = 1; }
+        s.m = m;
+        bool bad = false;
+        for (int kk = 1; kk <= m; ++kk) {
+          const int j = m - kk + 1;
+          const double denom = y[m] - y[j - 1];
+          if (fabs(denom) < 1.0e-10 * fabs(y[m])) { bad = true; break; }
+          x[j - 1] = (-y[j - 1] * x[j] + y[m] * x[j - 1]) / denom;
+        }
+        if (bad) {
+          s.c3 = 0.5 * (s.c1 + s.c2);
+          SWDK_REQ(s.c3, PH_NEV_HALF_GOT);
+        }
+        s.c3 = x[0];
+        SWDK_REQ(s.c3, PH_NEV_NEV_GOT);
+      }
+      case PH_NEV_HALF_GOT: {
+        s.del3 = s.last;
+        s.nev = 1; s.m = 1;
+        s.phase = PH_NEV_TOP;
+        break;
+      }
+      case PH_NEV_NEV_GOT: {
+        s.del3 = s.last;
+        s.nev = 2;
+        s.m = s.m + 1;
+        if (s.m > 10) s.m = 10;
+        s.phase = PH_NEV_TOP;
+        break;
+      }
+      // ---- tight refinement: Brent's zeroin on the scan bracket ----
+      case PH_BRENT_STEP: {
+        if (signbit(s.fb) == signbit(s.fc)) { s.rc_ = s.ra_; s.fc = s.fa; s.rd = s.rb_ - s.ra_; s.re = s.rd; }
+        if (fabs(s.fc) < fabs(s.fb)) {
+          s.ra_ = s.rb_; s.rb_ = s.rc_; s.rc_ = s.ra_;
+          s.fa = s.fb; s.fb = s.fc; s.fc = s.fa;
+        }
+        const double eps = 2.220446049250313e-16;
+        const double tol1 = 2.0 * eps * fabs(s.rb_) + 0.5 * P.rtol * fabs(s.rb_);
+        const double xm = 0.5 * (s.rc_ - s.rb_);
+        if (fabs(xm) <= tol1 || s.fb == 0.0) { s.c3 = s.rb_; s.phase = PH_REFINE_DONE; break; }
+        if (++s.nctrl > 200) { s.iterlim++; s.c3 = s.rb_; s.phase = PH_REFINE_DONE; break; }
+        if (fabs(s.re) >= tol1 && fabs(s.fa) > fabs(s.fb)) {
+          const double sr = s.fb / s.fa;
+          double p, q;
+          if (s.ra_ == s.rc_) { p = 2.0 * xm * sr; q = 1.0 - sr; }
+          else {
+            const double qq = s.fa / s.fc, r = s.fb / s.fc;
+            p = sr * (2.0 * xm * qq * (qq - r) - (s.rb_ - s.ra_) * (r - 1.0));
+            q = (qq - 1.0) * (r - 1.0) * (sr - 1.0);
+          }
+          if (p > 0.0) q = -q;
+          p = fabs(p);
+          if (2.0 * p < fmin(3.0 * xm * q - fabs(tol1 * q), fabs(s.re * q))) { s.re = s.rd; s.rd = p / q; }
+          else { s.rd = xm; s.re = s.rd; }
+        } else { s.rd = xm; s.re = s.rd; }
+        s.ra_ = s.rb_; s.fa = s.fb;
+        if (fabs(s.rd) > tol1) s.rb_ = s.rb_ + s.rd;
+        else s.rb_ = s.rb_ + copysign(tol1, xm);
+        SWDK_REQ(s.rb_, PH_BRENT_GOT);
+      }
+      case PH_BRENT_GOT: {
+        s.fb = s.last;
+        s.phase = PH_BRENT_STEP;
+        break;
+      }
+      case PH_REFINE_DONE: {  // getsol tail (surfdisp96.f:487-491)
+        s.c1 = s.c3;
+        if (s.c1 > (double)P.betmx || !(s.c1 == s.c1)) { s.phase = PH_GS_FAIL; break; }
+        s.phase = PH_GS_OK;
+        break;
+      }
+      case PH_GS_OK: {
+        if (s.gpass == 0) {
+          io.c[s.k - 1] = s.c1;
+          if (P.igr > 0) {
+            s.t1 = (double)s.t1b;
+            s.ifirst = 0;
+            s.clow = io.cb[s.k - 1] + ONE_DC * DC;
+            s.c1 = s.c1 - ONEA * DC;
+            s.gpass = 1;
+            s.phase = PH_GS_START;
+            break;
+          }
+          s.c1 = 0.0;
+        } else {
+          io.cb[s.k - 1] = s.c1;
+        }
+        s.phase = PH_PERIOD_OUT;
+        break;
+      }
+      case PH_GS_FAIL: {
+        if (s.gpass == 0) { s.phase = PH_FAIL; break; }
+        s.c1 = io.c[s.k - 1];
+        io.cb[s.k - 1] = s.c1;
+        s.phase = PH_PERIOD_OUT;
+        break;
+      }
+      case PH_PERIOD_OUT: {  // surfdisp96.f:307-319
+        const double ck = io.c[s.k - 1];
+        double v;
+        if (P.sngl) {
+          const float cc0 = (float)ck, cc1 = (float)s.c1;
+          if (P.igr == 0) v = (double)cc0;
+          else v = (double)((1.0f / s.t1a - 1.0f / s.t1b) / (1.0f / (s.t1a * cc0) - 1.0f / (s.t1b * cc1)));
+        } else {
+          if (P.igr == 0) v = ck;
+          else {
+            const double ta = s.t1a, tb = s.t1b;
+            v = (1.0 / ta - 1.0 / tb) / (1.0 / (ta * ck) - 1.0 / (tb * s.c1));
+          }
+        }
+        if (s.sub) { if (s.iq == nmode) s.sub_out = v; }
+        else { out_at(io, s.iq, s.k) = v; st_at(io, s.iq, s.k) = ST_OK; }
+        s.k = s.k + 1;
+        s.phase = PH_PERIOD_START;
+        break;
+      }
+      case PH_FAIL: {  // labels 1700/1750
+        if (s.iq <= 1) s.ierr = 1;
+        s.ift = s.k;
+        if (s.sub) { if (s.iq == nmode) s.sub_out = 0.0; }
+        else for (int i = s.k; i <= kmax; ++i) { out_at(io, s.iq, i) = 0.0; st_at(io, s.iq, i) = ST_NO_ROOT; }
+        s.phase = PH_MODE_END;
+        break;
+      }
+      case PH_MODE_END: {
+        s.iq = s.iq + 1;
+        s.k = 1;
+        s.phase = (s.iq > nmode) ? PH_CHAIN_END : PH_PERIOD_START;
+        break;
+      }
+      case PH_CHAIN_END: {
+        if (s.sub) {  // a single-period retry finished (surfdisp.cpp:97-108)
+          const double v = s.sub_out;
+          const bool ok = (s.ierr == 0) && v != 0.0 && (v == v);
+          out_at(io, s.rq_m, s.rq_k) = ok ? v : 0.0;
+          st_at(io, s.rq_m, s.rq_k) = ok ? ST_RETRIED : ST_NO_ROOT;
+          s.rq_k = s.rq_k + 1;
+          s.phase = PH_RETRY_NEXT;
+          break;
+        }
+        if (s.ierr == 0 || !P.retry) { s.phase = PH_DONE; break; }
+        s.rq_m = 1; s.rq_k = 1;
+        s.phase = PH_RETRY_NEXT;
+        break;
+      }
+      case PH_RETRY_NEXT: {
+        s.sub = 0;
+        bool found = false;
+        while (s.rq_m <= P.nmode && !found) {
+          while (s.rq_k <= P.kmax) {
+            const double v = out_at(io, s.rq_m, s.rq_k);
+            if (v == 0.0 || !(v == v)) { found = true; break; }
+            s.rq_k++;
+          }
+          if (!found) { s.rq_m++; s.rq_k = 1; }
+        }
+        if (!found) { s.phase = PH_DONE; break; }
+        s.sub = 1;
+        s.phase = PH_CHAIN_START;
+        break;
+      }
+      case PH_DONE:
+      default:
+        return false;
+    }
+  }
+}
+#undef SWDK_REQ
+
+// Runs a whole chain.  io.cb must have KMAX_CHAIN + 24 doubles (Neville x/y).
+// On the device every lane of the warp must call this (active = false for
+// lanes without a chain): a full-warp vote at the top of each iteration
+// reconverges the warp so that the secular function -- nearly all of the
+// work -- runs once for all lanes that need a value, instead of once per
+// divergent group of lanes.
+SWDK_HDI void run_chain(const LayerView& V, const ChainParams& P, const ChainIO& io, ChainState& s, bool active) {
+  chain_init(s);
+#ifdef __CUDA_ARCH__
+  for (;;) {
+    const bool need = active && chain_advance(s, P, io);
+    if (!need) active = false;
+    if (__ballot_sync(0xffffffffu, need) == 0u) break;
+    if (need) {
+      s.last = secular(V, P.iwave, s.omega / s.creq, s.omega);
+      s.nevals++;
+      s.phase = s.next;
+    }
+  }
+#else
+  if (!active) return;
+  while (chain_advance(s, P, io)) {
+    s.last = secular(V, P.iwave, s.omega / s.creq, s.omega);
+    s.nevals++;
+    s.phase = s.next;
+  }
+#endif
+}
+
+}  // namespace swdk

@@ -54,6 +54,10 @@
 //   * Columns with nw>=2 leading fluid nodes (vs==0) are merged into one
 //     homogeneous fluid layer (surfdisp96 supports exactly one, llw=2); the
 //     reference's grid2LayerModel handles only nw<=1 and the two agree there.
+//   * groupvel_l sets vp = 1.732*vs (surfdisp.cpp:139), which for a fluid top
+//     layer makes surfdisp96 start its scan at c = 0 (undefined); the layer's
+//     own vp is used instead.  For solid columns Love roots do not depend on
+//     vp, so the results are identical there.
 // ============================================================================
 #include <cmath>
 #include <cstdint>
@@ -1853,6 +1857,11 @@ void surfdisp_w(const float* thk, const float* vp, const float* vs, const float*
       }
     }
   }
+  // higher-mode periods beyond a mode's existence end as zeros without ierr
+  // (surfdisp96.f:322,358-364): no retry, marked NO_ROOT
+  if (status)
+    for (int i = 0; i < kmax; ++i)
+      if ((cg[i] == 0.0 || std::isnan(cg[i])) && status[i] == ST_OK) status[i] = ST_NO_ROOT;
   if (sphere && !keep_flat)
     for (int i = 0; i < kmax; ++i) cg[i] = flat2sphere(t[i], cg[i], wtype);
 }
@@ -1994,7 +2003,7 @@ void disp1d(const float* vs, const float* vp, const float* rho, const float* dep
         std::vector<double> cp(nt);
         std::vector<float> vpl(rmax);
         const float* VPu = VP;
-        if (w == 3) { for (int i = 0; i < rmax; ++i) vpl[i] = (float)(1.732 * VS[i]); VPu = vpl.data(); }
+        (void)vpl;  // groupvel_l's vp = 1.732 vs only matters for fluid layers (start value); the layer vp is used
         std::vector<int> sg(nt);
         surfdisp_w(TH, VPu, VS, RH, rmax, tt, cp.data(), nt, wp, mode, sphere, true, op.ro, nev, iterlim, sg.data());
         for (int i = 0; i < nt; ++i) {

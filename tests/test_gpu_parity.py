@@ -1,0 +1,183 @@
+"""GPU parity: libswdk through its C-ABI against the CPU oracle.
+
+Tolerances (stated by the task for floating point): phase/group velocity
+|dc|, |dU| <= 1e-6 km/s against the FP64 oracle in the tight refinement mode;
+kernels <= 1e-5 relative to the largest |kernel| of the slot.  In the
+reference-refinement mode (surfdisp96's own 1e-6*c stop) the same
+algorithm runs on both sides and the roots agree to 1e-6*c.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from jdsurfg_b200 import Engine, synth
+
+pytestmark = pytest.mark.gpu
+
+TOL_C = 1e-6
+TOL_K = 1e-5
+
+
+def _kernel_relerr(a, b):
+    scale = np.abs(b).max(axis=1, keepdims=True) + 1e-30
+    return (np.abs(a - b) / scale).max()
+
+
+def _layered_batch(n, L, seed, water=False):
+    rng = np.random.default_rng(seed)
+    thk = np.full((n, L), 0.6, np.float32)
+    thk[:, -1] = 0
+    base = np.linspace(2.4, 4.6, L)[None, :]
+    vs = (base * (1 + 0.04 * rng.standard_normal((n, L)))).astype(np.float32)
+    vp = (1.76 * vs).astype(np.float32)
+    rho = (0.32 * vp + 0.77).astype(np.float32)
+    if water:
+        vs[:, 0] = 0.0
+        vp[:, 0] = 1.5
+        rho[:, 0] = 1.03
+        thk[:, 0] = 1.0
+    return thk, vp, vs, rho
+
+
+@pytest.mark.parametrize("iwave", [1, 2])
+@pytest.mark.parametrize("refine", [0, 1])
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("water", [False, True])
+def test_surfdisp96_batch_matches_oracle(iwave, refine, mode, water):
+    thk, vp, vs, rho = _layered_batch(48, 57, seed=iwave * 10 + mode, water=water)
+    t = np.geomspace(1.5, 60.0, 17)
+    eng = Engine(refine=refine)
+    cg, ierr = eng.surfdisp96_batch(thk, vp, vs, rho, 1, iwave, mode, 0, t)
+    for m in range(len(thk)):
+        ref, rerr, _ = O.surfdisp96(thk[m], vp[m], vs[m], rho[m], 1, iwave, mode, 0, t, refine=refine, rtol=1e-10)
+        assert ierr[m] == rerr
+        tol = TOL_C if refine == 1 else 1e-6 * ref.max()
+        assert np.abs(cg[m] - ref).max() <= tol, (m, np.abs(cg[m] - ref).max())
+
+
+def test_surfdisp96_batch_group_igr():
+    thk, vp, vs, rho = _layered_batch(16, 41, seed=5)
+    t = np.geomspace(2.0, 40.0, 9)
+    eng = Engine(refine=1)
+    for iwave in (1, 2):
+        cg, ierr = eng.surfdisp96_batch(thk, vp, vs, rho, 1, iwave, 1, 1, t)
+        for m in range(len(thk)):
+            ref, rerr, _ = O.surfdisp96(thk[m], vp[m], vs[m], rho[m], 1, iwave, 1, 1, t, refine=1, rtol=1e-10)
+            # REAL*4 group-velocity formula of surfdisp96.f:315 on equal REAL*4 roots
+            assert np.abs(cg[m] - ref).max() <= 1e-4, np.abs(cg[m] - ref).max()
+
+
+@pytest.mark.parametrize("refine", [0, 1])
+def test_get_1d_kernel_tiny(refine):
+    case = synth.make_config("tiny", seed=7)
+    eng = Engine(refine=refine)
+    r = eng.run_case(case)
+    ref = O.get_1d_kernel(case, refine=refine)
+    np.testing.assert_array_equal(r["status"], ref["status"])
+    tol = TOL_C if refine == 1 else 1e-6 * 5.0
+    assert np.abs(r["vc"] - ref["vc"]).max() <= tol
+    assert np.abs(r["vout"] - ref["vout"]).max() <= tol
+    assert _kernel_relerr(r["kernel"], ref["kernel"]) <= (TOL_K if refine == 1 else 1e-3)
+
+
+def test_get_1d_kernel_golden_fixture():
+    """Against the committed oracle outputs (tests/golden) for the tiny case."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_golden.npz"))
+    case = synth.make_config("tiny", seed=7)
+    r = Engine(refine=1).run_case(case)
+    assert np.abs(r["vc"] - g["tiny_tight_vc"]).max() <= TOL_C
+    assert np.abs(r["vout"] - g["tiny_tight_vout"]).max() <= TOL_C
+    assert _kernel_relerr(r["kernel"], g["tiny_tight_kernel"]) <= TOL_K
+    np.testing.assert_array_equal(r["status"], g["tiny_tight_status"])
+
+
+def test_get_2d_map_tiny():
+    case = synth.make_config("tiny", seed=9)
+    eng = Engine(refine=1)
+    r = eng.run_case(case, path="map")
+    ref = O.get_2d_map(case, refine=1)
+    np.testing.assert_array_equal(r["status"], ref["status"])
+    assert np.abs(r["vc"] - ref["vc"]).max() <= TOL_C
+    assert np.abs(r["vout"] - ref["vout"]).max() <= TOL_C
+
+
+@pytest.mark.parametrize("name,ncols", [("small", 48), ("production", 40)])
+def test_get_1d_kernel_configs_subset(name, ncols):
+    """Seeded columns of the benchmark configurations: LVZ, fluid nodes,
+    higher modes, phase and group slots."""
+    case = synth.make_config(name)
+    ncol = case["nx"] * case["ny"]
+    rng = np.random.default_rng(0)
+    cols = rng.choice(ncol, ncols, replace=False)
+    if case["vp"] is not None:  # make sure fluid columns are exercised
+        wat = np.nonzero(case["vs"][0] == 0)[0]
+        cols = np.unique(np.concatenate([cols, wat[:8]]))
+    sub = synth.subset_columns(case, cols)
+    eng = Engine(refine=1)
+    r = eng.run_case(sub)
+    ref = O.get_1d_kernel(sub, refine=1)
+    np.testing.assert_array_equal(r["status"], ref["status"])
+    assert np.abs(r["vc"] - ref["vc"]).max() <= TOL_C
+    assert np.abs(r["vout"] - ref["vout"]).max() <= TOL_C
+    assert _kernel_relerr(r["kernel"], ref["kernel"]) <= TOL_K
+
+
+def test_model_txt_reference_kernels():
+    """The reference's test/swd model (41 nodes) at periods 4..40 s: GPU node
+    kernels (through get_1d_kernel with explicit vp/rho) against the oracle's
+    kernel1D + chain rule."""
+    z, vs, vp, rho = O.load_swd_model()
+    t = 4.0 + 2.0 * np.arange(19)
+    tables = [t[:, None]] * 4
+    case = dict(nx=1, ny=1, nz=len(z), depth=z, vs=vs[:, None].copy(), vp=vp[:, None].copy(),
+                rho=rho[:, None].copy(), tables=tables)
+    eng = Engine(refine=1)
+    r = eng.run_case(case)
+    ref = O.get_1d_kernel(case, refine=1)
+    assert np.abs(r["vc"] - ref["vc"]).max() <= TOL_C
+    assert np.abs(r["vout"] - ref["vout"]).max() <= TOL_C
+    assert _kernel_relerr(r["kernel"], ref["kernel"]) <= TOL_K
+
+
+def test_nan_and_invalid_columns_flagged():
+    case = synth.make_config("tiny", seed=3)
+    vs = case["vs"].copy()
+    vs[3, 1] = np.nan
+    vs[5, 4] = -1.0
+    case["vs"] = vs
+    r = Engine().run_case(case)
+    assert (r["status"][:, 1] == 3).all() and (r["status"][:, 4] == 3).all()
+    assert (r["vc"][:, 1] == 0).all()
+    good = [c for c in range(vs.shape[1]) if c not in (1, 4)]
+    assert (r["status"][:, good] == 0).all()
+
+
+def test_frechet_rows_match_oracle():
+    import torch
+    case = synth.make_config("tiny", seed=5, nx=6, ny=5)
+    eng = Engine(refine=1)
+    r = eng.run_case(case)
+    nx, ny, nz = case["nx"], case["ny"], case["nz"]
+    kmax = r["kernel"].shape[0]
+    rng = np.random.default_rng(1)
+    nrows = 7
+    slot = rng.integers(0, kmax, nrows).astype(np.int32)
+    fdm = (rng.standard_normal((nrows, ny, nx)) * (rng.random((nrows, ny, nx)) < 0.4)).astype(np.float32)
+    rows = O.frechet_rows(nx, ny, nz, r["kernel"], slot, fdm.reshape(nrows, -1))
+    n = (nx - 2) * (ny - 2) * (nz - 1)
+    dev = torch.device("cuda")
+    dk = torch.from_numpy(r["kernel"]).to(dev)
+    ds = torch.from_numpy(slot).to(dev)
+    df = torch.from_numpy(fdm.reshape(nrows, -1)).to(dev)
+    nnz = torch.zeros(nrows, dtype=torch.int32, device=dev)
+    idx = torch.zeros(nrows * n, dtype=torch.int32, device=dev)
+    val = torch.zeros(nrows * n, dtype=torch.float32, device=dev)
+    eng.frechet_rows_device(nx, ny, nz, kmax, dk, ds, df, nnz, idx, val)
+    torch.cuda.synchronize()
+    nnz, idx, val = nnz.cpu().numpy(), idx.cpu().numpy(), val.cpu().numpy()
+    for rr in range(nrows):
+        ri, rv = rows[rr]
+        assert nnz[rr] == len(ri)
+        np.testing.assert_array_equal(idx[rr * n:rr * n + nnz[rr]], ri)
+        np.testing.assert_array_equal(val[rr * n:rr * n + nnz[rr]], rv)
