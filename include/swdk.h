@@ -149,6 +149,38 @@ int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, co
                              const int32_t* d_row_slot, const float* d_fdm, int32_t* d_nnz, int32_t* d_indices,
                              float* d_values, void* stream);
 
+/* surfdisp96_ for callers that cannot allocate device memory.
+ *
+ * No counterpart in the reference: it is swdk_surfdisp96_batch on device
+ * pointers with no context and no allocation of any kind.  It is for host
+ * programs that own every byte of device memory themselves -- an inversion
+ * driver with a fixed, pre-reserved memory budget, or a framework whose
+ * allocator must stay the only one -- and so cannot let a library call
+ * cudaMalloc (or cudaFree, which also waits for the whole device) while an
+ * iteration is running.
+ *
+ * Inputs/outputs are the caller's DEVICE memory on `device`: thk/vp/vs/rho
+ * are (nlayer, nmodel) column-major floats, t has kmax doubles, cg receives
+ * (kmax, nmodel) doubles (model m's periods contiguous) and ierr nmodel ints,
+ * with surfdisp96's meaning; refine/rtol/sngl as in swdk_config.  The work is
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
+ *
+ * Scratch: a file-scope __device__ array of SWDK_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until the process exits.  A call needs
+ * 32*nlayer*nmodel + 12*mode*kmax*nmodel bytes (plus alignment and 32 bytes
+ * per model); larger calls return SWDK_E_LIMIT and do nothing.  The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current, so make that first call
+ * before any stream capture.  All calls on one device share the array and
+ * it keeps the last call's contents: calls whose GPU work overlaps (other
+ * streams, other host threads) race and corrupt each other's results, so
+ * serialise them.  The previously current device is restored on return. */
+#define SWDK_NOALLOC_SCRATCH_BYTES (64u << 20)
+int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_thk, const float* d_vp,
+                            const float* d_vs, const float* d_rho, int iflsph, int iwave, int mode, int igr, int kmax,
+                            const double* d_t, double* d_cg, int32_t* d_ierr, int refine, double rtol, int sngl,
+                            void* stream);
+
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -273,16 +274,14 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
 // ---------------------------------------------------------------------------
 // k_roots: one thread per (column, chain)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __restrict__ chains,
-                                               const double* __restrict__ periods, const float4* __restrict__ layR,
-                                               const float4* __restrict__ layL, const ColInfo* __restrict__ info,
-                                               int refine, double rtol, int sngl, int retry, double* __restrict__ croot,
-                                               int32_t* __restrict__ cstat, int32_t* __restrict__ ierr_out,
-                                               unsigned long long* __restrict__ nevals) {
+__device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const double* __restrict__ periods,
+                                           const float4* __restrict__ layR, const float4* __restrict__ layL,
+                                           const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
+                                           int retry, double* __restrict__ croot, int32_t* __restrict__ cstat,
+                                           int32_t* __restrict__ ierr_out, unsigned long long* __restrict__ nevals) {
   // nevals[0]: evaluations, nevals[1]: Rayleigh layer-evaluations,
   // nevals[2]: Love layer-evaluations
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  const ChainDesc cd = chains[blockIdx.y];
   unsigned long long my_evals = 0;
   // every lane runs run_chain (its warp vote needs the full warp); lanes
   // past the last column or with an invalid model take part inactive
@@ -339,10 +338,39 @@ __global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __rest
     my_evals += __shfl_down_sync(0xffffffffu, my_evals, o);
     my_layers += __shfl_down_sync(0xffffffffu, my_layers, o);
   }
-  if ((threadIdx.x & 31) == 0 && my_evals) {
+  if ((threadIdx.x & 31) == 0 && my_evals && nevals) {
     atomicAdd(nevals, my_evals);
     atomicAdd(nevals + (cd.iwave == 2 ? 1 : 2), my_layers);
   }
+}
+
+// one thread per (column, chain); chain = blockIdx.y
+__global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __restrict__ chains,
+                                               const double* __restrict__ periods, const float4* __restrict__ layR,
+                                               const float4* __restrict__ layL, const ColInfo* __restrict__ info,
+                                               int refine, double rtol, int sngl, int retry, double* __restrict__ croot,
+                                               int32_t* __restrict__ cstat, int32_t* __restrict__ ierr_out,
+                                               unsigned long long* __restrict__ nevals) {
+  roots_body(chains[blockIdx.y], ncol, periods, layR, layL, info, refine, rtol, sngl, retry, croot, cstat, ierr_out,
+             nevals);
+}
+
+// the same for one chain passed by value
+__global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const double* __restrict__ periods,
+                                                   const float4* __restrict__ layR, const float4* __restrict__ layL,
+                                                   const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
+                                                   double* __restrict__ croot, int32_t* __restrict__ cstat,
+                                                   int32_t* __restrict__ ierr_out) {
+  roots_body(cd, ncol, periods, layR, layL, info, refine, rtol, sngl, 0, croot, cstat, ierr_out, nullptr);
+}
+
+// cg(k, m) of model m = last mode's roots (surfdisp96's cg), model-major
+__global__ void k_copy_last_mode(int nmodel, int kmax, int mode, const double* __restrict__ croot,
+                                 double* __restrict__ cg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nmodel * kmax) return;
+  const int m = i / kmax, k = i % kmax;
+  cg[i] = croot[((size_t)(mode - 1) * kmax + k) * nmodel + m];
 }
 
 // ---------------------------------------------------------------------------
@@ -882,6 +910,20 @@ int run_host(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* vs, c
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// surfdisp96_ over device-resident models with no device allocation: the
+// scratch (layer models, start values, roots of all modes) lives in this
+// file-scope array.  Every GPU that loads the library holds it until exit.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SWDK_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};  // device address of g_noalloc_scratch, per device ordinal
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // C-ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -1083,5 +1125,57 @@ int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out) {
 }
 
 const char* swdk_last_error(const swdk_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_thk, const float* d_vp,
+                            const float* d_vs, const float* d_rho, int iflsph, int iwave, int mode, int igr, int kmax,
+                            const double* d_t, double* d_cg, int32_t* d_ierr, int refine, double rtol, int sngl,
+                            void* stream) {
+  if (nmodel <= 0 || nlayer < 2 || kmax <= 0 || mode < 1 || (iwave != 1 && iwave != 2) || !d_thk || !d_vp ||
+      !d_vs || !d_rho || !d_t || !d_cg || !d_ierr || device < 0 || device >= 256)
+    return SWDK_E_ARG;
+  if (nlayer > SWDK_MAX_LAYERS || kmax > SWDK_MAX_PERIODS) return SWDK_E_LIMIT;
+  // scratch layout: layR | layL | info | croot | cstat, each 256-byte aligned
+  const size_t nm = (size_t)nmodel, nin = nm * nlayer, nroot = (size_t)mode * kmax * nm;
+  const size_t o_layR = 0;
+  const size_t o_layL = align256(o_layR + nin * sizeof(float4));
+  const size_t o_info = align256(o_layL + nin * sizeof(float4));
+  const size_t o_croot = align256(o_info + nm * sizeof(ColInfo));
+  const size_t o_cstat = align256(o_croot + nroot * sizeof(double));
+  const size_t need = align256(o_cstat + nroot * sizeof(int32_t));
+  if (need > SWDK_NOALLOC_SCRATCH_BYTES) return SWDK_E_LIMIT;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return SWDK_E_CUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return SWDK_E_CUDA;
+  int rc = SWDK_OK;
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) rc = SWDK_E_CUDA;
+      else g_noalloc_ptr[device] = p;
+    }
+    base = (unsigned char*)g_noalloc_ptr[device];
+  }
+  if (rc == SWDK_OK) {
+    cudaStream_t st = (cudaStream_t)stream;
+    float4* layR = (float4*)(base + o_layR);
+    float4* layL = (float4*)(base + o_layL);
+    ColInfo* info = (ColInfo*)(base + o_info);
+    double* croot = (double*)(base + o_croot);
+    int32_t* cstat = (int32_t*)(base + o_cstat);
+    ChainDesc cd;
+    cd.t_off = 0; cd.np = kmax; cd.nmode = mode; cd.iwave = iwave; cd.igr = igr; cd.out_off = 0;
+    k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_thk, d_vp, d_vs, d_rho, iflsph, layR, layL,
+                                                         info);
+    k_roots_one<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(cd, nmodel, d_t, layR, layL, info, refine,
+                                                               rtol > 0.0 ? rtol : 1e-10, sngl, croot, cstat, d_ierr);
+    const int n = nmodel * kmax;
+    k_copy_last_mode<<<(n + 255) / 256, 256, 0, st>>>(nmodel, kmax, mode, croot, d_cg);
+    if (cudaGetLastError() != cudaSuccess) rc = SWDK_E_CUDA;
+  }
+  if (prev != device) cudaSetDevice(prev);
+  return rc;
+}
 
 }  // extern "C"
