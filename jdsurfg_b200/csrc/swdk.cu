@@ -165,6 +165,24 @@ __device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, cons
 
 __device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
 
+// layer-major, bottom-aligned REAL*4 layers plus the FP64 reciprocals the
+// secular functions use (1/a, 1/b; 1/rho and 1/(rho b^2) per wave type)
+__device__ void write_layers(int L, int ncol, int col, const float* th, const float* a, const float* b,
+                             const float* rR, const float* rL, float4* layR, float4* layL, double2* rab,
+                             double2* rrmR, double2* rrmL) {
+  for (int m = 0; m < L; ++m) {
+    const size_t o = (size_t)(L - 1 - m) * ncol + col;
+    layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
+    layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
+    if (rab) {
+      const double bd = b[m];
+      rab[o] = make_double2(1.0 / (double)a[m], 1.0 / bd);
+      rrmR[o] = make_double2(1.0 / (double)rR[m], 1.0 / ((double)rR[m] * bd * bd));
+      rrmL[o] = make_double2(1.0 / (double)rL[m], 1.0 / ((double)rL[m] * bd * bd));
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // k_prep: node model -> layer models (one thread per column)
 // ---------------------------------------------------------------------------
@@ -172,8 +190,9 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
                                               const float* __restrict__ vp_in, const float* __restrict__ rho_in,
                                               const float* __restrict__ depth, int sphere, int Lmax,
                                               float4* __restrict__ layR, float4* __restrict__ layL,
-                                              float4* __restrict__ lay0, ColInfo* __restrict__ info,
-                                              float2* __restrict__ chainrule) {
+                                              double2* __restrict__ rab, double2* __restrict__ rrmR,
+                                              double2* __restrict__ rrmL, float4* __restrict__ lay0,
+                                              ColInfo* __restrict__ info, float2* __restrict__ chainrule) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   float v[NZMAX], vp[NZMAX], rho[NZMAX], dep[NZMAX];
@@ -237,18 +256,15 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
   ci.nw = nw;
   ci.valid = valid ? 1 : 0;
   sd96_setup(L, sphere, th, a, b, r, rR, rL, ci);
-  for (int m = 0; m < L; ++m) {
-    const size_t o = (size_t)(L - 1 - m) * ncol + col;
-    layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
-    layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
-  }
+  write_layers(L, ncol, col, th, a, b, rR, rL, layR, layL, rab, rrmR, rrmL);
   info[col] = ci;
 }
 
 // k_prep_layers: layered models (surfdisp96_ input) -> layer models
 __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ thk, const float* __restrict__ vp,
                               const float* __restrict__ vs, const float* __restrict__ rho, int sphere,
-                              float4* __restrict__ layR, float4* __restrict__ layL, ColInfo* __restrict__ info) {
+                              float4* __restrict__ layR, float4* __restrict__ layL, double2* __restrict__ rab,
+                              double2* __restrict__ rrmR, double2* __restrict__ rrmL, ColInfo* __restrict__ info) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= nmodel) return;
   float th[LMAX], a[LMAX], b[LMAX], r[LMAX], rR[LMAX], rL[LMAX];
@@ -263,11 +279,7 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
   ci.nw = (b[0] <= 0.0f) ? 1 : 0;
   ci.valid = valid ? 1 : 0;
   sd96_setup(nlayer, sphere, th, a, b, r, rR, rL, ci);
-  for (int m = 0; m < nlayer; ++m) {
-    const size_t o = (size_t)(nlayer - 1 - m) * nmodel + col;
-    layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
-    layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
-  }
+  write_layers(nlayer, nmodel, col, th, a, b, rR, rL, layR, layL, rab, rrmR, rrmL);
   info[col] = ci;
 }
 
@@ -276,6 +288,8 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const double* __restrict__ periods,
                                            const float4* __restrict__ layR, const float4* __restrict__ layL,
+                                           const double2* __restrict__ rab, const double2* __restrict__ rrmR,
+                                           const double2* __restrict__ rrmL,
                                            const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
                                            int retry, double* __restrict__ croot, int32_t* __restrict__ cstat,
                                            int32_t* __restrict__ ierr_out, unsigned long long* __restrict__ nevals) {
@@ -297,6 +311,8 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   }
   LayerView V;
   V.lay = (cd.iwave == 2) ? layR : layL;
+  V.rab = rab;
+  V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
   V.ncol = ncol;
   V.col = ccol;
   V.L = ci.L;
@@ -351,8 +367,8 @@ __global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __rest
                                                int refine, double rtol, int sngl, int retry, double* __restrict__ croot,
                                                int32_t* __restrict__ cstat, int32_t* __restrict__ ierr_out,
                                                unsigned long long* __restrict__ nevals) {
-  roots_body(chains[blockIdx.y], ncol, periods, layR, layL, info, refine, rtol, sngl, retry, croot, cstat, ierr_out,
-             nevals);
+  roots_body(chains[blockIdx.y], ncol, periods, layR, layL, nullptr, nullptr, nullptr, info, refine, rtol, sngl, retry,
+             croot, cstat, ierr_out, nevals);
 }
 
 // the same for one chain passed by value
@@ -361,7 +377,112 @@ __global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const
                                                    const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
                                                    double* __restrict__ croot, int32_t* __restrict__ cstat,
                                                    int32_t* __restrict__ ierr_out) {
-  roots_body(cd, ncol, periods, layR, layL, info, refine, rtol, sngl, 0, croot, cstat, ierr_out, nullptr);
+  roots_body(cd, ncol, periods, layR, layL, nullptr, nullptr, nullptr, info, refine, rtol, sngl, 0, croot, cstat,
+             ierr_out, nullptr);
+}
+
+// Persistent root kernel: lanes take (chain, column) items from a queue
+// (chains in `order`, Rayleigh first, columns consecutive) whenever their
+// current chain is finished, so lanes stay busy while long chains run.
+// queue[0] is the next item; the launch covers the GPU once.
+#ifndef SWDK_ROOTS_MINB
+#define SWDK_ROOTS_MINB 3  // 168 registers: 3 blocks of 128 per SM
+#endif
+#ifndef SWDK_EIGEN_MINB
+#define SWDK_EIGEN_MINB 4  // 128 registers: 16 warps/SM measured faster than 2 blocks at 230
+#endif
+__global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, int nitems, const int* __restrict__ order,
+                                                     const ChainDesc* __restrict__ chains,
+                                                     const double* __restrict__ periods,
+                                                     const float4* __restrict__ layR, const float4* __restrict__ layL,
+                                                     const double2* __restrict__ rab,
+                                                     const double2* __restrict__ rrmR,
+                                                     const double2* __restrict__ rrmL,
+                                                     const ColInfo* __restrict__ info, int refine, double rtol,
+                                                     int sngl, int retry, double* __restrict__ croot,
+                                                     int32_t* __restrict__ cstat, unsigned int* __restrict__ queue,
+                                                     unsigned long long* __restrict__ nevals) {
+  double cbuf[KMAX_CHAIN];
+  double cbbuf[KMAX_CHAIN + 24];
+  ChainState s;
+  ChainParams P;
+  ChainIO io;
+  LayerView V;
+  ChainDesc cd;
+  int col = 0;
+  bool have = false, exhausted = false;
+  unsigned long long ev_r = 0, ev_l = 0, lay_r = 0, lay_l = 0;
+  io.c = cbuf;
+  io.cb = cbbuf;
+  for (;;) {
+    bool need = false;
+    for (;;) {
+      if (!have) {
+        if (exhausted) break;
+        const unsigned int item = atomicAdd(queue, 1u);
+        if (item >= (unsigned int)nitems) { exhausted = true; break; }
+        cd = chains[order[item / ncol]];
+        col = item % ncol;
+        const ColInfo ci = info[col];
+        double* outp = croot + (size_t)cd.out_off * ncol + col;
+        int32_t* stp = cstat + (size_t)cd.out_off * ncol + col;
+        if (!ci.valid) {
+          for (int i = 0; i < cd.nmode * cd.np; ++i) { outp[(size_t)i * ncol] = 0.0; stp[(size_t)i * ncol] = ST_NAN_INPUT; }
+          continue;
+        }
+        V.lay = (cd.iwave == 2) ? layR : layL;
+        V.rab = rab;
+        V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
+        V.ncol = ncol;
+        V.col = col;
+        V.L = ci.L;
+        V.llw = ci.llw;
+        P.t = periods + cd.t_off;
+        P.kmax = cd.np;
+        P.nmode = cd.nmode;
+        P.igr = cd.igr;
+        P.iwave = cd.iwave;
+        P.refine = refine;
+        P.rtol = rtol;
+        P.sngl = sngl;
+        P.cc = ci.cc;
+        P.betmx = ci.betmx;
+        P.retry = retry;
+        io.out = outp;
+        io.st = stp;
+        io.stride = cd.np * ncol;
+        io.ostride = ncol;
+        chain_init(s);
+        have = true;
+      }
+      need = chain_advance(s, P, io);
+      if (need) break;
+      // chain finished
+      if (s.iterlim)
+        for (int i = 0; i < cd.nmode * cd.np; ++i)
+          if (io.st[(size_t)i * ncol] == ST_OK) io.st[(size_t)i * ncol] = ST_ITER_LIMIT;
+      if (cd.iwave == 2) { ev_r += s.nevals; lay_r += (unsigned long long)s.nevals * V.L; }
+      else { ev_l += s.nevals; lay_l += (unsigned long long)s.nevals * V.L; }
+      have = false;
+    }
+    if (__ballot_sync(0xffffffffu, need) == 0u) break;
+    if (need) {
+      s.last = secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega);
+      s.nevals++;
+      s.phase = s.next;
+    }
+  }
+  unsigned long long e = ev_r + ev_l;
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    lay_r += __shfl_down_sync(0xffffffffu, lay_r, o);
+    lay_l += __shfl_down_sync(0xffffffffu, lay_l, o);
+  }
+  if ((threadIdx.x & 31) == 0 && nevals) {
+    atomicAdd(nevals, e);
+    atomicAdd(nevals + 1, lay_r);
+    atomicAdd(nevals + 2, lay_l);
+  }
 }
 
 // cg(k, m) of model m = last mode's roots (surfdisp96's cg), model-major
@@ -403,7 +524,7 @@ __device__ __forceinline__ void accumulate_nodes(double* kacc, const double* na,
   }
 }
 
-__global__ void __launch_bounds__(128) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+__global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                                const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
                                                const SlotDesc* __restrict__ slots, int nslots,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
@@ -662,6 +783,8 @@ struct DevBuf {
 };
 
 struct Plan {
+  std::vector<int> order;  // chains queued Rayleigh first
+  DevBuf d_order;
   std::vector<ChainDesc> chains;
   std::vector<double> periods;
   std::vector<SlotDesc> slots;
@@ -686,7 +809,8 @@ struct swdk_ctx {
   bool have_periods = false;
   bool dirty = true;
   Plan plan[2];  // 0: get_1d_kernel, 1: get_2d_map
-  DevBuf layR, layL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr;
+  DevBuf layR, layL, rab, rrmR, rrmL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr, queue;
+  int roots_blocks = 0;
   DevBuf in_vs, in_vp, in_rho, out_vc, out_vout, out_kernel, out_status, in_misc;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // stage marks; ev[4]: call done
   unsigned long long* h_nevals = nullptr;
@@ -781,6 +905,12 @@ int build_plan(swdk_ctx* ctx, int path) {
     P.slots.push_back(s);
   }
   if (P.chains.empty()) return fail(ctx, SWDK_E_NOPERIODS, "no periods");
+  P.order.clear();
+  for (int w = 2; w >= 1; --w)
+    for (size_t i = 0; i < P.chains.size(); ++i)
+      if (P.chains[i].iwave == w) P.order.push_back((int)i);
+  CK(P.d_order.ensure(P.order.size() * sizeof(int)));
+  CK(cudaMemcpy(P.d_order.p, P.order.data(), P.order.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(P.d_chains.ensure(P.chains.size() * sizeof(ChainDesc)));
   CK(P.d_periods.ensure(P.periods.size() * sizeof(double)));
   CK(P.d_slots.ensure(P.slots.size() * sizeof(SlotDesc)));
@@ -817,6 +947,10 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   const int Lmax = 4 * nz - 3;
   CK(ctx->layR.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->layL.ensure((size_t)Lmax * ncol * sizeof(float4)));
+  CK(ctx->rab.ensure((size_t)Lmax * ncol * sizeof(double2)));
+  CK(ctx->rrmR.ensure((size_t)Lmax * ncol * sizeof(double2)));
+  CK(ctx->rrmL.ensure((size_t)Lmax * ncol * sizeof(double2)));
+  CK(ctx->queue.ensure(sizeof(unsigned int)));
   CK(ctx->lay0.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->info.ensure((size_t)ncol * sizeof(ColInfo)));
   CK(ctx->chainrule.ensure((size_t)nz * ncol * sizeof(float2)));
@@ -829,16 +963,26 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
+                                             ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                              ctx->chainrule.as<float2>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
-  const int bt = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : 128;
-  dim3 gr((ncol + bt - 1) / bt, (unsigned)P.chains.size());
-  k_roots<<<gr, bt, 0, st>>>(ncol, P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
-                             ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol,
-                             ctx->cfg.sngl, 1, ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), nullptr,
-                             ctx->nevals.as<unsigned long long>());
+  if (ctx->roots_blocks == 0) {
+    int dev = 0, nsm = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0));
+    ctx->roots_blocks = std::max(1, nsm * std::max(1, per));
+  }
+  const int nitems = (int)P.chains.size() * ncol;
+  const int rblocks = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : ctx->roots_blocks;
+  CK(cudaMemsetAsync(ctx->queue.p, 0, sizeof(unsigned int), st));
+  k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, 0, st>>>(
+      ncol, nitems, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
+      ctx->layL.as<float4>(), ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
+      ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, 1, ctx->croot.as<double>(),
+      ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(), ctx->nevals.as<unsigned long long>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[2], st));
   const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
@@ -1067,6 +1211,9 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaMemcpyAsync(d_ch, &cd, sizeof(cd), cudaMemcpyHostToDevice, st));
   CK(ctx->layR.ensure(nin * sizeof(float4)));
   CK(ctx->layL.ensure(nin * sizeof(float4)));
+  CK(ctx->rab.ensure(nin * sizeof(double2)));
+  CK(ctx->rrmR.ensure(nin * sizeof(double2)));
+  CK(ctx->rrmL.ensure(nin * sizeof(double2)));
   CK(ctx->info.ensure(nm * sizeof(ColInfo)));
   CK(ctx->croot.ensure((size_t)mode * kmax * nm * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)mode * kmax * nm * sizeof(int32_t)));
@@ -1076,7 +1223,9 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_in, d_in + nin, d_in + 2 * nin,
                                                        d_in + 3 * nin, iflsph, ctx->layR.as<float4>(),
-                                                       ctx->layL.as<float4>(), ctx->info.as<ColInfo>());
+                                                       ctx->layL.as<float4>(), ctx->rab.as<double2>(),
+                                                       ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
+                                                       ctx->info.as<ColInfo>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
   k_roots<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(nmodel, d_ch, d_t, ctx->layR.as<float4>(),
@@ -1167,7 +1316,7 @@ int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_t
     ChainDesc cd;
     cd.t_off = 0; cd.np = kmax; cd.nmode = mode; cd.iwave = iwave; cd.igr = igr; cd.out_off = 0;
     k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_thk, d_vp, d_vs, d_rho, iflsph, layR, layL,
-                                                         info);
+                                                         nullptr, nullptr, nullptr, info);
     k_roots_one<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(cd, nmodel, d_t, layR, layL, info, refine,
                                                                rtol > 0.0 ? rtol : 1e-10, sngl, croot, cstat, d_ierr);
     const int n = nmodel * kmax;

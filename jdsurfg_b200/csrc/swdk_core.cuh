@@ -65,6 +65,7 @@ SWDK_HD cx operator*(double s, cx a) { return mkc(s * a.re, s * a.im); }
 SWDK_HD cx operator*(cx a, double s) { return mkc(a.re * s, a.im * s); }
 SWDK_HD cx operator/(cx a, double s) { return mkc(a.re / s, a.im / s); }
 SWDK_HD cx operator+(cx a, double s) { return mkc(a.re + s, a.im); }
+SWDK_HD cx operator+(double s, cx a) { return mkc(s + a.re, a.im); }
 SWDK_HD cx operator-(double s, cx a) { return mkc(s - a.re, -a.im); }
 SWDK_HD cx operator/(cx a, cx b) {
   if (fabs(b.re) >= fabs(b.im)) {
@@ -100,12 +101,15 @@ SWDK_HD int pow2_exponent(double t) {
 //   counts layers upward (bottom-aligned, layer-major)
 // ---------------------------------------------------------------------------
 struct LayerView {
-  const float4* lay;
+  const float4* lay;   // (d, a, b, rho) REAL*4 as surfdisp96 holds them
+  const double2* rab;  // (1/a, 1/b) in FP64, or null
+  const double2* rrm;  // (1/rho, 1/(rho b^2)) in FP64, or null
   int ncol, col;
   int L;    // layers including the half-space
   int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
+  SWDK_HD size_t idx(int m) const { return (size_t)(L - 1 - m) * ncol + col; }
   SWDK_HD float4 get(int m) const {  // m: reference (top-down, 0-based) index
-    return lay[(size_t)(L - 1 - m) * ncol + col];
+    return lay[idx(m)];
   }
 };
 
@@ -275,8 +279,228 @@ SWDK_HDI double dltar1(const LayerView& V, double wvno, double omega) {
   return e1;
 }
 
+// dltar4 with the per-layer reciprocals precomputed (1/a, 1/b, 1/rho), the
+// vertical wavenumber and its reciprocal from one rsqrt, exp(-(p+q)) as
+// exp(-p) exp(-q), and the max-normalisation applied every NORM layers
+// (NORM = 1 is surfdisp96's per-layer normc; larger NORM rescales the
+// propagated vector by a different positive factor, which changes neither
+// the sign nor the continuity of the period equation in c).
+struct LayerCoef {
+  double a0, cpcq, cpy, cpz, cqw, cqx, xy, xz, wy, wz, gam, gammk, rho, irho;
+};
+
+SWDK_HD LayerCoef layer_coef(const LayerView& V, int m, double wvno, double wvno2, double omega, double iom) {
+  const size_t ix = V.idx(m);
+  const float4 ly = V.lay[ix];
+  const double2 rr = V.rab[ix];
+  LayerCoef k;
+  k.irho = V.rrm[ix].x;
+  const double dpth = ly.x;
+  k.rho = ly.w;
+  const double xka = omega * rr.x, xkb = omega * rr.y;
+  const double t = (double)ly.z * iom;
+  k.gammk = 2.0 * t * t;
+  k.gam = k.gammk * wvno2;
+  const double Xa = (wvno + xka) * fabs(wvno - xka);
+  const double Xb = (wvno + xkb) * fabs(wvno - xkb);
+  // var (surfdisp96.f:901-1018); ep = exp(-pex), eq = exp(-sex)
+  double w, x, cosp, y, z, cosq, ep = 1.0, eq = 1.0, pex = 0.0, sex = 0.0;
+  if (wvno < xka) {
+    const double ir = rsqrt(Xa), r = Xa * ir;
+    double sp, cp;
+    sincos(r * dpth, &sp, &cp);
+    w = sp * ir; x = -r * sp; cosp = cp;
+  } else if (wvno == xka) {
+    cosp = 1.0; w = dpth; x = 0.0;
+  } else {
+    const double ir = rsqrt(Xa), r = Xa * ir, p = r * dpth;
+    pex = p;
+    ep = (p < 60.0) ? exp(-p) : 0.0;
+    const double fac = (p < 16.0) ? ep * ep : 0.0;
+    cosp = (1.0 + fac) * 0.5;
+    const double sp = (1.0 - fac) * 0.5;
+    w = sp * ir; x = r * sp;
+  }
+  if (wvno < xkb) {
+    const double ir = rsqrt(Xb), r = Xb * ir;
+    double sq, cq;
+    sincos(r * dpth, &sq, &cq);
+    y = sq * ir; z = -r * sq; cosq = cq;
+  } else if (wvno == xkb) {
+    cosq = 1.0; y = dpth; z = 0.0;
+  } else {
+    const double ir = rsqrt(Xb), r = Xb * ir, q = r * dpth;
+    sex = q;
+    eq = (q < 60.0) ? exp(-q) : 0.0;
+    const double fac = (q < 16.0) ? eq * eq : 0.0;
+    cosq = (1.0 + fac) * 0.5;
+    const double sq = (1.0 - fac) * 0.5;
+    y = sq * ir; z = r * sq;
+  }
+  // a0 = exp(-(pex+sex)) when pex+sex < 60 (both factors then below 60)
+  k.a0 = (pex + sex < 60.0) ? ep * eq : 0.0;
+  k.cpcq = cosp * cosq; k.cpy = cosp * y; k.cpz = cosp * z; k.cqw = cosq * w; k.cqx = cosq * x;
+  k.xy = x * y; k.xz = x * z; k.wy = w * y; k.wz = w * z;
+  return k;
+}
+
+// e <- e * Dunkin(k) (surfdisp96.f:1051-1095 and dltar4's product)
+SWDK_HD void apply_dunkin(const LayerCoef& k, double wvno2, double& e0, double& e1, double& e2, double& e3,
+                          double& e4) {
+  const double gam = k.gam, gammk = k.gammk, rho = k.rho, irho = k.irho;
+  const double gamm1 = gam - 1.0;
+  const double twgm1 = gam + gamm1, gmgmk = gam * gammk, gmgm1 = gam * gamm1, gm1sq = gamm1 * gamm1;
+  const double rho2 = rho * rho, irho2 = irho * irho;
+  const double a0pq = k.a0 - k.cpcq;
+  const double c11 = k.cpcq - 2.0 * gmgm1 * a0pq - gmgmk * k.xz - wvno2 * gm1sq * k.wy;
+  const double c12 = (wvno2 * k.cpy - k.cqx) * irho;
+  const double c13 = -(twgm1 * a0pq + gammk * k.xz + wvno2 * gamm1 * k.wy) * irho;
+  const double c14 = (k.cpz - wvno2 * k.cqw) * irho;
+  const double c15 = -(2.0 * wvno2 * a0pq + k.xz + wvno2 * wvno2 * k.wy) * irho2;
+  const double c21 = (gmgmk * k.cpz - gm1sq * k.cqw) * rho;
+  const double c22 = k.cpcq;
+  const double c23 = gammk * k.cpz - gamm1 * k.cqw;
+  const double c24 = -k.wz;
+  const double c41 = (gm1sq * k.cpy - gmgmk * k.cqx) * rho;
+  const double c42 = -k.xy;
+  const double c43 = gamm1 * k.cpy - gammk * k.cqx;
+  const double c51 = -(2.0 * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * k.xz + gm1sq * gm1sq * k.wy) * rho2;
+  const double c53 = -(gammk * gamm1 * twgm1 * a0pq + gam * gammk * gammk * k.xz + gamm1 * gm1sq * k.wy) * rho;
+  const double tt = -2.0 * wvno2;
+  const double c31 = tt * c53, c32 = tt * c43, c33 = k.a0 + 2.0 * (k.cpcq - c11), c34 = tt * c23, c35 = tt * c13;
+  const double f0 = e0 * c11 + e1 * c21 + e2 * c31 + e3 * c41 + e4 * c51;
+  const double f1 = e0 * c12 + e1 * c22 + e2 * c32 + e3 * c42 + e4 * c41;
+  const double f2 = e0 * c13 + e1 * c23 + e2 * c33 + e3 * c43 + e4 * c53;
+  const double f3 = e0 * c14 + e1 * c24 + e2 * c34 + e3 * c22 + e4 * c21;
+  const double f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
+  e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
+}
+
+template <int NORM>
+SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
+  double omega = omga;
+  if (omega < 1.0e-4) omega = 1.0e-4;
+  const double wvno2 = wvno * wvno;
+  const double iom = 1.0 / omega;
+  const size_t ih = V.idx(V.L - 1);
+  const float4 h = V.lay[ih];
+  const double2 hr = V.rab[ih];
+  double xka = omega * hr.x, xkb = omega * hr.y;
+  const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
+  const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+  const double t = (double)h.z * iom;
+  const double gammk = 2.0 * t * t;
+  const double gam = gammk * wvno2;
+  const double gamm1 = gam - 1.0;
+  const double rho1 = h.w;
+  double e0 = rho1 * rho1 * (gamm1 * gamm1 - gam * gammk * ra * rb);
+  double e1 = -rho1 * ra;
+  double e2 = rho1 * (gamm1 - gammk * ra * rb);
+  double e3 = rho1 * rb;
+  double e4 = wvno2 - ra * rb;
+  const int mlo = V.llw - 1;
+  int since = 0;
+  for (int m = V.L - 2; m >= mlo; --m) {
+    const LayerCoef cur = layer_coef(V, m, wvno, wvno2, omega, iom);
+    apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
+    if (++since >= NORM || m == mlo) {
+      since = 0;
+      double t1 = fmax(fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))), fabs(e4));
+      if (t1 < 1.e-40) t1 = 1.0;
+      if (NORM == 1) {
+        e0 = e0 / t1; e1 = e1 / t1; e2 = e2 / t1; e3 = e3 / t1; e4 = e4 / t1;
+      } else {
+        const double it1 = 1.0 / t1;
+        e0 *= it1; e1 *= it1; e2 *= it1; e3 *= it1; e4 *= it1;
+      }
+    }
+  }
+  if (V.llw != 1) {
+    const size_t ix = V.idx(0);
+    const float4 ly = V.lay[ix];
+    const double dpth = ly.x, rho = ly.w;
+    xka = omega * V.rab[ix].x;
+    const double Xa = (wvno + xka) * fabs(wvno - xka);
+    double w, cosp;
+    if (wvno < xka) {
+      const double ir = rsqrt(Xa), r = Xa * ir;
+      double sp, cp;
+      sincos(r * dpth, &sp, &cp);
+      w = sp * ir; cosp = cp;
+    } else if (wvno == xka) {
+      cosp = 1.0; w = dpth;
+    } else {
+      const double ir = rsqrt(Xa), r = Xa * ir, p = r * dpth;
+      const double fac = (p < 16.0) ? exp(-2.0 * p) : 0.0;
+      cosp = (1.0 + fac) * 0.5;
+      w = ((1.0 - fac) * 0.5) * ir;
+    }
+    const double w0 = -rho * w;
+    return cosp * e0 + w0 * e1;
+  }
+  return e0;
+}
+
+// dltar1 with precomputed 1/b and 1/(rho b^2)
+template <int NORM>
+SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
+  const size_t ih = V.idx(V.L - 1);
+  float4 h = V.lay[ih];
+  double beta1 = h.z, rho1 = h.w;
+  double xkb = omega * V.rab[ih].y;
+  double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+  double e1 = rho1 * rb;
+  double e2 = 1.0 / (beta1 * beta1);
+  int since = 0;
+  for (int m = V.L - 2; m >= V.llw - 1; --m) {
+    const size_t ix = V.idx(m);
+    const float4 ly = V.lay[ix];
+    const double ib = V.rab[ix].y, ixmu = V.rrm[ix].y;
+    beta1 = ly.z;
+    rho1 = ly.w;
+    const double dpth = ly.x;
+    const double xmu = rho1 * beta1 * beta1;
+    xkb = omega * ib;
+    const double Xb = (wvno + xkb) * fabs(wvno - xkb);
+    double cosq, y, z;
+    if (wvno < xkb) {
+      const double ir = rsqrt(Xb), r = Xb * ir;
+      double sq, cq;
+      sincos(dpth * r, &sq, &cq);
+      y = sq * ir; z = -r * sq; cosq = cq;
+    } else if (wvno == xkb) {
+      cosq = 1.0; y = dpth; z = 0.0;
+    } else {
+      const double ir = rsqrt(Xb), r = Xb * ir, q = dpth * r;
+      const double fac = (q < 16.0) ? exp(-2.0 * q) : 0.0;
+      cosq = (1.0 + fac) * 0.5;
+      const double sq = (1.0 - fac) * 0.5;
+      y = sq * ir; z = r * sq;
+    }
+    const double e10 = e1 * cosq + e2 * xmu * z;
+    const double e20 = e1 * y * ixmu + e2 * cosq;
+    if (++since >= NORM || m == V.llw - 1) {
+      since = 0;
+      double xnor = fmax(fabs(e10), fabs(e20));
+      if (xnor < 1.e-40) xnor = 1.0;
+      if (NORM == 1) { e1 = e10 / xnor; e2 = e20 / xnor; }
+      else { const double ix2 = 1.0 / xnor; e1 = e10 * ix2; e2 = e20 * ix2; }
+    } else {
+      e1 = e10; e2 = e20;
+    }
+  }
+  return e1;
+}
+
 SWDK_HD double secular(const LayerView& V, int iwave, double wvno, double omega) {
   return (iwave == 1) ? dltar1(V, wvno, omega) : dltar4(V, wvno, omega);
+}
+
+// production secular function: reciprocal-table variants; the reference
+// refinement keeps per-layer normalisation like surfdisp96
+SWDK_HD double secular_fast(const LayerView& V, int iwave, int refine, double wvno, double omega) {
+  if (refine == 0) return (iwave == 1) ? dltar1_fast<1>(V, wvno, omega) : dltar4_fast<1>(V, wvno, omega);
+  return (iwave == 1) ? dltar1_fast<4>(V, wvno, omega) : dltar4_fast<4>(V, wvno, omega);
 }
 
 // ---------------------------------------------------------------------------
@@ -677,7 +901,8 @@ SWDK_HDI void run_chain(const LayerView& V, const ChainParams& P, const ChainIO&
     if (!need) active = false;
     if (__ballot_sync(0xffffffffu, need) == 0u) break;
     if (need) {
-      s.last = secular(V, P.iwave, s.omega / s.creq, s.omega);
+      s.last = V.rab ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
+                     : secular(V, P.iwave, s.omega / s.creq, s.omega);
       s.nevals++;
       s.phase = s.next;
     }
@@ -685,7 +910,8 @@ SWDK_HDI void run_chain(const LayerView& V, const ChainParams& P, const ChainIO&
 #else
   if (!active) return;
   while (chain_advance(s, P, io)) {
-    s.last = secular(V, P.iwave, s.omega / s.creq, s.omega);
+    s.last = V.rab ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
+                   : secular(V, P.iwave, s.omega / s.creq, s.omega);
     s.nevals++;
     s.phase = s.next;
   }

@@ -274,89 +274,123 @@ struct Eig4 {
   double ur, uz, tz, tr;
 };
 
-// per-layer pieces of intijr that do not depend on (i, j)
-struct IntPieces {
-  cx kmpu, kmsu, km1pd, km1sd, FA, GA, FB, GB, H1, H2;
-};
-
-// intijr (sregn96.f90:1198-1317) for one (i, j) given the shared pieces
-SWDK_HD double intijr_c(const EMat& E, const IntPieces& P, int iwat, int typelyr, int i, int j) {
-  const cx(&e)[4][4] = E.e;
-  const cx ra = E.ra, rb = E.rb;
-  cx cint;
-  if (iwat == 1) {
-    if (typelyr == 0) {
-      cint = e[i][0] * e[j][0] * P.kmpu * P.kmpu * P.FA + (e[i][0] * e[j][1] + e[i][1] * e[j][0]) * P.kmpu * P.km1pd * P.GA +
-             e[i][1] * e[j][1] * P.km1pd * P.km1pd * P.FA;
-    } else {
-      cint = e[i][1] * e[j][1] * P.km1pd * P.km1pd / (2.0 * ra);
-    }
-  } else {
-    if (typelyr == 0) {
-      cint = e[i][0] * e[j][0] * P.kmpu * P.kmpu * P.FA + e[i][2] * e[j][2] * P.km1pd * P.km1pd * P.FA +
-             e[i][1] * e[j][1] * P.kmsu * P.kmsu * P.FB + e[i][3] * e[j][3] * P.km1sd * P.km1sd * P.FB +
-             P.H1 * ((e[i][0] * e[j][1] + e[i][1] * e[j][0]) * P.kmpu * P.kmsu +
-                     (e[i][2] * e[j][3] + e[i][3] * e[j][2]) * P.km1pd * P.km1sd) +
-             P.H2 * ((e[i][0] * e[j][3] + e[i][3] * e[j][0]) * P.kmpu * P.km1sd +
-                     (e[i][1] * e[j][2] + e[i][2] * e[j][1]) * P.km1pd * P.kmsu) +
-             P.GA * (e[i][0] * e[j][2] + e[i][2] * e[j][0]) * P.kmpu * P.km1pd +
-             P.GB * (e[i][1] * e[j][3] + e[i][3] * e[j][1]) * P.kmsu * P.km1sd;
-    } else {
-      cint = e[i][2] * e[j][2] * P.km1pd * P.km1pd / (2.0 * ra) +
-             (e[i][2] * e[j][3] + e[i][3] * e[j][2]) * P.km1pd * P.km1sd / (ra + rb) +
-             e[i][3] * e[j][3] * P.km1sd * P.km1sd / (2.0 * rb);
-    }
-  }
-  return cint.re;
-}
-
-SWDK_HD cx erow(const cx* r, const Eig4& u) {  // r[0]*ur + r[1]*uz + r[2]*tz + r[3]*tr
-  return r[0] * u.ur + r[1] * u.uz + r[2] * u.tz + r[3] * u.tr;
-}
 
 struct EnergyAcc {
   double sumi0, sumi1, sumi2, sumi3;
 };
 
 // energy() body for one layer m (sregn96.f90:1097-1178); writes the raw
-// (un-normalised) dcda, dcdb, dcdr of the layer
+// (un-normalised) dcda, dcdb, dcdr of the layer.
+//
+// intijr (sregn96.f90:1198-1317) is evaluated without forming E and E^-1:
+// row r of E (evalg, sregn96.f90:716-734) is (p_r, q_r, s_r p_r, -s_r q_r)
+// with s = (+,-,+,-), (p,q) = (k, rb), (ra, k), (g1, g2 rb), (g2 ra, g1),
+// k = wvno, g1 = rho om2 (gam-1), g2 = rho om2 gam / k; all six integrals
+// used by energy pair rows of equal sign s, so with P = p_i p_j,
+// Q = q_i q_j, X = p_i q_j + q_i p_j
+//   interior layer: cint = P SA_s + Q SB_s + X SX_s,
+//     SA_s = FA (kmpu^2 + km1pd^2) + 2 s GA kmpu km1pd
+//     SB_s = FB (kmsu^2 + km1sd^2) - 2 s GB kmsu km1sd
+//     SX_s = H1 (kmpu kmsu - km1pd km1sd) + s H2 (km1pd kmsu - kmpu km1sd)
+//   half-space:     cint = P km1pd^2/(2ra) - X km1pd km1sd/(ra+rb) + Q km1sd^2/(2rb)
+// and the potentials are rows of E^-1 applied to (ur, uz, tz, tr).
+// exp(-2 ra d), exp(-(ra+rb) d) are products of exp(-ra d), exp(-rb d).
+SWDK_HD double re_mul(cx a, cx b) { return a.re * b.re - a.im * b.im; }
+SWDK_HD cx cinv(cx a) {  // 1/a for pure real or pure imaginary a
+  if (a.im == 0.0) return mkc(1.0 / a.re, 0.0);
+  if (a.re == 0.0) return mkc(0.0, -1.0 / a.im);
+  return mkc(1.0) / a;
+}
+
 SWDK_HD void energy_layer_r(const EigModel& M, int m, int iwat, bool allfluid, const Eig4& u0, const Eig4& u1,
                             double om, double om2, double wvno, double wvno2, double c, EnergyAcc& acc,
                             double& dcda, double& dcdb, double& dcdr) {
+  (void)allfluid;
   const int typelyr = (m == M.L - 1) ? 1 : 0;
-  EMat E;
-  evalg_r(M, m, iwat, allfluid, wvno, om, om2, wvno2, E, nullptr);
-  IntPieces P;
-  const double zdm = M.zd[m];
-  if (iwat == 1) {
-    P.km1pd = E.ei[1][0] * u0.uz + E.ei[1][1] * u0.tz;
+  const double za = M.za[m], zb = M.zb[m], zr = M.zrho[m], zdm = M.zd[m];
+  const double xka = om / za;
+  const double xkb = (zb > 0.0) ? om / zb : 0.0;
+  const double ra2 = wvno2 - xka * xka, rb2 = wvno2 - xkb * xkb;
+  const cx ra = csqrt_real(ra2), rb = csqrt_real(rb2);
+  double gam = zb * wvno / om;
+  gam = 2.0 * (gam * gam);
+  const double gamm1 = gam - 1.0;
+  const double rom2 = zr * om2;
+  double INT11, INT13 = 0.0, INT22, INT24 = 0.0, INT33 = 0.0, INT44 = 0.0;
+  // exp(-ra d), exp(-rb d) with the reference's cut-offs applied by the users
+  auto cexp_neg = [](cx r, double d) { return cexpc(mkc(-r.re * d, -r.im * d)); };
+  if (iwat == 0) {
+    const double g1 = rom2 * gamm1, g2 = rom2 * gam / wvno;
+    const double h1 = 0.5 * gam / wvno, h2 = -(0.5 / rom2), ga = 0.5 * gamm1, wa = 0.5 * wvno / rom2;
+    const cx ira = cinv(ra), irb = cinv(rb);
+    const cx km1pd = (h1 * u0.ur + h2 * u0.tz) + (ga * u0.uz - wa * u0.tr) * ira;
+    const cx km1sd = (ga * u0.ur - wa * u0.tz) * irb + (h1 * u0.uz + h2 * u0.tr);
+    const double k = wvno, k2 = wvno2;
+    // pair coefficients: P (real), Q (real), X = xr * r (r = ra or rb)
     if (typelyr == 0) {
-      P.kmpu = E.ei[0][0] * u1.uz + E.ei[0][1] * u1.tz;
-      P.FA = ffunc_c(E.ra, zdm);
-      P.GA = gfunc_c(E.ra, zdm);
+      const cx kmpu = (h1 * u1.ur + h2 * u1.tz) - (ga * u1.uz - wa * u1.tr) * ira;
+      const cx kmsu = (h1 * u1.uz + h2 * u1.tr) - (ga * u1.ur - wa * u1.tz) * irb;
+      // FA, GA, FB, GB, H1, H2 (sregn96.f90:1319-1397)
+      const cx ard = ra * zdm, brd = rb * zdm;
+      const cx ea = (ard.re < 75.0) ? cexp_neg(ra, zdm) : mkc(0.0);
+      const cx eb = (brd.re < 75.0) ? cexp_neg(rb, zdm) : mkc(0.0);
+      const cx ea40 = (ard.re < 40.0) ? ea : mkc(0.0);
+      const cx eb40 = (brd.re < 40.0) ? eb : mkc(0.0);
+      const cx FA = (cabsc(ra) < 1.0e-08) ? mkc(zdm) : (1.0 - ea40 * ea40) / (2.0 * ra);
+      const cx FB = (cabsc(rb) < 1.0e-08) ? mkc(zdm) : (1.0 - eb40 * eb40) / (2.0 * rb);
+      const cx GA = ea * zdm, GB = eb * zdm;
+      const cx sab = ra + rb;
+      const cx H1 = (cabsc(sab) < 1.0e-08) ? mkc(zdm)
+                    : (1.0 - ((((ard + brd).re) < 40.0) ? ea * eb : mkc(0.0))) / sab;
+      const cx dab = ra - rb;
+      const cx H2 = (cabsc(dab) < 1.0e-08) ? mkc(zdm) : (eb40 - ea40) / dab;
+      const cx pp = kmpu * kmpu + km1pd * km1pd, ss = kmsu * kmsu + km1sd * km1sd;
+      const cx pd = kmpu * km1pd, sd = kmsu * km1sd;
+      const cx x1 = kmpu * kmsu - km1pd * km1sd, x2 = km1pd * kmsu - kmpu * km1sd;
+      const cx FApp = FA * pp, GApd2 = 2.0 * (GA * pd), FBss = FB * ss, GBsd2 = 2.0 * (GB * sd);
+      const cx H1x = H1 * x1, H2x = H2 * x2;
+      const cx SAp = FApp + GApd2, SAm = FApp - GApd2;
+      const cx SBp = FBss - GBsd2, SBm = FBss + GBsd2;
+      const cx SXp = H1x + H2x, SXm = H1x - H2x;
+      INT11 = k2 * SAp.re + rb2 * SBp.re + 2.0 * k * re_mul(rb, SXp);
+      INT13 = k * g1 * SAp.re + g2 * rb2 * SBp.re + (k * g2 + g1) * re_mul(rb, SXp);
+      INT33 = g1 * g1 * SAp.re + g2 * g2 * rb2 * SBp.re + 2.0 * g1 * g2 * re_mul(rb, SXp);
+      INT22 = ra2 * SAm.re + k2 * SBm.re + 2.0 * k * re_mul(ra, SXm);
+      INT24 = g2 * ra2 * SAm.re + k * g1 * SBm.re + (g1 + k * g2) * re_mul(ra, SXm);
+      INT44 = g2 * g2 * ra2 * SAm.re + g1 * g1 * SBm.re + 2.0 * g1 * g2 * re_mul(ra, SXm);
+    } else {
+      const cx TA = (km1pd * km1pd) / (2.0 * ra), TB = (km1sd * km1sd) / (2.0 * rb);
+      const cx TX = -((km1pd * km1sd) / (ra + rb));
+      INT11 = k2 * TA.re + rb2 * TB.re + 2.0 * k * re_mul(rb, TX);
+      INT13 = k * g1 * TA.re + g2 * rb2 * TB.re + (k * g2 + g1) * re_mul(rb, TX);
+      INT33 = g1 * g1 * TA.re + g2 * g2 * rb2 * TB.re + 2.0 * g1 * g2 * re_mul(rb, TX);
+      INT22 = ra2 * TA.re + k2 * TB.re + 2.0 * k * re_mul(ra, TX);
+      INT24 = g2 * ra2 * TA.re + k * g1 * TB.re + (g1 + k * g2) * re_mul(ra, TX);
+      INT44 = g2 * g2 * ra2 * TA.re + g1 * g1 * TB.re + 2.0 * g1 * g2 * re_mul(ra, TX);
     }
   } else {
-    P.km1pd = erow(E.ei[2], u0);
-    P.km1sd = erow(E.ei[3], u0);
+    // fluid layer: 2x2 E = [[ra, -ra], [-rho om2, -rho om2]] (sregn96.f90:791-801)
+    const cx ira = cinv(ra);
+    const double ir = -(0.5 / rom2);
+    const cx km1pd = (-0.5 * u0.uz) * ira + ir * u0.tz;
+    const double w = -rom2;
     if (typelyr == 0) {
-      P.kmpu = erow(E.ei[0], u1);
-      P.kmsu = erow(E.ei[1], u1);
-      P.FA = ffunc_c(E.ra, zdm);
-      P.GA = gfunc_c(E.ra, zdm);
-      P.FB = ffunc_c(E.rb, zdm);
-      P.GB = gfunc_c(E.rb, zdm);
-      P.H1 = h1func_c(E.ra, E.rb, zdm);
-      P.H2 = h2func_c(E.ra, E.rb, zdm);
+      const cx kmpu = (0.5 * u1.uz) * ira + ir * u1.tz;
+      const cx ard = ra * zdm;
+      const cx ea = (ard.re < 75.0) ? cexp_neg(ra, zdm) : mkc(0.0);
+      const cx ea40 = (ard.re < 40.0) ? ea : mkc(0.0);
+      const cx FA = (cabsc(ra) < 1.0e-08) ? mkc(zdm) : (1.0 - ea40 * ea40) / (2.0 * ra);
+      const cx GA = ea * zdm;
+      const cx sq = (kmpu * kmpu + km1pd * km1pd) * FA, cr = 2.0 * (kmpu * km1pd * GA);
+      INT11 = ra2 * (sq - cr).re;
+      INT22 = w * w * (sq + cr).re;
+    } else {
+      const cx t = (km1pd * km1pd) / (2.0 * ra);
+      INT11 = 0.0;
+      INT22 = w * w * t.re;
     }
   }
-  const double INT11 = intijr_c(E, P, iwat, typelyr, 0, 0);
-  const double INT13 = intijr_c(E, P, iwat, typelyr, 0, 2);
-  const double INT22 = intijr_c(E, P, iwat, typelyr, 1, 1);
-  const double INT24 = intijr_c(E, P, iwat, typelyr, 1, 3);
-  const double INT33 = intijr_c(E, P, iwat, typelyr, 2, 2);
-  const double INT44 = intijr_c(E, P, iwat, typelyr, 3, 3);
-  // getmat (sregn96.f90:1531-1583)
-  const double za = M.za[m], zb = M.zb[m], zr = M.zrho[m];
+  // getmat (sregn96.f90:1531-1583) and the energy sums
   const double rho = zr, ah = za, av = za, eta = 1.0;
   const double TA = zr * za * za, TC = zr * za * za;
   if (iwat == 1) {
@@ -378,8 +412,8 @@ SWDK_HD void energy_layer_r(const EigModel& M, int m, int iwat, bool allfluid, c
     dcdr = 0.5 * (av * facav + ah * facah) / rho + facr;
   } else {
     const double bv = zb;
-    const double TL = zr * zb * zb, TN = zr * zb * zb;
-    const double TF = TA - 2. * TN;
+    const double TL = zr * zb * zb;
+    const double TF = TA - 2. * TL;
     const double a12 = -wvno, a14 = 1.0 / TL, a21 = wvno * TF / TC, a23 = 1.0 / TC;
     const double URUR = INT11, UZUZ = INT22;
     const double DURDUR = a12 * a12 * INT22 + 2. * a12 * a14 * INT24 + a14 * a14 * INT44;
