@@ -5,8 +5,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "swdk.cu")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("swdk.cu", "swdk_core.cuh", "swdk_eigen.cuh")] + [
+SRC = [os.path.join(HERE, "csrc", f) for f in ("swdk.cu", "swdk_mlp.cu")]
+DEPS = [os.path.join(HERE, "csrc", f) for f in ("swdk.cu", "swdk_mlp.cu", "swdk_core.cuh", "swdk_eigen.cuh")] + [
     os.path.join(ROOT, "include", "swdk.h")]
 OUT = os.path.join(HERE, "libswdk.so")
 
@@ -35,7 +35,7 @@ def needs_build():
 def build(verbose=False, force=False):
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + [SRC, "-o", OUT + ".tmp"]
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + SRC + ["-o", OUT + ".tmp"]
     subprocess.run(cmd, check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT

@@ -1,0 +1,113 @@
+"""The proposal network's hand-written kernels on the GPU: the tcgen05 GEMM
+against torch, and forward/backward gradients against an FP64 CPU MLP."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 64), (256, 256, 320), (1024, 256, 256), (256, 320, 1024)])
+def test_tcgen05_gemm_matches_torch(M, N, K):
+    import torch
+    from jdsurfg_b200.mlp import gemm_bf16_tn
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    a = torch.randn(M, K, device="cuda", generator=g).bfloat16()
+    b = torch.randn(N, K, device="cuda", generator=g).bfloat16()
+    c = torch.full((M, N), float("nan"), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    gemm_bf16_tn(a, b, c, err)
+    torch.cuda.synchronize()
+    ref = a.double() @ b.double().T
+    assert int(err.item()) == 0
+    assert torch.isfinite(c).all()
+    rel = ((c.double() - ref).abs().max() / ref.abs().max()).item()
+    assert rel < 1e-5, rel
+
+
+def _np_mlp_loss_grads(w, x, y):
+    """FP64 reference of the network, its Gaussian NLL and gradients."""
+    from math import sqrt
+    from scipy.special import erf
+    from jdsurfg_b200.mlp import layout
+    L = layout()
+    acts, pre = [x], []
+    h = x
+    for i, (wo, n, k, bo) in enumerate(L):
+        W = w[wo:wo + n * k].reshape(n, k)
+        b = w[bo:bo + n]
+        z = h @ W.T + b
+        pre.append(z)
+        if i < len(L) - 1:
+            h = 0.5 * z * (1.0 + erf(z / sqrt(2.0)))
+            acts.append(h)
+    out = pre[-1]
+    M = len(y)
+    mu, ls = out[:, 0], np.clip(out[:, 1], -12, 4)
+    e = (y - mu) * np.exp(-ls)
+    loss = np.mean(0.5 * e * e + ls)
+    dz = np.zeros_like(out)
+    dz[:, 0] = -e * np.exp(-ls) / M
+    dz[:, 1] = (1 - e * e) / M
+    g = np.zeros_like(w)
+    for i in range(len(L) - 1, -1, -1):
+        wo, n, k, bo = L[i]
+        W = w[wo:wo + n * k].reshape(n, k)
+        g[wo:wo + n * k] = (dz.T @ acts[i]).ravel()
+        g[bo:bo + n] = dz.sum(0)
+        if i > 0:
+            dh = dz @ W
+            z = pre[i - 1]
+            cdf = 0.5 * (1 + erf(z / sqrt(2.0)))
+            pdf = np.exp(-0.5 * z * z) / sqrt(2 * np.pi)
+            dz = dh * (cdf + z * pdf)
+    return loss, g
+
+
+def test_mlp_gradients_match_fp64_cpu():
+    import torch
+    from jdsurfg_b200.mlp import MLP, layout
+    net = MLP(seed=7)
+    w = net.params().astype(np.float64)
+    # weights as the GPU sees them (bf16)
+    wb = torch.from_numpy(w.astype(np.float32)).bfloat16().double().numpy()
+    rng = np.random.default_rng(0)
+    M = 200
+    x = np.zeros((M, 320), np.float32)
+    x[:, :258] = rng.standard_normal((M, 258)).astype(np.float32) * 0.5
+    y = rng.standard_normal(M).astype(np.float32) * 0.3
+    xb = torch.from_numpy(x).cuda().bfloat16()
+    yt = torch.from_numpy(y).cuda()
+    loss = net.train_step(xb, yt, 0.0)
+    g = net.grads().astype(np.float64)
+    lref, gref = _np_mlp_loss_grads(wb, xb.double().cpu().numpy(), y.astype(np.float64))
+    assert abs(loss - lref) < 1e-2 * max(1.0, abs(lref)), (loss, lref)
+    for i, (wo, n, k, bo) in enumerate(layout()):
+        a, b = g[wo:wo + n * k], gref[wo:wo + n * k]
+        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)
+        rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30)
+        # BF16 activations and operands between layers: ~1 % agreement
+        assert cos > 0.999 and rel < 0.05, (i, cos, rel)
+
+
+def test_mlp_learns_and_checkpoints(tmp_path):
+    import torch
+    from jdsurfg_b200.mlp import MLP
+    net = MLP(seed=3)
+    rng = np.random.default_rng(1)
+    M = 1024
+    x = np.zeros((M, 320), np.float32)
+    x[:, :258] = rng.standard_normal((M, 258)).astype(np.float32) * 0.5
+    y = (x[:, :8].sum(1) * 0.2).astype(np.float32)
+    xb = torch.from_numpy(x).cuda().bfloat16()
+    yt = torch.from_numpy(y).cuda()
+    first = net.train_step(xb, yt, 1e-3)
+    for _ in range(300):
+        last = net.train_step(xb, yt, 1e-3)
+    assert last < first - 1.0, (first, last)
+    out1 = net.forward(xb).cpu().numpy()
+    path = str(tmp_path / "mlp.bin")
+    net.save(path)
+    net2 = MLP(seed=99)
+    net2.load(path)
+    out2 = net2.forward(xb).cpu().numpy()
+    np.testing.assert_array_equal(out1, out2)
