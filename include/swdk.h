@@ -85,6 +85,9 @@ typedef struct swdk_stats {
   int32_t nchains;       /* distinct (wave, period list) root chains per column */
   int32_t nslots;        /* kmax of the last call                            */
   float ms_prep, ms_roots, ms_eigen; /* device time of the last call's stages */
+  int64_t proposals_accepted;  /* learned brackets confirmed by the FP64 sign change */
+  int64_t proposals_rejected;  /* learned brackets that fell back to the plain scan  */
+  float ms_proposal;           /* device time of feature extraction + inference  */
 } swdk_stats;
 
 typedef struct swdk_ctx swdk_ctx;
@@ -180,6 +183,50 @@ int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_t
                             const float* d_vs, const float* d_rho, int iflsph, int iwave, int mode, int igr, int kmax,
                             const double* d_t, double* d_cg, int32_t* d_ierr, int refine, double rtol, int sngl,
                             void* stream);
+
+/* ---- learned bracket proposal (no counterpart in the reference) ----------
+ * A small MLP per wave type proposes each root's phase velocity c and a
+ * bracket half-width; the FP64 period equation must change sign across the
+ * bracket with the mode's polarity, otherwise the reference's plain scan
+ * runs.  Only the tight refinement uses proposals; roots are unchanged, the
+ * number of secular-function evaluations drops. */
+typedef struct swdk_mlp swdk_mlp;
+int swdk_mlp_create(swdk_mlp** out, int device, uint64_t seed);
+void swdk_mlp_destroy(swdk_mlp* mlp);
+int64_t swdk_mlp_num_params(const swdk_mlp* mlp);
+int swdk_mlp_get_params(swdk_mlp* mlp, float* host, int64_t n);
+int swdk_mlp_set_params(swdk_mlp* mlp, const float* host, int64_t n);
+int swdk_mlp_get_grads(swdk_mlp* mlp, float* host, int64_t n);
+/* d_x: (M, 320) bf16 features; d_out: (M, 2) float (mu, log sigma) */
+int swdk_mlp_forward(swdk_mlp* mlp, const void* d_x, int M, float* d_out, void* stream);
+int swdk_mlp_infer_rows(swdk_mlp* mlp, const void* d_x, int M, float* d_out2, void* stream);
+/* forward + Gaussian NLL + backward; Adam step when lr > 0 */
+int swdk_mlp_train_step(swdk_mlp* mlp, const void* d_x, const float* d_y, int M, float lr, float* loss_out,
+                        void* stream);
+int swdk_mlp_save(swdk_mlp* mlp, const char* path);
+int swdk_mlp_load(swdk_mlp* mlp, const char* path);
+int swdk_mlp_error_flag(swdk_mlp* mlp, int* flag);
+const char* swdk_mlp_last_error(const swdk_mlp* mlp);
+/* C = A * B^T on the tensor cores: A (M, K), B (N, K) bf16 device, C (M, N)
+ * float; M % 128 == 0, N % 64 == 0, K % 64 == 0. */
+int swdk_gemm_bf16_tn(int M, int N, int K, const void* d_a, const void* d_b, float* d_c, int* d_err, void* stream);
+
+/* Attach proposal networks (either may be NULL); kappa_* scales the
+ * predicted sigma into the bracket half-width of that wave type.  From the
+ * second period of a mode on, the bracket is centred on the previous
+ * period's root plus the predicted change, c(k-1) + mu(k) - mu(k-1); the
+ * first period keeps the plain scan.  NULL/NULL disables proposals.  The
+ * networks must outlive their use by this context. */
+int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double kappa_rayleigh, double kappa_love);
+
+/* Training support: root search only (all root chains of get_1d_kernel)
+ * on device models, then per-slot metadata, the roots and their status, and
+ * features/targets for chosen rows (row = slot * nx*ny + column). */
+int swdk_roots_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
+                      void* stream);
+int swdk_root_slots(swdk_ctx* ctx, int* nslots, int32_t* wave, int32_t* mode, double* period);
+int swdk_last_roots(swdk_ctx* ctx, double* h_c, int32_t* h_status);
+int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, float* d_y, void* stream);
 
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);

@@ -14,9 +14,11 @@
 //   k_eigen  : one block per column, one thread per output slot: sregn96 /
 //              sregnpu / slegn96 / slegnpu passes, sphericity, _ParamConvert
 //              and the empirical chain rule (SurfaceWave.cpp:491-500).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <mutex>
 #include <cstring>
@@ -30,6 +32,9 @@
 using namespace swdk;
 
 namespace {
+
+constexpr int FEAT_NODES = 64, FEAT_DIM = 320;  // proposal network input (see swdk_mlp.cu)
+constexpr double FEAT_C0 = 3.5;                  // phase velocity offset of the network target
 
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
@@ -192,7 +197,8 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
                                               float4* __restrict__ layR, float4* __restrict__ layL,
                                               double2* __restrict__ rab, double2* __restrict__ rrmR,
                                               double2* __restrict__ rrmL, float4* __restrict__ lay0,
-                                              ColInfo* __restrict__ info, float2* __restrict__ chainrule) {
+                                              ColInfo* __restrict__ info, float2* __restrict__ chainrule,
+                                              float4* __restrict__ nodefeat) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   float v[NZMAX], vp[NZMAX], rho[NZMAX], dep[NZMAX];
@@ -213,6 +219,13 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
   while (nw < nz - 1 && v[nw] == 0.0f) ++nw;
   for (int k = nw; k < nz; ++k)
     if (!(v[k] > 0.0f)) valid = false;
+  if (nodefeat) {  // proposal-network input: 64 nodes x (vs, vp, rho, thickness), normalised
+    for (int i = 0; i < FEAT_NODES; ++i) {
+      const int k = i < nz ? i : nz - 1;
+      const float thk = (i < nz - 1) ? dep[i + 1] - dep[i] : 0.0f;
+      nodefeat[(size_t)col * FEAT_NODES + i] = make_float4(v[k] / 4.5f, vp[k] / 8.0f, rho[k] / 3.3f, thk / 5.0f);
+    }
+  }
   for (int k = 0; k < nz; ++k) {
     float drda = 0.0f, dadb = 0.0f;
     brocher_deriv(vp[k], v[k], drda, dadb);
@@ -284,6 +297,57 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// proposal-network rows: row = slot * ncol + col; one warp per row
+//   x[0:64) vs, [64:128) vp, [128:192) rho, [192:256) thickness,
+//   x[256] log(T)/log(100), x[257] (mode-1)/2, zero to 320
+// ---------------------------------------------------------------------------
+__global__ void k_features(int64_t row0, int nrows, int ncol, int64_t rowmax, const float4* __restrict__ slotfeat,
+                           const float4* __restrict__ nodefeat, const int64_t* __restrict__ rowlist,
+                           __nv_bfloat16* __restrict__ x) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nrows) return;
+  const int64_t row = rowlist ? rowlist[w] : row0 + w;
+  if (row < 0 || row >= rowmax) {  // out-of-range request: zero row
+    for (int i = lane; i < FEAT_DIM; i += 32) x[(size_t)w * FEAT_DIM + i] = __float2bfloat16_rn(0.0f);
+    return;
+  }
+  const int s = (int)(row / ncol), col = (int)(row % ncol);
+  const float4 sf = slotfeat[s];
+  const float4* nf = nodefeat + (size_t)col * FEAT_NODES;
+  __nv_bfloat16* xr = x + (size_t)w * FEAT_DIM;
+  for (int i = lane; i < FEAT_NODES; i += 32) {
+    const float4 n = nf[i];
+    xr[i] = __float2bfloat16_rn(n.x);
+    xr[64 + i] = __float2bfloat16_rn(n.y);
+    xr[128 + i] = __float2bfloat16_rn(n.z);
+    xr[192 + i] = __float2bfloat16_rn(n.w);
+  }
+  for (int i = 256 + lane; i < FEAT_DIM; i += 32)
+    xr[i] = __float2bfloat16_rn(i == 256 ? sf.x : i == 257 ? sf.y : 0.0f);
+}
+
+// proposal (c, half-width) from the network output (mu, log sigma)
+__global__ void k_make_prop(int64_t row0, int nrows, const float* __restrict__ out2, double kappa,
+                            float2* __restrict__ prop) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
+  const float mu = out2[2 * i], ls = out2[2 * i + 1];
+  const double c = FEAT_C0 + (double)mu;
+  double hw = kappa * exp(fmin(fmax((double)ls, -12.0), 2.0));
+  hw = fmin(fmax(hw, 2.0e-5 * c), 0.2);
+  prop[row0 + i] = (mu == mu && ls == ls) ? make_float2((float)c, (float)hw) : make_float2(0.0f, 0.0f);
+}
+
+// training targets of chosen rows: y = c_flat - FEAT_C0
+__global__ void k_targets(int n, int64_t rowmax, const int64_t* __restrict__ rows, const double* __restrict__ croot,
+                          float* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t r = rows[i];
+  y[i] = (r >= 0 && r < rowmax) ? (float)(croot[r] - FEAT_C0) : 0.0f;
+}
+
+// ---------------------------------------------------------------------------
 // k_roots: one thread per (column, chain)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const double* __restrict__ periods,
@@ -338,6 +402,7 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   io.st = stp;
   io.stride = cd.np * ncol;
   io.ostride = ncol;
+  io.prop = nullptr;
   ChainState s;
   run_chain(V, P, io, s, active);
   if (active) {
@@ -401,6 +466,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      const ColInfo* __restrict__ info, int refine, double rtol,
                                                      int sngl, int retry, double* __restrict__ croot,
                                                      int32_t* __restrict__ cstat, unsigned int* __restrict__ queue,
+                                                     const float2* __restrict__ prop,
+                                                     int2* __restrict__ retry_list, unsigned int* __restrict__ retry_count,
+                                                     unsigned int retry_cap,
                                                      unsigned long long* __restrict__ nevals) {
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
@@ -409,9 +477,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
   ChainIO io;
   LayerView V;
   ChainDesc cd;
-  int col = 0;
+  int col = 0, item_of = 0;
   bool have = false, exhausted = false;
-  unsigned long long ev_r = 0, ev_l = 0, lay_r = 0, lay_l = 0;
+  unsigned long long ev_r = 0, ev_l = 0, lay_r = 0, lay_l = 0, pok = 0, pfail = 0;
   io.c = cbuf;
   io.cb = cbbuf;
   for (;;) {
@@ -421,6 +489,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         if (exhausted) break;
         const unsigned int item = atomicAdd(queue, 1u);
         if (item >= (unsigned int)nitems) { exhausted = true; break; }
+        item_of = (int)item;
         cd = chains[order[item / ncol]];
         col = item % ncol;
         const ColInfo ci = info[col];
@@ -452,6 +521,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         io.st = stp;
         io.stride = cd.np * ncol;
         io.ostride = ncol;
+        io.prop = prop ? prop + (size_t)cd.out_off * ncol + col : nullptr;
         chain_init(s);
         have = true;
       }
@@ -461,8 +531,21 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
       if (s.iterlim)
         for (int i = 0; i < cd.nmode * cd.np; ++i)
           if (io.st[(size_t)i * ncol] == ST_OK) io.st[(size_t)i * ncol] = ST_ITER_LIMIT;
+      if (retry == RETRY_DEFERRED && s.ierr != 0) {
+        // failed slots become single-period work items for k_retry
+        for (int m = 1; m <= cd.nmode; ++m)
+          for (int k = 1; k <= cd.np; ++k) {
+            const double v = out_at(io, m, k);
+            if (v == 0.0 || !(v == v)) {
+              const unsigned int r = atomicAdd(retry_count, 1u);
+              if (r < retry_cap) retry_list[r] = make_int2(item_of, (m << 16) | k);
+            }
+          }
+      }
       if (cd.iwave == 2) { ev_r += s.nevals; lay_r += (unsigned long long)s.nevals * V.L; }
       else { ev_l += s.nevals; lay_l += (unsigned long long)s.nevals * V.L; }
+      pok += s.nprop_ok;
+      pfail += s.nprop_fail;
       have = false;
     }
     if (__ballot_sync(0xffffffffu, need) == 0u) break;
@@ -477,9 +560,113 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
     e += __shfl_down_sync(0xffffffffu, e, o);
     lay_r += __shfl_down_sync(0xffffffffu, lay_r, o);
     lay_l += __shfl_down_sync(0xffffffffu, lay_l, o);
+    pok += __shfl_down_sync(0xffffffffu, pok, o);
+    pfail += __shfl_down_sync(0xffffffffu, pfail, o);
   }
   if ((threadIdx.x & 31) == 0 && nevals) {
     atomicAdd(nevals, e);
+    atomicAdd(nevals + 1, lay_r);
+    atomicAdd(nevals + 2, lay_l);
+    atomicAdd(nevals + 3, pok);
+    atomicAdd(nevals + 4, pfail);
+  }
+}
+
+// k_retry: the deferred single-period retries (surfdisp.cpp:94-109), one
+// per thread; a warp takes 32 records at a time
+__global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const int* __restrict__ order,
+                                                               const ChainDesc* __restrict__ chains,
+                                                               const double* __restrict__ periods,
+                                                               const float4* __restrict__ layR,
+                                                               const float4* __restrict__ layL,
+                                                               const double2* __restrict__ rab,
+                                                               const double2* __restrict__ rrmR,
+                                                               const double2* __restrict__ rrmL,
+                                                               const ColInfo* __restrict__ info, int refine,
+                                                               double rtol, int sngl, double* __restrict__ croot,
+                                                               int32_t* __restrict__ cstat,
+                                                               const int2* __restrict__ retry_list,
+                                                               const unsigned int* __restrict__ retry_count,
+                                                               unsigned int retry_cap, unsigned int* __restrict__ queue,
+                                                               unsigned long long* __restrict__ nevals) {
+  double cbuf[KMAX_CHAIN];
+  double cbbuf[KMAX_CHAIN + 24];
+  const unsigned int n = min(*retry_count, retry_cap);
+  const int lane = threadIdx.x & 31;
+  unsigned long long ev_r = 0, lay_r = 0, lay_l = 0;
+  for (;;) {
+    unsigned int base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const unsigned int r = base + lane;
+    const bool active = r < n;
+    ChainState s;
+    ChainParams P;
+    ChainIO io;
+    LayerView V;
+    ChainDesc cd = chains[order[0]];
+    int col = 0, m = 1, k = 1;
+    if (active) {
+      const int2 rec = retry_list[r];
+      cd = chains[order[rec.x / ncol]];
+      col = rec.x % ncol;
+      m = rec.y >> 16;
+      k = rec.y & 0xffff;
+    }
+    const ColInfo ci = info[col];
+    V.lay = (cd.iwave == 2) ? layR : layL;
+    V.rab = rab;
+    V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
+    V.ncol = ncol;
+    V.col = col;
+    V.L = ci.L;
+    V.llw = ci.llw;
+    P.t = periods + cd.t_off;
+    P.kmax = cd.np;
+    P.nmode = cd.nmode;
+    P.igr = cd.igr;
+    P.iwave = cd.iwave;
+    P.refine = refine;
+    P.rtol = rtol;
+    P.sngl = sngl;
+    P.cc = ci.cc;
+    P.betmx = ci.betmx;
+    P.retry = RETRY_ONE;
+    io.c = cbuf;
+    io.cb = cbbuf;
+    io.out = croot + (size_t)cd.out_off * ncol + col;
+    io.st = cstat + (size_t)cd.out_off * ncol + col;
+    io.stride = cd.np * ncol;
+    io.ostride = ncol;
+    io.prop = nullptr;
+    // run_chain's warp loop with a retry start state
+    chain_init_retry(s, m, k);
+    bool act = active;
+    for (;;) {
+      const bool need = act && chain_advance(s, P, io);
+      if (!need) act = false;
+      if (__ballot_sync(0xffffffffu, need) == 0u) break;
+      if (need) {
+        s.last = secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega);
+        s.nevals++;
+        s.phase = s.next;
+      }
+    }
+    if (active) {
+      if (s.iterlim && st_at(io, m, k) != ST_NO_ROOT) st_at(io, m, k) = ST_ITER_LIMIT;
+      ev_r += s.nevals;
+      if (cd.iwave == 2) lay_r += (unsigned long long)s.nevals * V.L;
+      else lay_l += (unsigned long long)s.nevals * V.L;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ev_r += __shfl_down_sync(0xffffffffu, ev_r, o);
+    lay_r += __shfl_down_sync(0xffffffffu, lay_r, o);
+    lay_l += __shfl_down_sync(0xffffffffu, lay_l, o);
+  }
+  if (lane == 0 && nevals && ev_r) {
+    atomicAdd(nevals, ev_r);
     atomicAdd(nevals + 1, lay_r);
     atomicAdd(nevals + 2, lay_l);
   }
@@ -788,8 +975,11 @@ struct Plan {
   std::vector<ChainDesc> chains;
   std::vector<double> periods;
   std::vector<SlotDesc> slots;
-  int kmax = 0, nroot = 0;
-  DevBuf d_chains, d_periods, d_slots;
+  std::vector<float4> rootfeat;  // per root slot: (log T / log 100, mode / 2, Rayleigh, 0)
+  std::vector<int> rootwave, rootmode;
+  std::vector<double> rootperiod;
+  int kmax = 0, nroot = 0, nrootR = 0;  // root slots [0, nrootR) are Rayleigh
+  DevBuf d_chains, d_periods, d_slots, d_rootfeat;
 };
 
 int nt_of(const double* col, int ntmax) {
@@ -812,7 +1002,14 @@ struct swdk_ctx {
   DevBuf layR, layL, rab, rrmR, rrmL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr, queue;
   int roots_blocks = 0;
   DevBuf in_vs, in_vp, in_rho, out_vc, out_vout, out_kernel, out_status, in_misc;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // stage marks; ev[4]: call done
+  // learned bracket proposals
+  swdk_mlp* net[2] = {nullptr, nullptr};  // 0: Rayleigh, 1: Love
+  double kappa[2] = {4.0, 4.0};
+  DevBuf nodefeat, pfeat, pout, prop;
+  DevBuf retry_list, retry_ctr;  // deferred retries: records and {count, queue}
+  int last_ncol = 0, last_path = -1;
+  // stage marks: 0 start, 1 prep, 5 proposals, 2 roots, 3 eigen, 4 call done
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   unsigned long long* h_nevals = nullptr;
   swdk_stats stats;
   bool stats_pending = false;
@@ -883,12 +1080,34 @@ int build_plan(swdk_ctx* ctx, int path) {
     }
   }
   P.kmax = idx;
-  int off = 0;
   for (size_t i = 0; i < P.chains.size(); ++i) {
     P.chains[i].t_off = (int)P.periods.size();
     P.periods.insert(P.periods.end(), lists[i].begin(), lists[i].end());
-    P.chains[i].out_off = off;
-    off += P.chains[i].nmode * P.chains[i].np;
+  }
+  // root slots: Rayleigh chains first, so one proposal network covers a
+  // contiguous row range
+  int off = 0;
+  P.rootfeat.clear();
+  P.rootwave.clear();
+  P.rootmode.clear();
+  P.rootperiod.clear();
+  for (int w = 2; w >= 1; --w) {
+    for (size_t i = 0; i < P.chains.size(); ++i) {
+      ChainDesc& d = P.chains[i];
+      if (d.iwave != w) continue;
+      d.out_off = off;
+      off += d.nmode * d.np;
+      for (int m = 0; m < d.nmode; ++m)
+        for (int k = 0; k < d.np; ++k) {
+          const double t = lists[i][k];
+          P.rootfeat.push_back(make_float4((float)(std::log(t) / std::log(100.0)), 0.5f * (float)m,
+                                           w == 2 ? 1.0f : 0.0f, 0.0f));
+          P.rootwave.push_back(w);
+          P.rootmode.push_back(m);
+          P.rootperiod.push_back(t);
+        }
+    }
+    if (w == 2) P.nrootR = off;
   }
   P.nroot = off;
   auto rslot = [&](int ch, int mode, int k) { return ch < 0 ? -1 : P.chains[ch].out_off + mode * P.chains[ch].np + k; };
@@ -914,6 +1133,8 @@ int build_plan(swdk_ctx* ctx, int path) {
   CK(P.d_chains.ensure(P.chains.size() * sizeof(ChainDesc)));
   CK(P.d_periods.ensure(P.periods.size() * sizeof(double)));
   CK(P.d_slots.ensure(P.slots.size() * sizeof(SlotDesc)));
+  CK(P.d_rootfeat.ensure(P.rootfeat.size() * sizeof(float4)));
+  CK(cudaMemcpy(P.d_rootfeat.p, P.rootfeat.data(), P.rootfeat.size() * sizeof(float4), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(P.d_chains.p, P.chains.data(), P.chains.size() * sizeof(ChainDesc), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(P.d_periods.p, P.periods.data(), P.periods.size() * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(P.d_slots.p, P.slots.data(), P.slots.size() * sizeof(SlotDesc), cudaMemcpyHostToDevice));
@@ -931,11 +1152,51 @@ int ensure_plans(swdk_ctx* ctx) {
   return SWDK_OK;
 }
 
-// model preparation + roots + eigen for one call on device pointers
+constexpr int PROP_CHUNK = 262144;  // proposal rows per inference launch group (multiple of 128)
+
+bool proposals_on(const swdk_ctx* ctx) { return ctx->cfg.refine == 1 && (ctx->net[0] || ctx->net[1]); }
+
+// features -> network -> (c, half-width) for every root row of plan P
+int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
+  const int64_t nrows = (int64_t)P.nroot * ncol;
+  CK(ctx->prop.ensure((size_t)nrows * sizeof(float2)));
+  CK(ctx->pfeat.ensure((size_t)PROP_CHUNK * FEAT_DIM * sizeof(__nv_bfloat16)));
+  CK(ctx->pout.ensure((size_t)PROP_CHUNK * 2 * sizeof(float)));
+  const int64_t bound[3] = {0, (int64_t)P.nrootR * ncol, nrows};
+  for (int w = 0; w < 2; ++w) {
+    const int64_t r0 = bound[w], r1 = bound[w + 1];
+    if (r1 <= r0) continue;
+    if (!ctx->net[w]) {
+      CK(cudaMemsetAsync(ctx->prop.as<float2>() + r0, 0, (size_t)(r1 - r0) * sizeof(float2), st));
+      continue;
+    }
+    for (int64_t a = r0; a < r1; a += PROP_CHUNK) {
+      const int n = (int)std::min<int64_t>(PROP_CHUNK, r1 - a);
+      const int m = (n + 127) / 128 * 128;
+      if (m > n)  // padding rows of the last tile: finite zeros
+        CK(cudaMemsetAsync(ctx->pfeat.as<__nv_bfloat16>() + (size_t)n * FEAT_DIM, 0,
+                           (size_t)(m - n) * FEAT_DIM * sizeof(__nv_bfloat16), st));
+      k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(),
+                                              ctx->nodefeat.as<float4>(), nullptr, ctx->pfeat.as<__nv_bfloat16>());
+      CK(cudaGetLastError());
+      int r = swdk_mlp_infer_rows(ctx->net[w], ctx->pfeat.p, m, ctx->pout.as<float>(), st);
+      if (r) return fail(ctx, r, std::string("proposal inference: ") + swdk_mlp_last_error(ctx->net[w]));
+      k_make_prop<<<(n + 255) / 256, 256, 0, st>>>(a, n, ctx->pout.as<float>(), ctx->kappa[w],
+                                                    ctx->prop.as<float2>());
+      CK(cudaGetLastError());
+    }
+  }
+  return SWDK_OK;
+}
+
+// model preparation + (proposals) + roots + (eigen) for one call on device
+// pointers; path 0 get_1d_kernel, 1 get_2d_map, 2 roots of path 0 only
 int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
                const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
                cudaStream_t st) {
-  if (nx <= 0 || ny <= 0 || !d_vs || !d_vc || !d_vout || (path == 0 && !d_kernel))
+  const bool roots_only = (path == 2);
+  if (roots_only) path = 0;
+  if (nx <= 0 || ny <= 0 || !d_vs || (!roots_only && (!d_vc || !d_vout || (path == 0 && !d_kernel))))
     return fail(ctx, SWDK_E_ARG, "bad arguments");
   if ((d_vp == nullptr) != (d_rho == nullptr)) return fail(ctx, SWDK_E_ARG, "vp and rho must both be given or both NULL");
   if ((int)ctx->depth.size() != nz) return fail(ctx, SWDK_E_NODEPTH, "nz does not match swdk_set_depth");
@@ -945,6 +1206,8 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   Plan& P = ctx->plan[path];
   const int ncol = nx * ny;
   const int Lmax = 4 * nz - 3;
+  const bool useprop = proposals_on(ctx);
+  const bool wantfeat = useprop || roots_only;
   CK(ctx->layR.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->layL.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->rab.ensure((size_t)Lmax * ncol * sizeof(double2)));
@@ -956,18 +1219,24 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(ctx->chainrule.ensure((size_t)nz * ncol * sizeof(float2)));
   CK(ctx->croot.ensure((size_t)P.nroot * ncol * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)P.nroot * ncol * sizeof(int32_t)));
-  CK(ctx->nevals.ensure(3 * sizeof(unsigned long long)));
+  CK(ctx->nevals.ensure(5 * sizeof(unsigned long long)));
+  if (wantfeat) CK(ctx->nodefeat.ensure((size_t)ncol * FEAT_NODES * sizeof(float4)));
   CK(ctx->depth_d.ensure((size_t)nz * sizeof(float)));
   CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(ctx->nevals.p, 0, 3 * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
                                              ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                             ctx->chainrule.as<float2>());
+                                             ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
+  if (useprop) {
+    r = run_proposals(ctx, P, ncol, st);
+    if (r) return r;
+  }
+  CK(cudaEventRecord(ctx->ev[5], st));
   if (ctx->roots_blocks == 0) {
     int dev = 0, nsm = 0, per = 0;
     CK(cudaGetDevice(&dev));
@@ -977,28 +1246,46 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   }
   const int nitems = (int)P.chains.size() * ncol;
   const int rblocks = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : ctx->roots_blocks;
+  const unsigned int rcap = (unsigned int)std::min<size_t>((size_t)P.nroot * ncol, 0x7fffffffu);
+  CK(ctx->retry_list.ensure((size_t)rcap * sizeof(int2)));
+  CK(ctx->retry_ctr.ensure(2 * sizeof(unsigned int)));
   CK(cudaMemsetAsync(ctx->queue.p, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(ctx->retry_ctr.p, 0, 2 * sizeof(unsigned int), st));
+  unsigned int* rctr = ctx->retry_ctr.as<unsigned int>();
   k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, 0, st>>>(
       ncol, nitems, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
       ctx->layL.as<float4>(), ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
-      ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, 1, ctx->croot.as<double>(),
-      ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(), ctx->nevals.as<unsigned long long>());
+      ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
+      ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(),
+      useprop ? ctx->prop.as<float2>() : nullptr, ctx->retry_list.as<int2>(), rctr, rcap,
+      ctx->nevals.as<unsigned long long>());
+  CK(cudaGetLastError());
+  k_retry<<<rblocks, 128, 0, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
+                                   ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->rab.as<double2>(),
+                                   ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(), ctx->info.as<ColInfo>(),
+                                   ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, ctx->croot.as<double>(),
+                                   ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
+                                   ctx->nevals.as<unsigned long long>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[2], st));
-  const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
-  const int nslots = (int)P.slots.size();
-  const int et = std::min(128, ((nslots + 31) / 32) * 32);
-  k_eigen<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                  ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), nslots,
-                                  ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
-                                  d_vout, d_kernel, d_status);
-  CK(cudaGetLastError());
+  if (!roots_only) {
+    const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
+    const int nslots = (int)P.slots.size();
+    const int et = std::min(128, ((nslots + 31) / 32) * 32);
+    k_eigen<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                    ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), nslots,
+                                    ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
+                                    d_vout, d_kernel, d_status);
+    CK(cudaGetLastError());
+  }
   CK(cudaEventRecord(ctx->ev[3], st));
-  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(ctx->ev[4], st));
   ctx->stats_pending = true;
   ctx->stats.nchains = (int)P.chains.size();
   ctx->stats.nslots = P.kmax;
+  ctx->last_ncol = ncol;
+  ctx->last_path = roots_only ? 2 : path;
   return SWDK_OK;
 }
 
@@ -1009,8 +1296,11 @@ void collect_stats(swdk_ctx* ctx) {
   ctx->stats.secular_evals = (int64_t)ctx->h_nevals[0];
   ctx->stats.layer_evals_rayleigh = (int64_t)ctx->h_nevals[1];
   ctx->stats.layer_evals_love = (int64_t)ctx->h_nevals[2];
+  ctx->stats.proposals_accepted = (int64_t)ctx->h_nevals[3];
+  ctx->stats.proposals_rejected = (int64_t)ctx->h_nevals[4];
   cudaEventElapsedTime(&ctx->stats.ms_prep, ctx->ev[0], ctx->ev[1]);
-  cudaEventElapsedTime(&ctx->stats.ms_roots, ctx->ev[1], ctx->ev[2]);
+  cudaEventElapsedTime(&ctx->stats.ms_proposal, ctx->ev[1], ctx->ev[5]);
+  cudaEventElapsedTime(&ctx->stats.ms_roots, ctx->ev[5], ctx->ev[2]);
   cudaEventElapsedTime(&ctx->stats.ms_eigen, ctx->ev[2], ctx->ev[3]);
 }
 
@@ -1093,14 +1383,14 @@ int swdk_create(swdk_ctx** out, const swdk_config* cfg) {
   memset(&ctx->stats, 0, sizeof(ctx->stats));
   cudaError_t e = cudaSetDevice(ctx->cfg.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-  for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_nevals, 3 * sizeof(unsigned long long));
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_nevals, 5 * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     fprintf(stderr, "swdk_create: %s\n", cudaGetErrorString(e));
     swdk_destroy(ctx);
     return SWDK_E_CUDA;
   }
-  ctx->h_nevals[0] = ctx->h_nevals[1] = ctx->h_nevals[2] = 0;
+  for (int i = 0; i < 5; ++i) ctx->h_nevals[i] = 0;
   *out = ctx;
   return SWDK_OK;
 }
@@ -1111,14 +1401,18 @@ void swdk_destroy(swdk_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->layR, &ctx->layL, &ctx->lay0, &ctx->info, &ctx->chainrule, &ctx->croot, &ctx->cstat,
                     &ctx->nevals, &ctx->depth_d, &ctx->ierr, &ctx->in_vs, &ctx->in_vp, &ctx->in_rho,
-                    &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc};
+                    &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc,
+                    &ctx->rab, &ctx->rrmR, &ctx->rrmL, &ctx->queue, &ctx->nodefeat, &ctx->pfeat,
+                    &ctx->pout, &ctx->prop, &ctx->retry_list, &ctx->retry_ctr};
   for (DevBuf* b : bufs) b->release();
   for (int p = 0; p < 2; ++p) {
     ctx->plan[p].d_chains.release();
     ctx->plan[p].d_periods.release();
     ctx->plan[p].d_slots.release();
+    ctx->plan[p].d_order.release();
+    ctx->plan[p].d_rootfeat.release();
   }
-  for (int i = 0; i < 5; ++i)
+  for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1218,8 +1512,8 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(ctx->croot.ensure((size_t)mode * kmax * nm * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)mode * kmax * nm * sizeof(int32_t)));
   CK(ctx->ierr.ensure(nm * sizeof(int32_t)));
-  CK(ctx->nevals.ensure(3 * sizeof(unsigned long long)));
-  CK(cudaMemsetAsync(ctx->nevals.p, 0, 3 * sizeof(unsigned long long), st));
+  CK(ctx->nevals.ensure(5 * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_in, d_in + nin, d_in + 2 * nin,
                                                        d_in + 3 * nin, iflsph, ctx->layR.as<float4>(),
@@ -1228,6 +1522,7 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
                                                        ctx->info.as<ColInfo>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
+  CK(cudaEventRecord(ctx->ev[5], st));
   k_roots<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(nmodel, d_ch, d_t, ctx->layR.as<float4>(),
                                                          ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                                          ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, 0,
@@ -1242,7 +1537,7 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaMemcpyAsync(tmp.data(), ctx->croot.as<double>() + (size_t)(mode - 1) * kmax * nm,
                      (size_t)kmax * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (ierr) CK(cudaMemcpyAsync(ierr, ctx->ierr.p, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(ctx->ev[4], st));
   ctx->stats_pending = true;
   CK(cudaStreamSynchronize(st));
@@ -1263,6 +1558,68 @@ int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, co
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
   k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, d_nnz, d_indices, d_values);
   CK(cudaGetLastError());
+  return SWDK_OK;
+}
+
+int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double kappa_rayleigh, double kappa_love) {
+  if (!ctx || !(kappa_rayleigh > 0.0) || !(kappa_rayleigh < 1.0e3) || !(kappa_love > 0.0) || !(kappa_love < 1.0e3))
+    return fail(ctx, SWDK_E_ARG, "bad arguments");
+  ctx->net[0] = rayleigh;
+  ctx->net[1] = love;
+  ctx->kappa[0] = kappa_rayleigh;
+  ctx->kappa[1] = kappa_love;
+  return SWDK_OK;
+}
+
+int swdk_roots_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
+                      void* stream) {
+  if (!ctx) return SWDK_E_ARG;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  return run_device(ctx, 2, nx, ny, nz, d_vs, d_vp, d_rho, nullptr, nullptr, nullptr, nullptr, st);
+}
+
+int swdk_root_slots(swdk_ctx* ctx, int* nslots, int32_t* wave, int32_t* mode, double* period) {
+  if (!ctx || !nslots) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  int r = ensure_plans(ctx);
+  if (r) return r;
+  const Plan& P = ctx->plan[0];
+  *nslots = P.nroot;
+  for (int i = 0; i < P.nroot; ++i) {
+    if (wave) wave[i] = P.rootwave[i];
+    if (mode) mode[i] = P.rootmode[i];
+    if (period) period[i] = P.rootperiod[i];
+  }
+  return SWDK_OK;
+}
+
+int swdk_last_roots(swdk_ctx* ctx, double* h_c, int32_t* h_status) {
+  if (!ctx || ctx->last_ncol <= 0 || ctx->last_path < 0) return fail(ctx, SWDK_E_ARG, "no root search ran yet");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const Plan& P = ctx->plan[ctx->last_path == 1 ? 1 : 0];
+  const size_t n = (size_t)P.nroot * ctx->last_ncol;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaDeviceSynchronize());
+  if (h_c) CK(cudaMemcpy(h_c, ctx->croot.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (h_status) CK(cudaMemcpy(h_status, ctx->cstat.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return SWDK_OK;
+}
+
+int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, float* d_y, void* stream) {
+  if (!ctx || n < 0 || (n > 0 && (!d_rows || !d_x))) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  if (ctx->last_path != 2) return fail(ctx, SWDK_E_ARG, "swdk_training_rows needs a preceding swdk_roots_device");
+  if (n == 0) return SWDK_OK;
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const Plan& P = ctx->plan[0];
+  const int64_t rowmax = (int64_t)P.nroot * ctx->last_ncol;
+  k_features<<<(n + 7) / 8, 256, 0, st>>>(0, n, ctx->last_ncol, rowmax, P.d_rootfeat.as<float4>(),
+                                          ctx->nodefeat.as<float4>(), d_rows, (__nv_bfloat16*)d_x);
+  CK(cudaGetLastError());
+  if (d_y) {
+    k_targets<<<(n + 255) / 256, 256, 0, st>>>(n, rowmax, d_rows, ctx->croot.as<double>(), d_y);
+    CK(cudaGetLastError());
+  }
   return SWDK_OK;
 }
 

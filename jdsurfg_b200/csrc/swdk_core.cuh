@@ -512,7 +512,7 @@ enum Phase : int {
   PH_CHAIN_START, PH_PERIOD_START, PH_GS_START, PH_GS_FIRST, PH_SCAN, PH_SCAN_GOT, PH_REFINE_START,
   PH_NEV_A, PH_NEV_TOP, PH_NEV_BODY_GOT, PH_NEV_BODY, PH_NEV_HALF_GOT, PH_NEV_NEV_GOT, PH_BRENT_STEP,
   PH_BRENT_GOT, PH_REFINE_DONE, PH_GS_OK, PH_GS_FAIL, PH_PERIOD_OUT, PH_FAIL, PH_MODE_END, PH_CHAIN_END,
-  PH_RETRY_NEXT, PH_DONE
+  PH_RETRY_NEXT, PH_PROP_LO, PH_PROP_HI, PH_PROP_CHECK, PH_PROP_DOWN, PH_PROP_DOWN_GOT, PH_DONE
 };
 
 struct ChainParams {
@@ -526,7 +526,7 @@ struct ChainParams {
   int sngl;         // REAL*4 output like the reference
   double cc;        // start value 0.95*0.90*c_R(slowest layer), surfdisp96.f:206-226
   float betmx;      // largest shear velocity of the flattened model
-  int retry;        // 1: surfdisp()'s single-period retry (surfdisp.cpp:94-109)
+  int retry;        // surfdisp()'s single-period retries (surfdisp.cpp:94-109): RETRY_*
 };
 
 struct ChainState {
@@ -544,6 +544,9 @@ struct ChainState {
   double c3, del3, ra_, fa, rb_, fb, rc_, fc, rd, re;
   int nev, nctrl, m;
   int nscan;
+  // learned proposals
+  double plo, phi, fplo, c1s, del1s;
+  int pm, nprop_ok, nprop_fail;
   // retries
   int sub, rq_m, rq_k, sub_ierr;
   double sub_out;
@@ -559,7 +562,14 @@ struct ChainIO {
   double* out;  // out[(iq-1)*stride + (k-1)*ostride]
   int stride, ostride;
   int32_t* st;  // status, same addressing as out
+  const float2* prop;  // learned (c, half-width) per (mode, period), same addressing; may be null
 };
+
+// Retries of failed periods (surfdisp.cpp:94-109): none; inline, one after
+// the other at the end of the chain; deferred, i.e. the caller collects the
+// failed slots of a chain with ierr != 0 and runs each as its own work item;
+// one such item (a single-period chain for slot (rq_m, rq_k)).
+constexpr int RETRY_NONE = 0, RETRY_INLINE = 1, RETRY_DEFERRED = 2, RETRY_ONE = 3;
 
 constexpr double ONE_DC = 1.0e-2;  // surfdisp96 "one"
 constexpr double ONEA = 1.5;       // dble(sone0)
@@ -574,13 +584,61 @@ SWDK_HD int32_t& st_at(const ChainIO& io, int iq, int k) {
   return io.st[(size_t)(iq - 1) * io.stride + (size_t)(k - 1) * io.ostride];
 }
 
+// a single-period retry of slot (mode m, period k) as its own chain
+SWDK_HD void chain_init_retry(ChainState& s, int m, int k);
+
 SWDK_HD void chain_init(ChainState& s) {
   s.phase = PH_CHAIN_START;
+  s.nprop_ok = 0;
+  s.nprop_fail = 0;
   s.sub = 0;
   s.iterlim = 0;
   s.nevals = 0;
   s.last = 0.0;
   s.del1st = 0.0;
+}
+
+SWDK_HD void chain_init_retry(ChainState& s, int m, int k) {
+  chain_init(s);
+  s.sub = 1;
+  s.rq_m = m;
+  s.rq_k = k;
+}
+
+// Learned proposals live on the reference's scan grid g_j = c1 + j*dc
+// (surfdisp96.f:452-470).  For period k > 1 of a mode, once the scan start
+// c1 has been evaluated and the scan goes upward, the network's anchored
+// estimate
+//   c* = c(k-1) + (mu(k) - mu(k-1))
+// (a bias of the network that is smooth in period cancels) names the grid
+// cell [g_m, g_m+1] expected to hold the root.  f is evaluated at both cell
+// ends: a sign change from the sign of f(c1) to the opposite one is the
+// cell the scan would have reached; otherwise the scan walks from that cell
+// up or down, one grid step at a time, to the sign change.  The cell and
+// hence the refinement are the plain scan's own.  The stretch [c1, g_m]
+// is not walked step by step, so the proposal is used only where that
+// saves steps (m >= 2) and the stretch is short: m*dc <= PROP_GAP_PER_S * T.
+constexpr double PROP_GAP_PER_S = 0.01;
+
+SWDK_HD bool proposal_cell(const ChainState& s, const ChainParams& P, const ChainIO& io, int& m) {
+  if (!io.prop || s.sub || P.igr > 0 || P.refine != 1 || s.k < 2 || s.gpass != 0 || s.idir <= 0) return false;
+  const size_t base = (size_t)(s.iq - 1) * io.stride;
+  const float2 pr = io.prop[base + (size_t)(s.k - 1) * io.ostride];
+  const float2 pp = io.prop[base + (size_t)(s.k - 2) * io.ostride];
+  if (!(pr.y > 0.0f) || !(pr.y <= 0.25f) || !(pp.y > 0.0f)) return false;
+  const double cs = io.c[s.k - 2] + ((double)pr.x - (double)pp.x);
+  const double x = (cs - s.c1) / DC;
+  if (!(x >= 2.0) || !(x < 1.0e4)) return false;
+  m = (int)floor(x);
+  if ((double)m * DC > PROP_GAP_PER_S * s.t1) return false;
+  return s.c1 + (double)(m + 1) * DC < (double)P.betmx + DC;
+}
+
+// grid point c1 + j*dc, accumulated like the scan does
+SWDK_HD double scan_grid(double c1, int j) {
+  double c = c1;
+  for (int i = 0; i < j; ++i) c = c + DC;
+  return c;
 }
 
 // request a secular-function value at c; continue with phase nxt
@@ -634,6 +692,55 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
         s.phase = PH_GS_START;
         break;
       }
+      case PH_PROP_LO: {
+        SWDK_REQ(s.plo, PH_PROP_HI);
+      }
+      case PH_PROP_HI: {
+        s.fplo = s.last;
+        SWDK_REQ(s.phi, PH_PROP_CHECK);
+      }
+      case PH_PROP_CHECK: {
+        const double fphi = s.last;
+        const bool lo_same = dsign1(s.fplo) == dsign1(s.del1), hi_same = dsign1(fphi) == dsign1(s.del1);
+        if (lo_same && !hi_same) {  // the cell of the sign change
+          s.nprop_ok++;
+          s.c1 = s.plo; s.del1 = s.fplo; s.c2 = s.phi; s.del2 = fphi;
+          s.phase = PH_REFINE_START;
+        } else if (lo_same) {  // root above the cell: scan on upward from g_m+1
+          s.nprop_ok++;
+          s.c1 = s.phi; s.del1 = fphi;
+          s.phase = PH_SCAN;
+        } else if (!hi_same) {  // root below the cell: walk down from g_m
+          s.nprop_ok++;
+          s.c2 = s.plo; s.del2 = s.fplo;
+          s.pm = s.pm - 1;
+          s.phase = PH_PROP_DOWN;
+        } else {  // two sign changes inside one cell: plain scan from c1
+          s.nprop_fail++;
+          s.phase = PH_SCAN;
+        }
+        break;
+      }
+      case PH_PROP_DOWN: {  // c2 = g_pm+1 has the opposite sign; try g_pm
+        if (s.pm <= 0) {  // cell [c1, g_1]; f(c1) is known
+          s.c1 = s.c1s; s.del1 = s.del1s;
+          s.phase = PH_REFINE_START;
+          break;
+        }
+        s.plo = scan_grid(s.c1s, s.pm);
+        SWDK_REQ(s.plo, PH_PROP_DOWN_GOT);
+      }
+      case PH_PROP_DOWN_GOT: {
+        if (dsign1(s.last) == dsign1(s.del1s)) {  // sign change in [g_pm, g_pm+1]
+          s.c1 = s.plo; s.del1 = s.last;
+          s.phase = PH_REFINE_START;
+        } else {
+          s.c2 = s.plo; s.del2 = s.last;
+          s.pm = s.pm - 1;
+          s.phase = PH_PROP_DOWN;
+        }
+        break;
+      }
       case PH_GS_START: {  // getsol entry (surfdisp96.f:439-451)
         s.omega = TWOPI / s.t1;
         s.nscan = 0;
@@ -647,6 +754,15 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
         else if (plmn >= 0.0) s.idir = 1;
         else s.idir = -1;
         s.phase = PH_SCAN;
+        int m;
+        if (proposal_cell(s, P, io, m)) {
+          s.c1s = s.c1;
+          s.del1s = s.del1;
+          s.pm = m;
+          s.plo = scan_grid(s.c1, m);
+          s.phi = s.plo + DC;
+          s.phase = PH_PROP_LO;
+        }
         break;
       }
       case PH_SCAN: {  // label 1000
@@ -855,10 +971,10 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
           out_at(io, s.rq_m, s.rq_k) = ok ? v : 0.0;
           st_at(io, s.rq_m, s.rq_k) = ok ? ST_RETRIED : ST_NO_ROOT;
           s.rq_k = s.rq_k + 1;
-          s.phase = PH_RETRY_NEXT;
+          s.phase = (P.retry == RETRY_ONE) ? PH_DONE : PH_RETRY_NEXT;
           break;
         }
-        if (s.ierr == 0 || !P.retry) { s.phase = PH_DONE; break; }
+        if (s.ierr == 0 || P.retry != RETRY_INLINE) { s.phase = PH_DONE; break; }
         s.rq_m = 1; s.rq_k = 1;
         s.phase = PH_RETRY_NEXT;
         break;

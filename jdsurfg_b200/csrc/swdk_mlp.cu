@@ -288,6 +288,10 @@ struct swdk_mlp {
   __nv_bfloat16 *xin = nullptr, *h[MLP_LAYERS] = {}, *dz[MLP_LAYERS] = {}, *xt = nullptr, *dzt = nullptr,
                 *dh = nullptr;
   float *z[MLP_LAYERS] = {}, *out = nullptr, *y = nullptr, *loss = nullptr, *gscr = nullptr;
+  // inference: ping-pong activations and the final pre-activation
+  int icap = 0;
+  __nv_bfloat16 *ia = nullptr, *ib = nullptr;
+  float* iz = nullptr;
   int* err = nullptr;
   cudaStream_t stream = nullptr;
   std::string msg;
@@ -422,6 +426,9 @@ void swdk_mlp_destroy(swdk_mlp* p) {
     if (p->dz[l]) cudaFree(p->dz[l]);
     if (p->z[l]) cudaFree(p->z[l]);
   }
+  if (p->ia) cudaFree(p->ia);
+  if (p->ib) cudaFree(p->ib);
+  if (p->iz) cudaFree(p->iz);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -452,6 +459,45 @@ int swdk_gemm_bf16_tn(int M, int N, int K, const void* d_a, const void* d_b, flo
   k_gemm_tn<<<grid, 128, 0, (cudaStream_t)stream>>>(M, N, K, (const __nv_bfloat16*)d_a, K, (const __nv_bfloat16*)d_b,
                                                      K, nullptr, 0, d_c, nullptr, N, d_err);
   return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
+}
+
+// inference on device features x (M x 320 bf16, M a multiple of 128) ->
+// out2 (M x 2 fp32: mu, log sigma); activations ping-pong in bf16
+int swdk_mlp_infer_rows(swdk_mlp* p, const void* d_x, int M, float* d_out2, void* stream) {
+  if (!p || !d_x || !d_out2 || M <= 0 || M % TM) return SWDK_E_ARG;
+  MCK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  if (M > p->icap) {
+    if (p->ia) cudaFree(p->ia);
+    if (p->ib) cudaFree(p->ib);
+    if (p->iz) cudaFree(p->iz);
+    p->ia = p->ib = nullptr;
+    p->iz = nullptr;
+    p->icap = 0;
+    MCK(cudaMalloc(&p->ia, (size_t)M * MLP_H * sizeof(__nv_bfloat16)));
+    MCK(cudaMalloc(&p->ib, (size_t)M * MLP_H * sizeof(__nv_bfloat16)));
+    MCK(cudaMalloc(&p->iz, (size_t)M * MLP_OUT * sizeof(float)));
+    p->icap = M;
+  }
+  const __nv_bfloat16* x = (const __nv_bfloat16*)d_x;
+  __nv_bfloat16* bufs[2] = {p->ia, p->ib};
+  for (int l = 0; l < MLP_LAYERS; ++l) {
+    const bool last = (l == MLP_LAYERS - 1);
+    __nv_bfloat16* o = bufs[l & 1];
+    const int r = gemm(p, M, p->nout[l], p->kin[l], x, p->kin[l], p->wb + p->woff[l], p->kin[l], p->w + p->boff[l],
+                       last ? 0 : 1, last ? p->iz : nullptr, last ? nullptr : o, p->nout[l], st);
+    if (r) return r;
+    x = o;
+  }
+  MCK(cudaMemcpy2DAsync(d_out2, 2 * sizeof(float), p->iz, MLP_OUT * sizeof(float), 2 * sizeof(float), M,
+                        cudaMemcpyDeviceToDevice, st));
+  return SWDK_OK;
+}
+
+int swdk_mlp_error_flag(swdk_mlp* p, int* flag) {
+  if (!p || !flag) return SWDK_E_ARG;
+  MCK(cudaMemcpy(flag, p->err, sizeof(int), cudaMemcpyDeviceToHost));
+  return SWDK_OK;
 }
 
 // forward on device features x (M x 320 bf16) -> out (M x 2 fp32: mu, log sigma)

@@ -33,7 +33,8 @@ class Config(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("secular_evals", C.c_int64), ("layer_evals_rayleigh", C.c_int64), ("layer_evals_love", C.c_int64),
                 ("nchains", C.c_int32), ("nslots", C.c_int32),
-                ("ms_prep", C.c_float), ("ms_roots", C.c_float), ("ms_eigen", C.c_float)]
+                ("ms_prep", C.c_float), ("ms_roots", C.c_float), ("ms_eigen", C.c_float),
+                ("proposals_accepted", C.c_int64), ("proposals_rejected", C.c_int64), ("ms_proposal", C.c_float)]
 
 
 _LIB = None
@@ -62,6 +63,11 @@ def lib():
         L.swdk_frechet_rows_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp,
                                                vp, vp, vp]
         L.swdk_get_stats.argtypes = [vp, C.POINTER(Stats)]
+        L.swdk_set_proposal.argtypes = [vp, vp, vp, C.c_double, C.c_double]
+        L.swdk_roots_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
+        L.swdk_root_slots.argtypes = [vp, C.POINTER(C.c_int), vp, vp, vp]
+        L.swdk_last_roots.argtypes = [vp, vp, vp]
+        L.swdk_training_rows.argtypes = [vp, vp, C.c_int, vp, vp, vp]
         L.swdk_last_error.argtypes = [vp]
         L.swdk_last_error.restype = C.c_char_p
         _LIB = L
@@ -205,9 +211,47 @@ class Engine:
                                                    _p(fdm), _p(nnz), _p(indices), _p(values), stream),
                     "swdk_frechet_rows_device")
 
+    # -- learned bracket proposals -------------------------------------------
+    def set_proposal(self, rayleigh=None, love=None, kappa_rayleigh=4.0, kappa_love=4.0):
+        """Attach proposal networks (jdsurfg_b200.mlp.MLP or None each)."""
+        self._nets = (rayleigh, love)
+        hr = rayleigh._h if rayleigh is not None else None
+        hl = love._h if love is not None else None
+        self._check(lib().swdk_set_proposal(self._h, hr, hl, kappa_rayleigh, kappa_love), "swdk_set_proposal")
+
+    def roots_device(self, nx, ny, nz, vs, vp=None, rho=None, stream=None):
+        """Root search of every get_1d_kernel root slot on device models."""
+        self._check(lib().swdk_roots_device(self._h, nx, ny, nz, _p(vs), _p(vp), _p(rho), stream),
+                    "swdk_roots_device")
+
+    def root_slots(self):
+        """(wave, mode, period) per root slot (wave 2 Rayleigh, 1 Love; mode 0-based)."""
+        n = C.c_int(0)
+        self._check(lib().swdk_root_slots(self._h, C.byref(n), None, None, None), "swdk_root_slots")
+        w = np.empty(n.value, np.int32)
+        m = np.empty(n.value, np.int32)
+        t = np.empty(n.value, np.float64)
+        self._check(lib().swdk_root_slots(self._h, C.byref(n), _p(w), _p(m), _p(t)), "swdk_root_slots")
+        return w, m, t
+
+    def last_roots(self, ncol):
+        """Roots (nslot, ncol) and their status of the last root search."""
+        w, _, _ = self.root_slots()
+        c = np.empty((len(w), ncol))
+        st = np.empty((len(w), ncol), np.int32)
+        self._check(lib().swdk_last_roots(self._h, _p(c), _p(st)), "swdk_last_roots")
+        return c, st
+
+    def training_rows(self, rows, x, y=None, stream=None):
+        """Features (bf16 (n, 320)) and targets (c - 3.5) of rows slot*ncol+col
+        after roots_device; rows is an int64 device tensor."""
+        self._check(lib().swdk_training_rows(self._h, _p(rows), rows.shape[0], _p(x), _p(y), stream),
+                    "swdk_training_rows")
+
     def stats(self):
         s = Stats()
         self._check(lib().swdk_get_stats(self._h, C.byref(s)), "swdk_get_stats")
         return dict(secular_evals=s.secular_evals, layer_evals_rayleigh=s.layer_evals_rayleigh,
                     layer_evals_love=s.layer_evals_love, nchains=s.nchains, nslots=s.nslots, ms_prep=s.ms_prep,
-                    ms_roots=s.ms_roots, ms_eigen=s.ms_eigen)
+                    ms_roots=s.ms_roots, ms_eigen=s.ms_eigen, proposals_accepted=s.proposals_accepted,
+                    proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal)
