@@ -1,13 +1,17 @@
 #!/usr/bin/env python
 """Throughput of SurfTime::get_1d_kernel (dispersion + depth kernels for every
-column, period and mode of a 3-D model) on B200.
+column, period and mode of a 3-D model) on B200, learned-bracket path against
+the plain GPU scan.
 
-A step is one get_1d_kernel call over the whole workload (the "production"
-grid: 128x128 columns, 48 nodes, 40 periods 1-60 s, Rayleigh and Love, modes
-0-1, phase and group, LVZ in 20 % and fluid layers in 10 % of the columns;
-seeded synthetic models).  value = column-period-mode slots per second with
-inputs resident in HBM; e2e = the same through the host-memory C-ABI call
-with pinned host buffers, host<->device copies inside the timed region.
+A step is one get_1d_kernel call over the whole workload.  The default
+workload ("large") is the 256x256-column model with 64 nodes, 60 periods
+1-80 s, Rayleigh and Love fundamental-mode phase velocity and dc/dvs
+kernels, LVZ in 20 % of the columns (seeded synthetic models).  The learned
+bracket proposal (jdsurfg_b200/weights) is on; the same steps are then timed
+with it off ("plain" in the line).  value = column-period-mode slots per
+second with inputs resident in HBM; e2e = the same through the host-memory
+C-ABI call with pinned host buffers, host<->device copies inside the timed
+region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl swdk|reference]
 
@@ -38,15 +42,19 @@ UNIT = "column-period-modes/s"
 # divisions, square roots and exp/sin/cos are not counted.
 F_SEC_RAYLEIGH = 161
 F_SEC_LOVE = 19
+# proposal network multiply-adds per row: 320x256 + 3 x 256x256 + 256x64
+MLP_MACS_PER_ROW = 320 * 256 + 3 * 256 * 256 + 256 * 64
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="swdk", choices=["swdk", "reference"])
-    ap.add_argument("--workload", default="production", choices=["production", "large", "small", "tiny"])
+    ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny"])
+    ap.add_argument("--proposal", default="learned", choices=["learned", "none"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-scan comparison timing")
     ap.add_argument("--ncols", type=int, default=0, help="use only the first N columns (profiling)")
     ap.add_argument("--refine", default="tight", choices=["tight", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -68,9 +76,18 @@ def workload(args, rank):
     return case
 
 
+WORKLOAD_TEXT = {
+    "large": "256x256 columns x 64 nodes, 60 periods 1-80 s, Rayleigh+Love mode 0 phase, dc/dvs kernels",
+    "production": "128x128 columns x 48 nodes, 40 periods 1-60 s, Rayleigh+Love modes 0-1 phase+group, water",
+    "small": "16x16 columns x 20 nodes, 25 periods 2-40 s, Rayleigh mode 0 phase+group",
+    "tiny": "4x3 columns x 12 nodes, 6 periods, all wave types",
+}
+
+
 def case_desc(args, case, kmax):
-    return {"workload": args.workload, "nx": case["nx"], "ny": case["ny"], "nz": case["nz"], "kmax": kmax,
-            "columns": case["nx"] * case["ny"], "refine": args.refine, "root_tolerance_km_s": 1e-6,
+    return {"workload": args.workload, "what": WORKLOAD_TEXT[args.workload], "nx": case["nx"], "ny": case["ny"],
+            "nz": case["nz"], "kmax": kmax, "columns": case["nx"] * case["ny"], "refine": args.refine,
+            "proposal": args.proposal, "root_tolerance_km_s": 1e-6,
             "l2": "flushed between steps (256 MiB write)", "sphere": True}
 
 
@@ -227,6 +244,10 @@ def main():
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
     eng = Engine(device=local, refine=args.refine)
+    nets = None
+    from jdsurfg_b200 import learn
+    if args.proposal == "learned":
+        nets, _ = learn.load_proposals(eng)
     eng.setup(case)
     nx, ny, nz = case["nx"], case["ny"], case["nz"]
     ncol, kmax = nx * ny, eng.kmax
@@ -252,32 +273,58 @@ def main():
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
+    def timed(nsteps):
+        """device time of nsteps steps (max over ranks) and summed stage stats"""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        acc = dict(ms_roots=0.0, ms_proposal=0.0, ms_eigen=0.0, ms_prep=0.0, secular_evals=0,
+                   layer_evals_rayleigh=0, layer_evals_love=0, proposals_accepted=0, proposals_rejected=0,
+                   kernel_launches=0)
+        e0.record(stream)
+        for _ in range(nsteps):
+            step()
+            s = eng.stats()  # synchronises on the engine's work; collects per-stage events
+            for k in acc:
+                acc[k] += s[k]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if pg:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, acc
+
     clocks = ClockSampler(local)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    roots_ms, evals, lr, ll = 0.0, 0, 0, 0
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-        s = eng.stats()  # synchronises on the engine's work; collects per-stage events
-        roots_ms += s["ms_roots"]
-        evals += s["secular_evals"]
-        lr += s["layer_evals_rayleigh"]
-        ll += s["layer_evals_love"]
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
+    ms, acc = timed(args.steps)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
     ms_per_step = ms / args.steps
     value = world * units / (ms_per_step * 1e-3)
+    roots_ms, lr, ll, evals = acc["ms_roots"], acc["layer_evals_rayleigh"], acc["layer_evals_love"], acc["secular_evals"]
     stats = eng.stats()
     status = np.bincount(st.cpu().numpy().ravel(), minlength=5).tolist()
+    vc_learned = vc.cpu().numpy() if args.proposal == "learned" and not args.no_plain else None
+
+    plain = None
+    if args.proposal == "learned" and not args.no_plain:
+        eng.set_proposal(None, None)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        pms, pacc = timed(args.steps)
+        dmax = float(np.abs(vc.cpu().numpy() - vc_learned).max())
+        plain = {"value": world * units / (pms / args.steps * 1e-3), "ms_per_step": pms / args.steps,
+                 "ms_roots": pacc["ms_roots"] / args.steps,
+                 "evals_per_slot": pacc["secular_evals"] / args.steps / units,
+                 "learned_speedup": (pms / args.steps) / ms_per_step,
+                 "learned_roots_speedup": pacc["ms_roots"] / max(1e-9, roots_ms + acc["ms_proposal"]),
+                 "learned_eval_reduction": pacc["secular_evals"] / max(1, evals),
+                 "max_abs_dc_learned_vs_plain_km_s": dmax}
+        nets, _ = learn.load_proposals(eng)  # the e2e leg runs the learned path again
 
     # e2e: host-memory C-ABI call, pinned buffers, copies in the timed region
     e2e = None
@@ -321,15 +368,32 @@ def main():
         e2e = {"value": world * units * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
 
-    # roofline of the dominant kernel (k_roots: secular functions, FP64 pipe)
+    # roofline of the dominant kernels: the root search (k_roots_queue +
+    # k_retry; FP64 secular functions) and the proposal network (tcgen05 GEMMs)
     peak = fp64_peak_tflops(torch, dev)
     flops = lr * F_SEC_RAYLEIGH + ll * F_SEC_LOVE
     achieved = flops / (roots_ms * 1e-3) / 1e12 if roots_ms > 0 else 0.0
-    roofline = {"kernel": "k_roots", "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None, "traffic": None,
+    roofline = {"kernel": "k_roots_queue+k_retry", "bound": "fp64", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
                 "peak_source": "measured in this run: cuBLAS float64 GEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_layer_eval": {"rayleigh": F_SEC_RAYLEIGH, "love": F_SEC_LOVE},
                 "share_of_step": roots_ms / ms if ms else None}
+    if args.proposal == "learned" and acc["ms_proposal"] > 0:
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except Exception:
+            pass
+        bf16_peak = peaks.get("bf16_tflops") or 1590.0
+        rows = units  # one proposal row per root slot
+        gflops = 2.0 * rows * MLP_MACS_PER_ROW * args.steps
+        ach = gflops / (acc["ms_proposal"] * 1e-3) / 1e12
+        roofline["proposal"] = {"kernel": "k_features+k_gemm_tn+k_make_prop", "bound": "tensor", "achieved": ach,
+                                "peak": bf16_peak, "unit": "TFLOP/s", "frac": ach / bf16_peak,
+                                "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks.get("bf16_tflops")
+                                else "fallback 1590 TFLOP/s",
+                                "share_of_step": acc["ms_proposal"] / ms}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,11 +408,15 @@ def main():
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py); no public dataset exists for this path",
                 "config": case_desc(args, case, kmax), "clocks": clk, "e2e": e2e,
-                "gpu_launches": 3 * args.steps, "roofline": roofline, "cpu_baseline": cb,
+                "gpu_launches": int(acc["kernel_launches"]), "roofline": roofline, "cpu_baseline": cb,
+                "plain": plain,
                 "detail": {"secular_evals_per_step": evals / args.steps,
                            "evals_per_slot": evals / args.steps / units,
-                           "ms_roots": roots_ms / args.steps, "ms_prep": stats["ms_prep"],
-                           "ms_eigen": stats["ms_eigen"], "status_counts": status}}
+                           "proposals_used": acc["proposals_accepted"] / args.steps,
+                           "proposals_fell_back": acc["proposals_rejected"] / args.steps,
+                           "ms_prep": acc["ms_prep"] / args.steps, "ms_proposal": acc["ms_proposal"] / args.steps,
+                           "ms_roots": roots_ms / args.steps, "ms_eigen": acc["ms_eigen"] / args.steps,
+                           "status_counts": status}}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

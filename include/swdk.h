@@ -88,6 +88,7 @@ typedef struct swdk_stats {
   int64_t proposals_accepted;  /* learned brackets confirmed by the FP64 sign change */
   int64_t proposals_rejected;  /* learned brackets that fell back to the plain scan  */
   float ms_proposal;           /* device time of feature extraction + inference  */
+  int32_t kernel_launches;     /* kernels this library launched for the call       */
 } swdk_stats;
 
 typedef struct swdk_ctx swdk_ctx;

@@ -35,6 +35,7 @@ namespace {
 
 constexpr int FEAT_NODES = 64, FEAT_DIM = 320;  // proposal network input (see swdk_mlp.cu)
 constexpr double FEAT_C0 = 3.5;                  // phase velocity offset of the network target
+constexpr int MLP_INFER_KERNELS = 5;             // tcgen05 GEMM launches of one swdk_mlp_infer_rows
 
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
@@ -1008,6 +1009,7 @@ struct swdk_ctx {
   DevBuf nodefeat, pfeat, pout, prop;
   DevBuf retry_list, retry_ctr;  // deferred retries: records and {count, queue}
   int last_ncol = 0, last_path = -1;
+  int launches = 0;  // kernels launched by the current call
   // stage marks: 0 start, 1 prep, 5 proposals, 2 roots, 3 eigen, 4 call done
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   unsigned long long* h_nevals = nullptr;
@@ -1176,6 +1178,7 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
       if (m > n)  // padding rows of the last tile: finite zeros
         CK(cudaMemsetAsync(ctx->pfeat.as<__nv_bfloat16>() + (size_t)n * FEAT_DIM, 0,
                            (size_t)(m - n) * FEAT_DIM * sizeof(__nv_bfloat16), st));
+      ctx->launches += 2 + MLP_INFER_KERNELS;
       k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(),
                                               ctx->nodefeat.as<float4>(), nullptr, ctx->pfeat.as<__nv_bfloat16>());
       CK(cudaGetLastError());
@@ -1225,6 +1228,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
   CK(cudaEventRecord(ctx->ev[0], st));
+  ctx->launches = 1;
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
                                              ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
@@ -1252,6 +1256,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaMemsetAsync(ctx->queue.p, 0, sizeof(unsigned int), st));
   CK(cudaMemsetAsync(ctx->retry_ctr.p, 0, 2 * sizeof(unsigned int), st));
   unsigned int* rctr = ctx->retry_ctr.as<unsigned int>();
+  ctx->launches += 2;
   k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, 0, st>>>(
       ncol, nitems, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
       ctx->layL.as<float4>(), ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
@@ -1272,6 +1277,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
     const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
     const int nslots = (int)P.slots.size();
     const int et = std::min(128, ((nslots + 31) / 32) * 32);
+    ctx->launches += 1;
     k_eigen<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                     ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), nslots,
                                     ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
@@ -1284,6 +1290,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   ctx->stats_pending = true;
   ctx->stats.nchains = (int)P.chains.size();
   ctx->stats.nslots = P.kmax;
+  ctx->stats.kernel_launches = ctx->launches;
   ctx->last_ncol = ncol;
   ctx->last_path = roots_only ? 2 : path;
   return SWDK_OK;
@@ -1523,6 +1530,7 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
   CK(cudaEventRecord(ctx->ev[5], st));
+  ctx->stats.kernel_launches = 2;
   k_roots<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(nmodel, d_ch, d_t, ctx->layR.as<float4>(),
                                                          ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                                          ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, 0,

@@ -34,7 +34,8 @@ class Stats(C.Structure):
     _fields_ = [("secular_evals", C.c_int64), ("layer_evals_rayleigh", C.c_int64), ("layer_evals_love", C.c_int64),
                 ("nchains", C.c_int32), ("nslots", C.c_int32),
                 ("ms_prep", C.c_float), ("ms_roots", C.c_float), ("ms_eigen", C.c_float),
-                ("proposals_accepted", C.c_int64), ("proposals_rejected", C.c_int64), ("ms_proposal", C.c_float)]
+                ("proposals_accepted", C.c_int64), ("proposals_rejected", C.c_int64), ("ms_proposal", C.c_float),
+                ("kernel_launches", C.c_int32)]
 
 
 _LIB = None
@@ -254,4 +255,5 @@ class Engine:
         return dict(secular_evals=s.secular_evals, layer_evals_rayleigh=s.layer_evals_rayleigh,
                     layer_evals_love=s.layer_evals_love, nchains=s.nchains, nslots=s.nslots, ms_prep=s.ms_prep,
                     ms_roots=s.ms_roots, ms_eigen=s.ms_eigen, proposals_accepted=s.proposals_accepted,
-                    proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal)
+                    proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal,
+                    kernel_launches=s.kernel_launches)
