@@ -229,6 +229,11 @@ int swdk_root_slots(swdk_ctx* ctx, int* nslots, int32_t* wave, int32_t* mode, do
 int swdk_last_roots(swdk_ctx* ctx, double* h_c, int32_t* h_status);
 int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, float* d_y, void* stream);
 
+/* The reciprocal the secular functions use for 1/alpha, 1/beta, 1/rho and
+ * 1/(rho beta^2) (hardware estimate + two Newton-Raphson steps), applied to
+ * n device doubles; exported for its accuracy test. */
+int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream);
+
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 

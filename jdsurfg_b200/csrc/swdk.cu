@@ -171,21 +171,14 @@ __device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, cons
 
 __device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
 
-// layer-major, bottom-aligned REAL*4 layers plus the FP64 reciprocals the
-// secular functions use (1/a, 1/b; 1/rho and 1/(rho b^2) per wave type)
+// layer-major, bottom-aligned REAL*4 layers (h, alpha, beta, rho) of the
+// flattened model, one table per wave type (the density transform differs)
 __device__ void write_layers(int L, int ncol, int col, const float* th, const float* a, const float* b,
-                             const float* rR, const float* rL, float4* layR, float4* layL, double2* rab,
-                             double2* rrmR, double2* rrmL) {
+                             const float* rR, const float* rL, float4* layR, float4* layL) {
   for (int m = 0; m < L; ++m) {
     const size_t o = (size_t)(L - 1 - m) * ncol + col;
     layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
     layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
-    if (rab) {
-      const double bd = b[m];
-      rab[o] = make_double2(1.0 / (double)a[m], 1.0 / bd);
-      rrmR[o] = make_double2(1.0 / (double)rR[m], 1.0 / ((double)rR[m] * bd * bd));
-      rrmL[o] = make_double2(1.0 / (double)rL[m], 1.0 / ((double)rL[m] * bd * bd));
-    }
   }
 }
 
@@ -196,8 +189,7 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
                                               const float* __restrict__ vp_in, const float* __restrict__ rho_in,
                                               const float* __restrict__ depth, int sphere, int Lmax,
                                               float4* __restrict__ layR, float4* __restrict__ layL,
-                                              double2* __restrict__ rab, double2* __restrict__ rrmR,
-                                              double2* __restrict__ rrmL, float4* __restrict__ lay0,
+                                              float4* __restrict__ lay0,
                                               ColInfo* __restrict__ info, float2* __restrict__ chainrule,
                                               float4* __restrict__ nodefeat) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,15 +262,14 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
   ci.nw = nw;
   ci.valid = valid ? 1 : 0;
   sd96_setup(L, sphere, th, a, b, r, rR, rL, ci);
-  write_layers(L, ncol, col, th, a, b, rR, rL, layR, layL, rab, rrmR, rrmL);
+  write_layers(L, ncol, col, th, a, b, rR, rL, layR, layL);
   info[col] = ci;
 }
 
 // k_prep_layers: layered models (surfdisp96_ input) -> layer models
 __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ thk, const float* __restrict__ vp,
                               const float* __restrict__ vs, const float* __restrict__ rho, int sphere,
-                              float4* __restrict__ layR, float4* __restrict__ layL, double2* __restrict__ rab,
-                              double2* __restrict__ rrmR, double2* __restrict__ rrmL, ColInfo* __restrict__ info) {
+                              float4* __restrict__ layR, float4* __restrict__ layL, ColInfo* __restrict__ info) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= nmodel) return;
   float th[LMAX], a[LMAX], b[LMAX], r[LMAX], rR[LMAX], rL[LMAX];
@@ -293,7 +284,7 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
   ci.nw = (b[0] <= 0.0f) ? 1 : 0;
   ci.valid = valid ? 1 : 0;
   sd96_setup(nlayer, sphere, th, a, b, r, rR, rL, ci);
-  write_layers(nlayer, nmodel, col, th, a, b, rR, rL, layR, layL, rab, rrmR, rrmL);
+  write_layers(nlayer, nmodel, col, th, a, b, rR, rL, layR, layL);
   info[col] = ci;
 }
 
@@ -353,8 +344,6 @@ __global__ void k_targets(int n, int64_t rowmax, const int64_t* __restrict__ row
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const double* __restrict__ periods,
                                            const float4* __restrict__ layR, const float4* __restrict__ layL,
-                                           const double2* __restrict__ rab, const double2* __restrict__ rrmR,
-                                           const double2* __restrict__ rrmL,
                                            const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
                                            int retry, double* __restrict__ croot, int32_t* __restrict__ cstat,
                                            int32_t* __restrict__ ierr_out, unsigned long long* __restrict__ nevals) {
@@ -376,8 +365,7 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   }
   LayerView V;
   V.lay = (cd.iwave == 2) ? layR : layL;
-  V.rab = rab;
-  V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
+  V.fast = 0;  // dltar1/dltar4 as the reference writes them
   V.ncol = ncol;
   V.col = ccol;
   V.L = ci.L;
@@ -433,7 +421,7 @@ __global__ void __launch_bounds__(128) k_roots(int ncol, const ChainDesc* __rest
                                                int refine, double rtol, int sngl, int retry, double* __restrict__ croot,
                                                int32_t* __restrict__ cstat, int32_t* __restrict__ ierr_out,
                                                unsigned long long* __restrict__ nevals) {
-  roots_body(chains[blockIdx.y], ncol, periods, layR, layL, nullptr, nullptr, nullptr, info, refine, rtol, sngl, retry,
+  roots_body(chains[blockIdx.y], ncol, periods, layR, layL, info, refine, rtol, sngl, retry,
              croot, cstat, ierr_out, nevals);
 }
 
@@ -443,7 +431,7 @@ __global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const
                                                    const ColInfo* __restrict__ info, int refine, double rtol, int sngl,
                                                    double* __restrict__ croot, int32_t* __restrict__ cstat,
                                                    int32_t* __restrict__ ierr_out) {
-  roots_body(cd, ncol, periods, layR, layL, nullptr, nullptr, nullptr, info, refine, rtol, sngl, 0, croot, cstat,
+  roots_body(cd, ncol, periods, layR, layL, info, refine, rtol, sngl, 0, croot, cstat,
              ierr_out, nullptr);
 }
 
@@ -461,9 +449,6 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      const ChainDesc* __restrict__ chains,
                                                      const double* __restrict__ periods,
                                                      const float4* __restrict__ layR, const float4* __restrict__ layL,
-                                                     const double2* __restrict__ rab,
-                                                     const double2* __restrict__ rrmR,
-                                                     const double2* __restrict__ rrmL,
                                                      const ColInfo* __restrict__ info, int refine, double rtol,
                                                      int sngl, int retry, double* __restrict__ croot,
                                                      int32_t* __restrict__ cstat, unsigned int* __restrict__ queue,
@@ -501,8 +486,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
           continue;
         }
         V.lay = (cd.iwave == 2) ? layR : layL;
-        V.rab = rab;
-        V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
+        V.fast = 1;
         V.ncol = ncol;
         V.col = col;
         V.L = ci.L;
@@ -580,9 +564,6 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                const double* __restrict__ periods,
                                                                const float4* __restrict__ layR,
                                                                const float4* __restrict__ layL,
-                                                               const double2* __restrict__ rab,
-                                                               const double2* __restrict__ rrmR,
-                                                               const double2* __restrict__ rrmL,
                                                                const ColInfo* __restrict__ info, int refine,
                                                                double rtol, int sngl, double* __restrict__ croot,
                                                                int32_t* __restrict__ cstat,
@@ -617,8 +598,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     }
     const ColInfo ci = info[col];
     V.lay = (cd.iwave == 2) ? layR : layL;
-    V.rab = rab;
-    V.rrm = (cd.iwave == 2) ? rrmR : rrmL;
+    V.fast = 1;
     V.ncol = ncol;
     V.col = col;
     V.L = ci.L;
@@ -671,6 +651,12 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     atomicAdd(nevals + 1, lay_r);
     atomicAdd(nevals + 2, lay_l);
   }
+}
+
+// recip() on an array (its accuracy test)
+__global__ void k_recip(int n, const double* __restrict__ x, double* __restrict__ r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = recip(x[i]);
 }
 
 // cg(k, m) of model m = last mode's roots (surfdisp96's cg), model-major
@@ -1000,7 +986,7 @@ struct swdk_ctx {
   bool have_periods = false;
   bool dirty = true;
   Plan plan[2];  // 0: get_1d_kernel, 1: get_2d_map
-  DevBuf layR, layL, rab, rrmR, rrmL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr, queue;
+  DevBuf layR, layL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr, queue;
   int roots_blocks = 0;
   DevBuf in_vs, in_vp, in_rho, out_vc, out_vout, out_kernel, out_status, in_misc;
   // learned bracket proposals
@@ -1213,9 +1199,6 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   const bool wantfeat = useprop || roots_only;
   CK(ctx->layR.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->layL.ensure((size_t)Lmax * ncol * sizeof(float4)));
-  CK(ctx->rab.ensure((size_t)Lmax * ncol * sizeof(double2)));
-  CK(ctx->rrmR.ensure((size_t)Lmax * ncol * sizeof(double2)));
-  CK(ctx->rrmL.ensure((size_t)Lmax * ncol * sizeof(double2)));
   CK(ctx->queue.ensure(sizeof(unsigned int)));
   CK(ctx->lay0.ensure((size_t)Lmax * ncol * sizeof(float4)));
   CK(ctx->info.ensure((size_t)ncol * sizeof(ColInfo)));
@@ -1231,7 +1214,6 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   ctx->launches = 1;
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
-                                             ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                              ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr);
   CK(cudaGetLastError());
@@ -1259,15 +1241,13 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   ctx->launches += 2;
   k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, 0, st>>>(
       ncol, nitems, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
-      ctx->layL.as<float4>(), ctx->rab.as<double2>(), ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
-      ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
+      ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
       ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(),
       useprop ? ctx->prop.as<float2>() : nullptr, ctx->retry_list.as<int2>(), rctr, rcap,
       ctx->nevals.as<unsigned long long>());
   CK(cudaGetLastError());
   k_retry<<<rblocks, 128, 0, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
-                                   ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->rab.as<double2>(),
-                                   ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(), ctx->info.as<ColInfo>(),
+                                   ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                    ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, ctx->croot.as<double>(),
                                    ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
                                    ctx->nevals.as<unsigned long long>());
@@ -1409,7 +1389,7 @@ void swdk_destroy(swdk_ctx* ctx) {
   DevBuf* bufs[] = {&ctx->layR, &ctx->layL, &ctx->lay0, &ctx->info, &ctx->chainrule, &ctx->croot, &ctx->cstat,
                     &ctx->nevals, &ctx->depth_d, &ctx->ierr, &ctx->in_vs, &ctx->in_vp, &ctx->in_rho,
                     &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc,
-                    &ctx->rab, &ctx->rrmR, &ctx->rrmL, &ctx->queue, &ctx->nodefeat, &ctx->pfeat,
+                    &ctx->queue, &ctx->nodefeat, &ctx->pfeat,
                     &ctx->pout, &ctx->prop, &ctx->retry_list, &ctx->retry_ctr};
   for (DevBuf* b : bufs) b->release();
   for (int p = 0; p < 2; ++p) {
@@ -1512,9 +1492,6 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaMemcpyAsync(d_ch, &cd, sizeof(cd), cudaMemcpyHostToDevice, st));
   CK(ctx->layR.ensure(nin * sizeof(float4)));
   CK(ctx->layL.ensure(nin * sizeof(float4)));
-  CK(ctx->rab.ensure(nin * sizeof(double2)));
-  CK(ctx->rrmR.ensure(nin * sizeof(double2)));
-  CK(ctx->rrmL.ensure(nin * sizeof(double2)));
   CK(ctx->info.ensure(nm * sizeof(ColInfo)));
   CK(ctx->croot.ensure((size_t)mode * kmax * nm * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)mode * kmax * nm * sizeof(int32_t)));
@@ -1524,8 +1501,7 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_in, d_in + nin, d_in + 2 * nin,
                                                        d_in + 3 * nin, iflsph, ctx->layR.as<float4>(),
-                                                       ctx->layL.as<float4>(), ctx->rab.as<double2>(),
-                                                       ctx->rrmR.as<double2>(), ctx->rrmL.as<double2>(),
+                                                       ctx->layL.as<float4>(),
                                                        ctx->info.as<ColInfo>());
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[1], st));
@@ -1631,6 +1607,13 @@ int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, f
   return SWDK_OK;
 }
 
+int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream) {
+  if (n < 0 || (n > 0 && (!d_x || !d_r))) return SWDK_E_ARG;
+  if (n == 0) return SWDK_OK;
+  k_recip<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, d_x, d_r);
+  return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
+}
+
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out) {
   if (!ctx || !out) return SWDK_E_ARG;
   collect_stats(ctx);  // waits for the last call's completion event
@@ -1681,7 +1664,7 @@ int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_t
     ChainDesc cd;
     cd.t_off = 0; cd.np = kmax; cd.nmode = mode; cd.iwave = iwave; cd.igr = igr; cd.out_off = 0;
     k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_thk, d_vp, d_vs, d_rho, iflsph, layR, layL,
-                                                         nullptr, nullptr, nullptr, info);
+                                                         info);
     k_roots_one<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(cd, nmodel, d_t, layR, layL, info, refine,
                                                                rtol > 0.0 ? rtol : 1e-10, sngl, croot, cstat, d_ierr);
     const int n = nmodel * kmax;

@@ -102,8 +102,7 @@ SWDK_HD int pow2_exponent(double t) {
 // ---------------------------------------------------------------------------
 struct LayerView {
   const float4* lay;   // (d, a, b, rho) REAL*4 as surfdisp96 holds them
-  const double2* rab;  // (1/a, 1/b) in FP64, or null
-  const double2* rrm;  // (1/rho, 1/(rho b^2)) in FP64, or null
+  int fast;            // 1: secular_fast (recip()-based), 0: dltar1/dltar4 as written
   int ncol, col;
   int L;    // layers including the half-space
   int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
@@ -279,7 +278,26 @@ SWDK_HDI double dltar1(const LayerView& V, double wvno, double omega) {
   return e1;
 }
 
-// dltar4 with the per-layer reciprocals precomputed (1/a, 1/b, 1/rho), the
+// 1/x for the positive, normal layer parameters: the hardware estimate
+// (PTX rcp.approx.ftz.f64) refined by two Newton-Raphson steps
+// r <- r + r (1 - x r), each with fused multiply-adds; the relative error
+// is then below one unit in the last place.  Computing the reciprocals here
+// instead of reading FP64 tables keeps one float4 per layer as the only
+// memory traffic of an evaluation.
+SWDK_HD double recip(double x) {
+#ifdef __CUDA_ARCH__
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+#else
+  return 1.0 / x;
+#endif
+}
+
+// dltar4 with the per-layer reciprocals (1/a, 1/b, 1/rho) from recip(), the
 // vertical wavenumber and its reciprocal from one rsqrt, exp(-(p+q)) as
 // exp(-p) exp(-q), and the max-normalisation applied every NORM layers
 // (NORM = 1 is surfdisp96's per-layer normc; larger NORM rescales the
@@ -290,14 +308,12 @@ struct LayerCoef {
 };
 
 SWDK_HD LayerCoef layer_coef(const LayerView& V, int m, double wvno, double wvno2, double omega, double iom) {
-  const size_t ix = V.idx(m);
-  const float4 ly = V.lay[ix];
-  const double2 rr = V.rab[ix];
+  const float4 ly = V.lay[V.idx(m)];
   LayerCoef k;
-  k.irho = V.rrm[ix].x;
+  k.irho = recip((double)ly.w);
   const double dpth = ly.x;
   k.rho = ly.w;
-  const double xka = omega * rr.x, xkb = omega * rr.y;
+  const double xka = omega * recip((double)ly.y), xkb = omega * recip((double)ly.z);
   const double t = (double)ly.z * iom;
   k.gammk = 2.0 * t * t;
   k.gam = k.gammk * wvno2;
@@ -382,10 +398,8 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   if (omega < 1.0e-4) omega = 1.0e-4;
   const double wvno2 = wvno * wvno;
   const double iom = 1.0 / omega;
-  const size_t ih = V.idx(V.L - 1);
-  const float4 h = V.lay[ih];
-  const double2 hr = V.rab[ih];
-  double xka = omega * hr.x, xkb = omega * hr.y;
+  const float4 h = V.lay[V.idx(V.L - 1)];
+  double xka = omega * recip((double)h.y), xkb = omega * recip((double)h.z);
   const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
   const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
   const double t = (double)h.z * iom;
@@ -416,10 +430,9 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
     }
   }
   if (V.llw != 1) {
-    const size_t ix = V.idx(0);
-    const float4 ly = V.lay[ix];
+    const float4 ly = V.lay[V.idx(0)];
     const double dpth = ly.x, rho = ly.w;
-    xka = omega * V.rab[ix].x;
+    xka = omega * recip((double)ly.y);
     const double Xa = (wvno + xka) * fabs(wvno - xka);
     double w, cosp;
     if (wvno < xka) {
@@ -441,26 +454,24 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   return e0;
 }
 
-// dltar1 with precomputed 1/b and 1/(rho b^2)
+// dltar1 with 1/b and 1/(rho b^2) from recip()
 template <int NORM>
 SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
-  const size_t ih = V.idx(V.L - 1);
-  float4 h = V.lay[ih];
+  float4 h = V.lay[V.idx(V.L - 1)];
   double beta1 = h.z, rho1 = h.w;
-  double xkb = omega * V.rab[ih].y;
+  double xkb = omega * recip(beta1);
   double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
   double e1 = rho1 * rb;
   double e2 = 1.0 / (beta1 * beta1);
   int since = 0;
   for (int m = V.L - 2; m >= V.llw - 1; --m) {
-    const size_t ix = V.idx(m);
-    const float4 ly = V.lay[ix];
-    const double ib = V.rab[ix].y, ixmu = V.rrm[ix].y;
+    const float4 ly = V.lay[V.idx(m)];
     beta1 = ly.z;
     rho1 = ly.w;
     const double dpth = ly.x;
     const double xmu = rho1 * beta1 * beta1;
-    xkb = omega * ib;
+    const double ixmu = recip(xmu);
+    xkb = omega * recip(beta1);
     const double Xb = (wvno + xkb) * fabs(wvno - xkb);
     double cosq, y, z;
     if (wvno < xkb) {
@@ -1017,7 +1028,7 @@ SWDK_HDI void run_chain(const LayerView& V, const ChainParams& P, const ChainIO&
     if (!need) active = false;
     if (__ballot_sync(0xffffffffu, need) == 0u) break;
     if (need) {
-      s.last = V.rab ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
+      s.last = V.fast ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
                      : secular(V, P.iwave, s.omega / s.creq, s.omega);
       s.nevals++;
       s.phase = s.next;
@@ -1026,7 +1037,7 @@ SWDK_HDI void run_chain(const LayerView& V, const ChainParams& P, const ChainIO&
 #else
   if (!active) return;
   while (chain_advance(s, P, io)) {
-    s.last = V.rab ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
+    s.last = V.fast ? secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega)
                    : secular(V, P.iwave, s.omega / s.creq, s.omega);
     s.nevals++;
     s.phase = s.next;

@@ -181,3 +181,24 @@ def test_frechet_rows_match_oracle():
         assert nnz[rr] == len(ri)
         np.testing.assert_array_equal(idx[rr * n:rr * n + nnz[rr]], ri)
         np.testing.assert_array_equal(val[rr * n:rr * n + nnz[rr]], rv)
+
+
+def test_recip_within_one_ulp_of_division():
+    """recip() (estimate + two Newton-Raphson steps) against IEEE 1/x over
+    the range of layer parameters and of rho*beta^2."""
+    import ctypes as C
+    import torch
+    from jdsurfg_b200.engine import lib
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.exp(torch.empty(1 << 20, dtype=torch.float64, device="cuda").uniform_(-3.0, 6.0, generator=g))
+    x[:4] = torch.tensor([1.0, 1.5, 1.732, 4.7], dtype=torch.float64)
+    r = torch.empty_like(x)
+    L = lib()
+    L.swdk_recip_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    assert L.swdk_recip_device(C.c_void_p(x.data_ptr()), C.c_void_p(r.data_ptr()), x.numel(), None) == 0
+    torch.cuda.synchronize()
+    ref = (1.0 / x.cpu().numpy())
+    got = r.cpu().numpy()
+    ulp = np.spacing(ref)
+    assert np.max(np.abs(got - ref) / ulp) <= 1.0
+    assert np.mean(got == ref) > 0.99
