@@ -178,7 +178,7 @@ def cpu_baseline(case, args, target_s):
     O._LIB.swdo_frechet_rows.restype = C.c_long
     cores = os.cpu_count() or 1
     ncol = case["nx"] * case["ny"]
-    refine = 1 if args.refine == "tight" else 0
+    refine = 0  # the reference's own algorithm: surfdisp96's scan + nevill refinement
     n = min(ncol, max(cores, 8))
     t0 = time.perf_counter()
     r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n))
@@ -192,7 +192,8 @@ def cpu_baseline(case, args, target_s):
     r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n2))
     dt = time.perf_counter() - t0
     return {"value": n2 * kmax / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n2} of {ncol} columns x {kmax} slots ({dt:.1f} s, {how}, OpenMP over columns)"}, n2, dt
+            "sample": f"{n2} of {ncol} columns x {kmax} slots ({dt:.1f} s, {how}, OpenMP over columns, "
+                      f"reference-faithful refinement)"}, n2, dt
 
 
 def run_reference(args):
@@ -208,7 +209,7 @@ def run_reference(args):
     per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     cb, n2, _ = cpu_baseline(case, args, per_step_s)
     import oracle_lib as O
-    refine = 1 if args.refine == "tight" else 0
+    refine = 0  # reference-faithful: surfdisp96's own scan + nevill refinement
     cols = np.arange(n2)
     for _ in range(args.warmup):
         O.get_1d_kernel(case, refine=refine, nthreads=cb["cores"], cols=cols[:max(1, n2 // 4)])
@@ -308,6 +309,7 @@ def main():
     vc_learned = vc.cpu().numpy() if args.proposal == "learned" and not args.no_plain else None
 
     plain = None
+    alg_lr, alg_ll = lr, ll  # algorithmic layer-evaluations: the plain method's count
     if args.proposal == "learned" and not args.no_plain:
         eng.set_proposal(None, None)
         for _ in range(2):
@@ -317,6 +319,7 @@ def main():
             pg.barrier()
         pms, pacc = timed(args.steps)
         dmax = float(np.abs(vc.cpu().numpy() - vc_learned).max())
+        alg_lr, alg_ll = pacc["layer_evals_rayleigh"], pacc["layer_evals_love"]
         plain = {"value": world * units / (pms / args.steps * 1e-3), "ms_per_step": pms / args.steps,
                  "ms_roots": pacc["ms_roots"] / args.steps,
                  "evals_per_slot": pacc["secular_evals"] / args.steps / units,
@@ -371,12 +374,14 @@ def main():
     # roofline of the dominant kernels: the root search (k_roots_queue +
     # k_retry; FP64 secular functions) and the proposal network (tcgen05 GEMMs)
     peak = fp64_peak_tflops(torch, dev)
-    flops = lr * F_SEC_RAYLEIGH + ll * F_SEC_LOVE
+    flops = alg_lr * F_SEC_RAYLEIGH + alg_ll * F_SEC_LOVE
     achieved = flops / (roots_ms * 1e-3) / 1e12 if roots_ms > 0 else 0.0
     roofline = {"kernel": "k_roots_queue+k_retry", "bound": "fp64", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
                 "peak_source": "measured in this run: cuBLAS float64 GEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_layer_eval": {"rayleigh": F_SEC_RAYLEIGH, "love": F_SEC_LOVE},
+                "work": "plain-method secular evaluations x layers x flops per layer (the learned "
+                        "path's saved evaluations show up as a shorter duration)",
                 "share_of_step": roots_ms / ms if ms else None}
     if args.proposal == "learned" and acc["ms_proposal"] > 0:
         peaks = {}
