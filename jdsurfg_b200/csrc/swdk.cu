@@ -686,18 +686,6 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
   return group ? c * tm : c / tm;
 }
 
-// node contribution x_b + x_a*dadb + x_r*drda*dadb of one pass, scaled by s
-__device__ __forceinline__ void accumulate_nodes(double* kacc, const double* na, const double* nb, const double* nr,
-                                                 const float2* cr, int nz, double s, bool has_a) {
-  for (int i = 0; i < nz; ++i) {
-    const double dadb = cr[i].x, drda = cr[i].y;
-    double v = nb[i];
-    if (has_a) v = v + na[i] * dadb;
-    v = v + nr[i] * drda * dadb;
-    kacc[i] += s * v;
-  }
-}
-
 __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                                const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
                                                const SlotDesc* __restrict__ slots, int nslots,
@@ -758,7 +746,13 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
   ML.zd = zd; ML.za = za; ML.zb = zb; ML.zrho = zrL; ML.vtp = vtp; ML.rtp = rtL; ML.L = L;
 
   double scr[LMAX * 6];
-  double kacc[NZMAX], na[NZMAX], nb[NZMAX], nr[NZMAX];
+  double kacc[NZMAX], kp[NZMAX];
+  NodeSink sink;
+  sink.kp = (path == 0) ? kp : nullptr;
+  sink.crs = crs;
+  sink.L = L;
+  sink.nw = ci.nw;
+  const NodeSink nosink = {nullptr, crs, L, ci.nw};
   for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
     const SlotDesc sd = slots[s];
     const bool love = sd.wtype >= 2;
@@ -795,8 +789,8 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
         vc[oo] = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
         const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
         double ugr, norm;
-        if (love) love_pass(M, omega, wvno, scr, ugr, norm);
-        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
+        if (love) love_pass(M, omega, wvno, scr, ugr, norm, nosink);
+        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, nosink);
         double tm = 1.0;
         if (sphere) {
           const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
@@ -808,29 +802,19 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
     }
     // ---- get_1d_kernel: kernel1D (SurfaceWave.cpp:266-412) ----
     for (int i = 0; i < nz; ++i) kacc[i] = 0.0;
-    const int stride = love ? 3 : 6;
-    const double* fac_a = M.vtp;
-    const double* fac_r = M.rtp;
     if (!group) {
       const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
       double ugr, norm;
-      if (love) love_pass(M, omega, wvno, scr, ugr, norm);
-      else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
+      for (int i = 0; i < nz; ++i) kp[i] = 0.0;
+      if (love) love_pass(M, omega, wvno, scr, ugr, norm, sink);
+      else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, sink);
       double tm = 1.0;
       if (sphere) {
         const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
         tm = sqrt(1. + x * x);
       }
-      const double tm3 = tm * tm * tm;
-      if (love) {
-        param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, nb);
-        param_convert_dev(scr, stride, 1, norm, fac_r, L, nz, ci.nw, nr);
-      } else {
-        param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, na);
-        param_convert_dev(scr, stride, 1, norm, fac_a, L, nz, ci.nw, nb);
-        param_convert_dev(scr, stride, 2, norm, fac_r, L, nz, ci.nw, nr);
-      }
-      accumulate_nodes(kacc, na, nb, nr, crs, nz, 1.0 / tm3, !love);
+      const double s1 = 1.0 / (norm * tm * tm * tm);
+      for (int i = 0; i < nz; ++i) kacc[i] = kp[i] * s1;
       const double cs = c0 / tm;
       vc[oo] = cs;
       vout[oo] = cs;
@@ -844,16 +828,9 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
         const double cc = (pass == 0) ? c0 : (pass == 1) ? c1 : c2;
         const double omega = twopi / tt, wvno = omega / cc;
         double ugr, norm;
-        if (love) love_pass(M, omega, wvno, scr, ugr, norm);
-        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm);
-        if (love) {
-          param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, nb);
-          param_convert_dev(scr, stride, 1, norm, fac_r, L, nz, ci.nw, nr);
-        } else {
-          param_convert_dev(scr, stride, 0, norm, fac_a, L, nz, ci.nw, na);
-          param_convert_dev(scr, stride, 1, norm, fac_a, L, nz, ci.nw, nb);
-          param_convert_dev(scr, stride, 2, norm, fac_r, L, nz, ci.nw, nr);
-        }
+        for (int i = 0; i < nz; ++i) kp[i] = 0.0;
+        if (love) love_pass(M, omega, wvno, scr, ugr, norm, sink);
+        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, sink);
         double coef;
         if (pass == 0) {
           cg = ugr;
@@ -877,7 +854,10 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
         } else {
           coef = tm * (f1 - f2 / dtt);
         }
-        if (coef != 0.0) accumulate_nodes(kacc, na, nb, nr, crs, nz, coef, !love);
+        if (coef != 0.0) {
+          const double s1 = coef / norm;
+          for (int i = 0; i < nz; ++i) kacc[i] += kp[i] * s1;
+        }
       }
       vc[oo] = cp / tm;
       vout[oo] = cg * tm;

@@ -23,6 +23,51 @@ struct EigModel {
   int L;
 };
 
+// _ParamConvert (SurfaceWave.cpp:59-101) and the empirical chain rule
+// (SurfaceWave.cpp:491-500) applied to each layer's raw kernels as the energy
+// sweep produces them, so no per-layer kernel array is kept.  With nw = 0,
+// layer l feeds node l/4 with weight 1 - (2j+1)/8 and node l/4 + 1 with
+// (2j+1)/8, j = l % 4; with nw > 0 leading fluid nodes, solid layer l feeds
+// the same pattern shifted to l-1 and nw (the fluid layer feeds a fluid node,
+// whose kernel is zero).  The half-space weighs 4.875 (the reference's loop
+// adds it once with 7/8 and four more times).  Node n accumulates
+//   w * (x_b fa(l) + x_a fa(l) dalpha/dbeta(n) + x_r fr(l) drho/dalpha(n) dalpha/dbeta(n))
+// with fa = vtp, fr = rtp; the pass's normaliser divides the sum afterwards.
+struct NodeSink {
+  double* kp;         // node accumulator [nz] (null: no kernels wanted)
+  const float2* crs;  // (dalpha/dbeta, drho/dalpha) per node
+  int L, nw;
+  SWDK_HD void add(const EigModel& M, int l, double xa, double xb, double xr) const {
+    if (!kp) return;
+    int n0, n1 = -1;
+    double w0, w1 = 0.0;
+    if (nw > 0 && l == 0) return;
+    const int lp = (nw > 0) ? l - 1 : l;
+    if (l == L - 1) {
+      n0 = (lp >> 2) + nw;
+      w0 = 4.875;
+    } else {
+      const double t = (double)(2 * (lp & 3) + 1) / 8.0;
+      n0 = (lp >> 2) + nw;
+      w0 = 1.0 - t;
+      n1 = n0 + 1;
+      w1 = t;
+    }
+    const double fa = M.vtp[l], fr = M.rtp[l];
+    const double xbf = xb * fa, xaf = xa * fa, xrf = xr * fr;
+    {
+      const float2 c = crs[n0];
+      const double dadb = c.x, drda = c.y;
+      kp[n0] += w0 * (xbf + xaf * dadb + xrf * drda * dadb);
+    }
+    if (n1 >= 0) {
+      const float2 c = crs[n1];
+      const double dadb = c.x, drda = c.y;
+      kp[n1] += w1 * (xbf + xaf * dadb + xrf * drda * dadb);
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // varsv (sregn96.f90:827-911) for the pure real / pure imaginary vertical
 // wavenumbers that cdsqrt of a real argument produces
@@ -460,7 +505,7 @@ SWDK_HD Eig4 eigen_at(const double* cd, const double* vv, double ext, double f12
 // the raw layer kernels (dcda, dcdb, dcdr) once the layer has been consumed.
 // Returns ugr (flat) and norm = ugr*sumi0; scr[6m+0..2] = raw dcda/dcdb/dcdr.
 SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, double wvno, double* scr, double& ugr,
-                            double& norm) {
+                            double& norm, const NodeSink& sink) {
   const int L = M.L;
   const double wvno2 = wvno * wvno, om2 = omega * omega;
   // ---- up (sregn96.f90:401-489) ----
@@ -543,8 +588,7 @@ SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, doub
     }
     double da, db, dr;
     energy_layer_r(M, m, iw, allfluid, u0, u1, omega, om2, wvno, wvno2, c, acc, da, db, dr);
-    double* sm = scr + 6 * m;
-    sm[0] = da; sm[1] = db; sm[2] = dr;
+    sink.add(M, m, da, db, dr);
     u0 = u1;
   }
   ugr = (wvno * acc.sumi1 + acc.sumi2) / (omega * acc.sumi0);
@@ -556,7 +600,8 @@ SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, doub
 // doubles per layer (uu, tt, exl) then the raw (dcdb, dcdr).  Returns ugr and
 // the normaliser sumi1.
 // ---------------------------------------------------------------------------
-SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* scr, double& ugr, double& norm) {
+SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* scr, double& ugr, double& norm,
+                        const NodeSink& sink) {
   const int L = M.L;
   const double wvno2 = wvno * wvno;
   // ---- up (slegn96.f90:372-445) ----
@@ -631,7 +676,6 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
   double sumi0 = 0.0, sumi1 = 0.0;
   double prev_uu = scr[0] * iumax, prev_tt = scr[1] * iumax;
   for (int k = 0; k < L; ++k) {
-    double* sk = scr + 3 * k;
     const double uu = prev_uu, tt = prev_tt;
     double nuu = 0.0, ntt = 0.0;
     if (k < L - 1) {
@@ -641,9 +685,9 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
     prev_uu = nuu;
     prev_tt = ntt;
     const double zb = M.zb[k];
-    if (!(zb > 0.0)) { sk[0] = 0.0; sk[1] = 0.0; continue; }
+    if (!(zb > 0.0)) continue;
     const double zr = M.zrho[k];
-    const double TN = zr * zb * zb, TL = zr * zb * zb;
+    const double TN = zr * zb * zb;
     const double drho = zr, dpth = M.zd[k];
     const double xkb = omega / zb;
     double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
@@ -679,8 +723,7 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
     const double VSHH = zb, VSHV = zb;
     const double DCDBH = c * drho * VSHH * upup;
     const double DCDBV = c * drho * VSHV * dupdup / wvno2;
-    sk[0] = DCDBH + DCDBV;
-    sk[1] = 0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup / wvno2);
+    sink.add(M, k, 0.0, DCDBH + DCDBV, 0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup / wvno2));
   }
   ugr = sumi1 / (c * sumi0);
   norm = sumi1;
