@@ -394,7 +394,7 @@ def main():
         rows = units  # one proposal row per root slot
         gflops = 2.0 * rows * MLP_MACS_PER_ROW * args.steps
         ach = gflops / (acc["ms_proposal"] * 1e-3) / 1e12
-        roofline["proposal"] = {"kernel": "k_features+k_gemm_tn+k_make_prop", "bound": "tensor", "achieved": ach,
+        roofline["proposal"] = {"kernel": "k_features+k_mlp_propose", "bound": "tensor", "achieved": ach,
                                 "peak": bf16_peak, "unit": "TFLOP/s", "frac": ach / bf16_peak,
                                 "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks.get("bf16_tflops")
                                 else "fallback 1590 TFLOP/s",

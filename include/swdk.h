@@ -200,7 +200,15 @@ int swdk_mlp_set_params(swdk_mlp* mlp, const float* host, int64_t n);
 int swdk_mlp_get_grads(swdk_mlp* mlp, float* host, int64_t n);
 /* d_x: (M, 320) bf16 features; d_out: (M, 2) float (mu, log sigma) */
 int swdk_mlp_forward(swdk_mlp* mlp, const void* d_x, int M, float* d_out, void* stream);
-int swdk_mlp_infer_rows(swdk_mlp* mlp, const void* d_x, int M, float* d_out2, void* stream);
+/* Fused inference (all layers of a 128-row tile in one persistent tcgen05
+ * kernel) straight to bracket proposals: d_prop[r] = (3.5 + mu, clamp(kappa *
+ * sigma, 2e-5 c, 0.2)) as float2 for r < nrows.  d_xtiles holds the rows as
+ * 128-row tile images of 320 bf16 in the 128-byte-swizzled K-major layout
+ * (tile t, K-block kb of 64 columns, row r, column c at byte
+ * t*81920 + kb*16384 + r*128 + (((c%64)/8 ^ r%8) * 16) + (c%8)*2), rows padded
+ * to a multiple of 128.  Asynchronous on `stream`; a timed-out wait sets the
+ * flag read by swdk_mlp_error_flag. */
+int swdk_mlp_propose(swdk_mlp* mlp, const void* d_xtiles, int nrows, double kappa, void* d_prop, void* stream);
 /* forward + Gaussian NLL + backward; Adam step when lr > 0 */
 int swdk_mlp_train_step(swdk_mlp* mlp, const void* d_x, const float* d_y, int M, float lr, float* loss_out,
                         void* stream);

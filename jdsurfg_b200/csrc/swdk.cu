@@ -35,7 +35,6 @@ namespace {
 
 constexpr int FEAT_NODES = 64, FEAT_DIM = 320;  // proposal network input (see swdk_mlp.cu)
 constexpr double FEAT_C0 = 3.5;                  // phase velocity offset of the network target
-constexpr int MLP_INFER_KERNELS = 5;             // tcgen05 GEMM launches of one swdk_mlp_infer_rows
 
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
@@ -289,45 +288,53 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// proposal-network rows: row = slot * ncol + col; one warp per row
+// proposal-network rows: row = slot * ncol + col; one warp per row, a lane
+// writes 8 consecutive columns (16 bytes)
 //   x[0:64) vs, [64:128) vp, [128:192) rho, [192:256) thickness,
 //   x[256] log(T)/log(100), x[257] (mode-1)/2, zero to 320
+// tiled = 0: row-major (n, 320); tiled = 1: the 128-row tile images
+// swdk_mlp_propose reads (128-byte swizzled K-major, 81920 bytes per tile)
 // ---------------------------------------------------------------------------
 __global__ void k_features(int64_t row0, int nrows, int ncol, int64_t rowmax, const float4* __restrict__ slotfeat,
                            const float4* __restrict__ nodefeat, const int64_t* __restrict__ rowlist,
-                           __nv_bfloat16* __restrict__ x) {
+                           __nv_bfloat16* __restrict__ x, int tiled) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= nrows) return;
   const int64_t row = rowlist ? rowlist[w] : row0 + w;
-  if (row < 0 || row >= rowmax) {  // out-of-range request: zero row
-    for (int i = lane; i < FEAT_DIM; i += 32) x[(size_t)w * FEAT_DIM + i] = __float2bfloat16_rn(0.0f);
-    return;
-  }
-  const int s = (int)(row / ncol), col = (int)(row % ncol);
+  const bool inr = row >= 0 && row < rowmax;
+  const int s = inr ? (int)(row / ncol) : 0, col = inr ? (int)(row % ncol) : 0;
   const float4 sf = slotfeat[s];
   const float4* nf = nodefeat + (size_t)col * FEAT_NODES;
-  __nv_bfloat16* xr = x + (size_t)w * FEAT_DIM;
-  for (int i = lane; i < FEAT_NODES; i += 32) {
-    const float4 n = nf[i];
-    xr[i] = __float2bfloat16_rn(n.x);
-    xr[64 + i] = __float2bfloat16_rn(n.y);
-    xr[128 + i] = __float2bfloat16_rn(n.z);
-    xr[192 + i] = __float2bfloat16_rn(n.w);
+  for (int q = lane; q < FEAT_DIM / 8; q += 32) {
+    float v[8];
+    const int c0 = q * 8;
+    if (c0 < 4 * FEAT_NODES) {
+      const int comp = c0 / FEAT_NODES, n0 = c0 % FEAT_NODES;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const float4 n = nf[n0 + e];
+        v[e] = comp == 0 ? n.x : comp == 1 ? n.y : comp == 2 ? n.z : n.w;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = (c0 + e == 256) ? sf.x : (c0 + e == 257) ? sf.y : 0.0f;
+    }
+    uint32_t pk[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const __nv_bfloat162 b2 = __floats2bfloat162_rn(inr ? v[2 * e] : 0.0f, inr ? v[2 * e + 1] : 0.0f);
+      pk[e] = *reinterpret_cast<const uint32_t*>(&b2);
+    }
+    uint8_t* dst;
+    if (tiled) {
+      const int t = w >> 7, r = w & 127, kb = c0 >> 6, j = (c0 & 63) >> 3;
+      dst = reinterpret_cast<uint8_t*>(x) + (size_t)t * (128 * FEAT_DIM * 2) + kb * (128 * 128) + r * 128 +
+            ((j ^ (r & 7)) << 4);
+    } else {
+      dst = reinterpret_cast<uint8_t*>(x + (size_t)w * FEAT_DIM + c0);
+    }
+    *reinterpret_cast<uint4*>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
   }
-  for (int i = 256 + lane; i < FEAT_DIM; i += 32)
-    xr[i] = __float2bfloat16_rn(i == 256 ? sf.x : i == 257 ? sf.y : 0.0f);
-}
-
-// proposal (c, half-width) from the network output (mu, log sigma)
-__global__ void k_make_prop(int64_t row0, int nrows, const float* __restrict__ out2, double kappa,
-                            float2* __restrict__ prop) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nrows) return;
-  const float mu = out2[2 * i], ls = out2[2 * i + 1];
-  const double c = FEAT_C0 + (double)mu;
-  double hw = kappa * exp(fmin(fmax((double)ls, -12.0), 2.0));
-  hw = fmin(fmax(hw, 2.0e-5 * c), 0.2);
-  prop[row0 + i] = (mu == mu && ls == ls) ? make_float2((float)c, (float)hw) : make_float2(0.0f, 0.0f);
 }
 
 // training targets of chosen rows: y = c_flat - FEAT_C0
@@ -972,7 +979,7 @@ struct swdk_ctx {
   // learned bracket proposals
   swdk_mlp* net[2] = {nullptr, nullptr};  // 0: Rayleigh, 1: Love
   double kappa[2] = {4.0, 4.0};
-  DevBuf nodefeat, pfeat, pout, prop;
+  DevBuf nodefeat, pfeat, prop;
   DevBuf retry_list, retry_ctr;  // deferred retries: records and {count, queue}
   int last_ncol = 0, last_path = -1;
   int launches = 0;  // kernels launched by the current call
@@ -1120,16 +1127,15 @@ int ensure_plans(swdk_ctx* ctx) {
   return SWDK_OK;
 }
 
-constexpr int PROP_CHUNK = 262144;  // proposal rows per inference launch group (multiple of 128)
+constexpr int PROP_CHUNK = 1 << 20;  // proposal rows per feature/inference launch pair (multiple of 128)
 
 bool proposals_on(const swdk_ctx* ctx) { return ctx->cfg.refine == 1 && (ctx->net[0] || ctx->net[1]); }
 
-// features -> network -> (c, half-width) for every root row of plan P
+// features -> fused network -> (c, half-width) for every root row of plan P
 int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
   const int64_t nrows = (int64_t)P.nroot * ncol;
   CK(ctx->prop.ensure((size_t)nrows * sizeof(float2)));
   CK(ctx->pfeat.ensure((size_t)PROP_CHUNK * FEAT_DIM * sizeof(__nv_bfloat16)));
-  CK(ctx->pout.ensure((size_t)PROP_CHUNK * 2 * sizeof(float)));
   const int64_t bound[3] = {0, (int64_t)P.nrootR * ncol, nrows};
   for (int w = 0; w < 2; ++w) {
     const int64_t r0 = bound[w], r1 = bound[w + 1];
@@ -1140,19 +1146,12 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
     }
     for (int64_t a = r0; a < r1; a += PROP_CHUNK) {
       const int n = (int)std::min<int64_t>(PROP_CHUNK, r1 - a);
-      const int m = (n + 127) / 128 * 128;
-      if (m > n)  // padding rows of the last tile: finite zeros
-        CK(cudaMemsetAsync(ctx->pfeat.as<__nv_bfloat16>() + (size_t)n * FEAT_DIM, 0,
-                           (size_t)(m - n) * FEAT_DIM * sizeof(__nv_bfloat16), st));
-      ctx->launches += 2 + MLP_INFER_KERNELS;
+      ctx->launches += 2;
       k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(),
-                                              ctx->nodefeat.as<float4>(), nullptr, ctx->pfeat.as<__nv_bfloat16>());
+                                              ctx->nodefeat.as<float4>(), nullptr, ctx->pfeat.as<__nv_bfloat16>(), 1);
       CK(cudaGetLastError());
-      int r = swdk_mlp_infer_rows(ctx->net[w], ctx->pfeat.p, m, ctx->pout.as<float>(), st);
+      int r = swdk_mlp_propose(ctx->net[w], ctx->pfeat.p, n, ctx->kappa[w], ctx->prop.as<float2>() + a, st);
       if (r) return fail(ctx, r, std::string("proposal inference: ") + swdk_mlp_last_error(ctx->net[w]));
-      k_make_prop<<<(n + 255) / 256, 256, 0, st>>>(a, n, ctx->pout.as<float>(), ctx->kappa[w],
-                                                    ctx->prop.as<float2>());
-      CK(cudaGetLastError());
     }
   }
   return SWDK_OK;
@@ -1370,7 +1369,7 @@ void swdk_destroy(swdk_ctx* ctx) {
                     &ctx->nevals, &ctx->depth_d, &ctx->ierr, &ctx->in_vs, &ctx->in_vp, &ctx->in_rho,
                     &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc,
                     &ctx->queue, &ctx->nodefeat, &ctx->pfeat,
-                    &ctx->pout, &ctx->prop, &ctx->retry_list, &ctx->retry_ctr};
+                    &ctx->prop, &ctx->retry_list, &ctx->retry_ctr};
   for (DevBuf* b : bufs) b->release();
   for (int p = 0; p < 2; ++p) {
     ctx->plan[p].d_chains.release();
@@ -1578,7 +1577,7 @@ int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, f
   const Plan& P = ctx->plan[0];
   const int64_t rowmax = (int64_t)P.nroot * ctx->last_ncol;
   k_features<<<(n + 7) / 8, 256, 0, st>>>(0, n, ctx->last_ncol, rowmax, P.d_rootfeat.as<float4>(),
-                                          ctx->nodefeat.as<float4>(), d_rows, (__nv_bfloat16*)d_x);
+                                          ctx->nodefeat.as<float4>(), d_rows, (__nv_bfloat16*)d_x, 0);
   CK(cudaGetLastError());
   if (d_y) {
     k_targets<<<(n + 255) / 256, 256, 0, st>>>(n, rowmax, d_rows, ctx->croot.as<double>(), d_y);

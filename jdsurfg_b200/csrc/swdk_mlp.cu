@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -189,6 +190,250 @@ __global__ void __launch_bounds__(128) k_gemm_tn(int M, int N, int K, const __nv
 }
 
 // ---------------------------------------------------------------------------
+// Fused inference for the engine: one persistent CTA per SM pushes 128-row
+// tiles through all five layers.  The tile's activations stay in shared
+// memory in the SW128 K-major image the MMA descriptors read (input: 5
+// K-blocks of 64 columns, hidden: 4); weight K-blocks (N x 64, pre-swizzled
+// in global memory by k_swizzle_weights) stream through a 3-deep ring of
+// 32 KB buffers with cp.async.bulk (no multicast) and mbarrier transaction
+// counts.  Thread 0 issues copies and tcgen05.mma (M=128, N=256/64, K=16) into
+// a 256-column TMEM accumulator; 8 warps run the bias+GELU epilogue (warp w
+// reads TMEM lanes 32(w%4).., columns 128(w/4)..) and write the next layer's
+// activations back into shared memory; the output layer's epilogue turns
+// (mu, log sigma) into the bracket proposal (c = 3.5 + mu, half-width =
+// kappa sigma clamped to [2e-5 c, 0.2]).  Every wait is bounded; a timeout
+// sets *err, drains the copies in flight and releases TMEM.
+// ---------------------------------------------------------------------------
+constexpr int PX_ROWS = 128;
+constexpr int PX_KB_IN = MLP_IN / 64, PX_KB_H = MLP_H / 64;     // 5, 4
+constexpr int PX_TILE_BYTES = PX_ROWS * MLP_IN * 2;              // 80 KB input tile image
+constexpr int PX_WBUF = MLP_H * 64 * 2;                          // 32 KB weight block
+constexpr int PX_NBUF = 3;
+constexpr int PX_BLOCKS = PX_KB_IN + 3 * PX_KB_H + PX_KB_H;      // 21 weight blocks per tile
+constexpr int PX_SMEM = PX_TILE_BYTES + PX_NBUF * PX_WBUF + 1024; // + barriers, 1 KB alignment slack
+
+__device__ __forceinline__ int px_layer_of(int idx, int& kb) {
+  if (idx < PX_KB_IN) { kb = idx; return 0; }
+  idx -= PX_KB_IN;
+  kb = idx % PX_KB_H;
+  return 1 + idx / PX_KB_H;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(256, 1) k_mlp_propose(int ntiles, int nrows, const uint8_t* __restrict__ xtiles,
+                                                        const uint8_t* __restrict__ wsw, const float* __restrict__ w,
+                                                        const size_t* __restrict__ boffs, double kappa,
+                                                        float2* __restrict__ prop, int* __restrict__ err) {
+  extern __shared__ uint8_t px_raw[];
+  uint8_t* base = (uint8_t*)(((uintptr_t)px_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* act = base;                          // 80 KB activation image
+  uint8_t* wbuf = base + PX_TILE_BYTES;         // 3 x 32 KB weight ring
+  uint64_t* bars = (uint64_t*)(wbuf + PX_NBUF * PX_WBUF);
+  // bars[0..2] full, [3..5] empty, [6] accumulator ready, [7] input tile
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(256));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 8; ++i) mbar_init(&bars[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const uint32_t act_s = smem_u32(act), wbuf_s = smem_u32(wbuf);
+  const uint32_t bar_full = smem_u32(&bars[0]), bar_empty = smem_u32(&bars[3]);
+  const uint32_t bar_acc = smem_u32(&bars[6]), bar_in = smem_u32(&bars[7]);
+  // weight block idx -> global image offset and bytes
+  auto wblock = [&](int idx, size_t& off, uint32_t& bytes) {
+    int kb;
+    const int l = px_layer_of(idx, kb);
+    const int n = (l == MLP_LAYERS - 1) ? MLP_OUT : MLP_H;
+    size_t o = 0;
+    for (int q = 0; q < l; ++q) o += (size_t)MLP_H * ((q == 0) ? MLP_IN : MLP_H) * 2;
+    off = o + (size_t)kb * n * 128;
+    bytes = (uint32_t)(n * 128);
+  };
+  const int my_tiles = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const long long total = (long long)my_tiles * PX_BLOCKS;
+  long long issued = 0, consumed = 0;  // weight blocks copied / handed to the MMA (thread 0)
+  uint32_t acc_phase = 0, in_phase = 0;
+  bool ok = true, in_pending = false;
+  if (tid == 0) {
+    for (; issued < total && issued < PX_NBUF; ++issued) {
+      size_t off; uint32_t bytes;
+      wblock((int)(issued % PX_BLOCKS), off, bytes);
+      const int b = (int)(issued % PX_NBUF);
+      mbar_expect(bar_full + 8 * b, bytes);
+      bulk_g2s(wbuf_s + b * PX_WBUF, wsw + off, bytes, bar_full + 8 * b);
+    }
+  }
+  for (int it = 0; it < my_tiles; ++it) {
+    const int tile = (int)blockIdx.x + it * (int)gridDim.x;
+    if (tid == 0) {
+      mbar_expect(bar_in, PX_TILE_BYTES);
+      bulk_g2s(act_s, xtiles + (size_t)tile * PX_TILE_BYTES, PX_TILE_BYTES, bar_in);
+      in_pending = true;
+    }
+    if (!mbar_wait(&bars[7], in_phase)) ok = false;
+    else in_pending = false;
+    if (!__syncthreads_and(ok)) { ok = false; break; }
+    in_phase ^= 1u;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+      const int nkb = (l == 0) ? PX_KB_IN : PX_KB_H;
+      const int n = (l == MLP_LAYERS - 1) ? MLP_OUT : MLP_H;
+      if (tid == 0 && ok) {
+        const uint32_t idesc = (n == MLP_H) ? idesc_bf16(128, 256) : idesc_bf16(128, 64);
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+          const long long g = consumed;
+          const int b = (int)(g % PX_NBUF);
+          if (!mbar_wait(&bars[b], (uint32_t)((g / PX_NBUF) & 1))) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint64_t da = sw128_desc(act_s + kb * (PX_ROWS * 128)), db = sw128_desc(wbuf_s + b * PX_WBUF);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint32_t accf = (kb > 0 || kk > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                ::"r"(tmem), "l"(da + (uint64_t)(kk * 2)), "l"(db + (uint64_t)(kk * 2)), "r"(idesc), "r"(accf));
+          }
+          mma_commit(bar_empty + 8 * b);
+          ++consumed;
+          // refill the buffer the previous block used, once its MMAs are done
+          if (g >= 1 && issued < total) {
+            const long long gp = g - 1;
+            const int bp = (int)(gp % PX_NBUF);
+            if (!mbar_wait(&bars[3 + bp], (uint32_t)((gp / PX_NBUF) & 1))) { ok = false; break; }
+            size_t off; uint32_t bytes;
+            wblock((int)(issued % PX_BLOCKS), off, bytes);
+            mbar_expect(bar_full + 8 * bp, bytes);
+            bulk_g2s(wbuf_s + bp * PX_WBUF, wsw + off, bytes, bar_full + 8 * bp);
+            ++issued;
+          }
+        }
+        mma_commit(bar_acc);
+      }
+      if (tid == 0 && !ok) s_fail = 1;
+      __syncthreads();
+      if (s_fail) { ok = false; break; }
+      if (!mbar_wait(&bars[6], acc_phase)) ok = false;
+      acc_phase ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      if (!__syncthreads_and(ok)) { ok = false; break; }
+      const int q = warp & 3, h = warp >> 2;
+      const int r = q * 32 + lane;  // tile row = TMEM lane
+      const float* bias = w + boffs[l];
+      if (l < MLP_LAYERS - 1) {
+        for (int cb = 0; cb < 4; ++cb) {  // 32-column chunks of this warp's half
+          const int c0 = h * 128 + cb * 32;
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+          for (int j8 = 0; j8 < 4; ++j8) {  // 8 columns = one 16-byte chunk
+            uint32_t pk[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int c = c0 + j8 * 8 + 2 * e;
+              const float x0 = gelu(__uint_as_float(v[j8 * 8 + 2 * e]) + bias[c]);
+              const float x1 = gelu(__uint_as_float(v[j8 * 8 + 2 * e + 1]) + bias[c + 1]);
+              const __nv_bfloat162 b2 = __floats2bfloat162_rn(x0, x1);
+              pk[e] = *reinterpret_cast<const uint32_t*>(&b2);
+            }
+            const int c = c0 + j8 * 8;
+            const int kb = c >> 6, j = (c & 63) >> 3;
+            uint8_t* dst = act + kb * (PX_ROWS * 128) + r * 128 + ((j ^ (r & 7)) << 4);
+            *reinterpret_cast<uint4*>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;");
+      } else if (h == 0) {
+        uint32_t v2[2];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];"
+                     : "=r"(v2[0]), "=r"(v2[1])
+                     : "r"(tmem + ((uint32_t)(q * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        const long long row = (long long)tile * PX_ROWS + r;
+        if (row < nrows) {
+          const float mu = __uint_as_float(v2[0]) + bias[0];
+          const float ls = __uint_as_float(v2[1]) + bias[1];
+          const double c = 3.5 + (double)mu;
+          double hw = kappa * exp(fmin(fmax((double)ls, -12.0), 2.0));
+          hw = fmin(fmax(hw, 2.0e-5 * c), 0.2);
+          prop[row] = (mu == mu && ls == ls) ? make_float2((float)c, (float)hw) : make_float2(0.0f, 0.0f);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncthreads();
+    }
+    if (!ok) break;
+  }
+  // drain: copies still in flight and the last MMAs, then release TMEM
+  if (tid == 0) {
+    if (in_pending) mbar_wait(&bars[7], in_phase);
+    for (long long g = consumed; g < issued; ++g) mbar_wait(&bars[g % PX_NBUF], (uint32_t)((g / PX_NBUF) & 1));
+    if (consumed > 0) {
+      const long long g = consumed - 1;
+      mbar_wait(&bars[3 + g % PX_NBUF], (uint32_t)((g / PX_NBUF) & 1));
+    }
+    if (!ok) atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+}
+
+// bf16 weights (flat block, layer l: nout x kin row-major) -> the SW128
+// K-major image k_mlp_propose streams: layer by layer, K-block by K-block,
+// row n of a block at n*128 bytes, 16-byte chunk j at (j ^ (n & 7)) * 16
+__global__ void k_swizzle_weights(const __nv_bfloat16* __restrict__ wb, const size_t* __restrict__ woffs,
+                                  uint8_t* __restrict__ wsw) {
+  const int l = blockIdx.y;
+  const int kin = (l == 0) ? MLP_IN : MLP_H, n = (l == MLP_LAYERS - 1) ? MLP_OUT : MLP_H;
+  size_t o = 0;
+  for (int q = 0; q < l; ++q) o += (size_t)MLP_H * ((q == 0) ? MLP_IN : MLP_H) * 2;
+  const int nchunk = n * kin / 8;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunk; c += gridDim.x * blockDim.x) {
+    const int row = c / (kin / 8), k8 = c % (kin / 8);
+    const int kb = k8 >> 3, j = k8 & 7;
+    const uint4 v = *reinterpret_cast<const uint4*>(wb + woffs[l] + (size_t)row * kin + k8 * 8);
+    *reinterpret_cast<uint4*>(wsw + o + (size_t)kb * n * 128 + row * 128 + ((j ^ (row & 7)) << 4)) = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // elementwise kernels of the MLP
 // ---------------------------------------------------------------------------
 __global__ void k_to_bf16(int n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
@@ -288,10 +533,11 @@ struct swdk_mlp {
   __nv_bfloat16 *xin = nullptr, *h[MLP_LAYERS] = {}, *dz[MLP_LAYERS] = {}, *xt = nullptr, *dzt = nullptr,
                 *dh = nullptr;
   float *z[MLP_LAYERS] = {}, *out = nullptr, *y = nullptr, *loss = nullptr, *gscr = nullptr;
-  // inference: ping-pong activations and the final pre-activation
-  int icap = 0;
-  __nv_bfloat16 *ia = nullptr, *ib = nullptr;
-  float* iz = nullptr;
+  // fused inference: swizzled weight image, layer offsets on the device
+  uint8_t* wsw = nullptr;
+  size_t* d_offs = nullptr;  // woff[5], boff[5]
+  bool wsw_dirty = true;
+  int nsm = 0;
   int* err = nullptr;
   cudaStream_t stream = nullptr;
   std::string msg;
@@ -407,6 +653,7 @@ int swdk_mlp_create(swdk_mlp** out, int device, uint64_t seed) {
   MCK(cudaMemset(p->g, 0, off * sizeof(float)));
   MCK(cudaMemset(p->err, 0, sizeof(int)));
   k_to_bf16<<<(int)((off + 255) / 256), 256, 0, p->stream>>>((int)off, p->w, p->wb);
+  p->wsw_dirty = true;
   MCK(cudaGetLastError());
   MCK(cudaStreamSynchronize(p->stream));
   *out = p;
@@ -418,7 +665,7 @@ void swdk_mlp_destroy(swdk_mlp* p) {
   cudaSetDevice(p->device);
   if (p->stream) cudaStreamSynchronize(p->stream);
   void* bufs[] = {p->w, p->m, p->v, p->g, p->mask, p->wb, p->wt, p->loss, p->gscr, p->err, p->xin, p->xt, p->dzt,
-                  p->dh, p->out, p->y};
+                  p->dh, p->out, p->y, p->wsw, p->d_offs};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int l = 0; l < MLP_LAYERS; ++l) {
@@ -426,9 +673,6 @@ void swdk_mlp_destroy(swdk_mlp* p) {
     if (p->dz[l]) cudaFree(p->dz[l]);
     if (p->z[l]) cudaFree(p->z[l]);
   }
-  if (p->ia) cudaFree(p->ia);
-  if (p->ib) cudaFree(p->ib);
-  if (p->iz) cudaFree(p->iz);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -447,6 +691,7 @@ int swdk_mlp_set_params(swdk_mlp* p, const float* host, int64_t n) {
   MCK(cudaSetDevice(p->device));
   MCK(cudaMemcpy(p->w, host, p->nparam * sizeof(float), cudaMemcpyHostToDevice));
   k_to_bf16<<<(int)((p->nparam + 255) / 256), 256, 0, p->stream>>>((int)p->nparam, p->w, p->wb);
+  p->wsw_dirty = true;
   MCK(cudaGetLastError());
   MCK(cudaStreamSynchronize(p->stream));
   return SWDK_OK;
@@ -461,36 +706,34 @@ int swdk_gemm_bf16_tn(int M, int N, int K, const void* d_a, const void* d_b, flo
   return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
 }
 
-// inference on device features x (M x 320 bf16, M a multiple of 128) ->
-// out2 (M x 2 fp32: mu, log sigma); activations ping-pong in bf16
-int swdk_mlp_infer_rows(swdk_mlp* p, const void* d_x, int M, float* d_out2, void* stream) {
-  if (!p || !d_x || !d_out2 || M <= 0 || M % TM) return SWDK_E_ARG;
+// fused inference on tile-image features -> bracket proposals
+int swdk_mlp_propose(swdk_mlp* p, const void* d_xtiles, int nrows, double kappa, void* d_prop, void* stream) {
+  if (!p || !d_xtiles || !d_prop || nrows <= 0 || !(kappa > 0.0)) return SWDK_E_ARG;
   MCK(cudaSetDevice(p->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
-  if (M > p->icap) {
-    if (p->ia) cudaFree(p->ia);
-    if (p->ib) cudaFree(p->ib);
-    if (p->iz) cudaFree(p->iz);
-    p->ia = p->ib = nullptr;
-    p->iz = nullptr;
-    p->icap = 0;
-    MCK(cudaMalloc(&p->ia, (size_t)M * MLP_H * sizeof(__nv_bfloat16)));
-    MCK(cudaMalloc(&p->ib, (size_t)M * MLP_H * sizeof(__nv_bfloat16)));
-    MCK(cudaMalloc(&p->iz, (size_t)M * MLP_OUT * sizeof(float)));
-    p->icap = M;
+  if (st != p->stream) MCK(cudaStreamSynchronize(p->stream));  // weights written on the network's own stream
+  if (!p->wsw) {
+    size_t bytes = 0;
+    for (int l = 0; l < MLP_LAYERS; ++l) bytes += (size_t)p->nout[l] * p->kin[l] * 2;
+    MCK(cudaMalloc(&p->wsw, bytes));
+    MCK(cudaMalloc(&p->d_offs, 2 * MLP_LAYERS * sizeof(size_t)));
+    size_t h[2 * MLP_LAYERS];
+    for (int l = 0; l < MLP_LAYERS; ++l) { h[l] = p->woff[l]; h[MLP_LAYERS + l] = p->boff[l]; }
+    MCK(cudaMemcpy(p->d_offs, h, sizeof(h), cudaMemcpyHostToDevice));
+    MCK(cudaFuncSetAttribute(k_mlp_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, PX_SMEM));
+    MCK(cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device));
+    p->wsw_dirty = true;
   }
-  const __nv_bfloat16* x = (const __nv_bfloat16*)d_x;
-  __nv_bfloat16* bufs[2] = {p->ia, p->ib};
-  for (int l = 0; l < MLP_LAYERS; ++l) {
-    const bool last = (l == MLP_LAYERS - 1);
-    __nv_bfloat16* o = bufs[l & 1];
-    const int r = gemm(p, M, p->nout[l], p->kin[l], x, p->kin[l], p->wb + p->woff[l], p->kin[l], p->w + p->boff[l],
-                       last ? 0 : 1, last ? p->iz : nullptr, last ? nullptr : o, p->nout[l], st);
-    if (r) return r;
-    x = o;
+  if (p->wsw_dirty) {
+    k_swizzle_weights<<<dim3(64, MLP_LAYERS), 256, 0, st>>>(p->wb, p->d_offs, p->wsw);
+    MCK(cudaGetLastError());
+    p->wsw_dirty = false;
   }
-  MCK(cudaMemcpy2DAsync(d_out2, 2 * sizeof(float), p->iz, MLP_OUT * sizeof(float), 2 * sizeof(float), M,
-                        cudaMemcpyDeviceToDevice, st));
+  const int ntiles = (nrows + PX_ROWS - 1) / PX_ROWS;
+  const int grid = std::min(p->nsm > 0 ? p->nsm : 148, ntiles);
+  k_mlp_propose<<<grid, 256, PX_SMEM, st>>>(ntiles, nrows, (const uint8_t*)d_xtiles, p->wsw, p->w,
+                                            p->d_offs + MLP_LAYERS, kappa, (float2*)d_prop, p->err);
+  MCK(cudaGetLastError());
   return SWDK_OK;
 }
 
@@ -580,6 +823,7 @@ int swdk_mlp_train_step(swdk_mlp* p, const void* d_x, const float* d_y, int M, f
     const float c1 = 1.0f - powf(b1, (float)p->step), c2 = 1.0f - powf(b2, (float)p->step);
     k_adam<<<(int)((p->nparam + 255) / 256), 256, 0, st>>>((int)p->nparam, p->w, p->g, p->m, p->v, lr, b1, b2, 1e-8f,
                                                            c1, c2, p->mask, p->wb);
+  p->wsw_dirty = true;
     MCK(cudaGetLastError());
   }
   if (loss_out) {
@@ -647,6 +891,7 @@ int swdk_mlp_load(swdk_mlp* p, const char* path) {
   MCK(cudaMemcpy(p->v, buf.data() + 2 * p->nparam, p->nparam * 4, cudaMemcpyHostToDevice));
   p->step = step;
   k_to_bf16<<<(int)((p->nparam + 255) / 256), 256, 0, p->stream>>>((int)p->nparam, p->w, p->wb);
+  p->wsw_dirty = true;
   MCK(cudaGetLastError());
   MCK(cudaStreamSynchronize(p->stream));
   return SWDK_OK;

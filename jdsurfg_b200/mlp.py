@@ -23,7 +23,7 @@ def _bind():
     L.swdk_mlp_set_params.argtypes = [vp, vp, C.c_int64]
     L.swdk_mlp_get_grads.argtypes = [vp, vp, C.c_int64]
     L.swdk_mlp_forward.argtypes = [vp, vp, C.c_int, vp, vp]
-    L.swdk_mlp_infer_rows.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.swdk_mlp_propose.argtypes = [vp, vp, C.c_int, C.c_double, vp, vp]
     L.swdk_mlp_error_flag.argtypes = [vp, C.POINTER(C.c_int)]
     L.swdk_mlp_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.POINTER(C.c_float), vp]
     L.swdk_mlp_save.argtypes = [vp, C.c_char_p]
@@ -89,14 +89,13 @@ class MLP:
         self._check(_bind().swdk_mlp_forward(self._h, _p(x_bf16), M, _p(out), None), "forward")
         return out
 
-    def infer_rows(self, x_bf16, out=None):
-        """Inference path of the engine: M a multiple of 128, no synchronisation."""
+    def propose(self, x_tiles, nrows, kappa, prop):
+        """Fused inference on tile-image features straight to (c, half-width)
+        per row (prop: (nrows, 2) float32), on torch's current stream."""
         import torch
-        M = x_bf16.shape[0]
-        if out is None:
-            out = torch.empty((M, 2), dtype=torch.float32, device=x_bf16.device)
-        self._check(_bind().swdk_mlp_infer_rows(self._h, _p(x_bf16), M, _p(out), None), "infer_rows")
-        return out
+        st = C.c_void_p(torch.cuda.current_stream(prop.device).cuda_stream)
+        self._check(_bind().swdk_mlp_propose(self._h, _p(x_tiles), nrows, kappa, _p(prop), st), "propose")
+        return prop
 
     def error_flag(self):
         f = C.c_int(0)

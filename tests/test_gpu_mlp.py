@@ -111,3 +111,47 @@ def test_mlp_learns_and_checkpoints(tmp_path):
     net2.load(path)
     out2 = net2.forward(xb).cpu().numpy()
     np.testing.assert_array_equal(out1, out2)
+
+
+def _tile_image(x):
+    """(M, 320) bf16 rows -> the 128-row swizzled tile images swdk_mlp_propose reads."""
+    import torch
+    M = x.shape[0]
+    T = (M + 127) // 128
+    xp = torch.zeros((T * 128, 320), dtype=torch.bfloat16, device=x.device)
+    xp[:M] = x
+    # (T, 128 rows, 5 K-blocks, 8 chunks, 8 elems) -> (T, kb, r, swizzled chunk, e)
+    v = xp.view(T, 128, 5, 8, 8).permute(0, 2, 1, 3, 4).contiguous()
+    out = torch.empty_like(v)
+    r = torch.arange(128, device=x.device)
+    for j in range(8):
+        out[:, :, r, (j ^ (r % 8)), :] = v[:, :, r, j, :]
+    return out.reshape(-1)
+
+
+def test_fused_proposal_matches_training_forward():
+    """k_mlp_propose (all layers of a tile in one tcgen05 kernel, activations in
+    shared memory) against the training path's layer-by-layer forward, with a
+    ragged last tile."""
+    import torch
+    from jdsurfg_b200.mlp import MLP
+    net = MLP(device=0, seed=3)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    M = 128 * 37 + 45
+    x = (0.5 * torch.randn(M, 320, device="cuda", generator=g)).bfloat16()
+    x[:, 258:] = 0
+    torch.cuda.synchronize()
+    ref = net.forward(x).double()
+    kappa = 2.5
+    c_ref = 3.5 + ref[:, 0]
+    hw_ref = kappa * torch.exp(torch.clamp(ref[:, 1], -12.0, 2.0))
+    hw_ref = torch.maximum(hw_ref, 2e-5 * c_ref).clamp(max=0.2)
+    xt = _tile_image(x)
+    prop = torch.full((M, 2), float("nan"), device="cuda")
+    net.propose(xt, M, kappa, prop)
+    torch.cuda.synchronize()
+    assert net.error_flag() == 0
+    p = prop.double()
+    assert torch.isfinite(p).all()
+    assert (p[:, 0] - c_ref).abs().max().item() < 1e-5
+    assert ((p[:, 1] - hw_ref).abs() / hw_ref).max().item() < 1e-4
