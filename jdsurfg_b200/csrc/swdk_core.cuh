@@ -307,8 +307,7 @@ struct LayerCoef {
   double a0, cpcq, cpy, cpz, cqw, cqx, xy, xz, wy, wz, gam, gammk, rho, irho;
 };
 
-SWDK_HD LayerCoef layer_coef(const LayerView& V, int m, double wvno, double wvno2, double omega, double iom) {
-  const float4 ly = V.lay[V.idx(m)];
+SWDK_HD LayerCoef layer_coef(const float4 ly, double wvno, double wvno2, double omega, double iom) {
   LayerCoef k;
   k.irho = recip((double)ly.w);
   const double dpth = ly.x;
@@ -414,8 +413,12 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   double e4 = wvno2 - ra * rb;
   const int mlo = V.llw - 1;
   int since = 0;
+  // the next layer's float4 is loaded one layer ahead of its use
+  float4 ly = V.lay[V.idx(V.L - 2 >= mlo ? V.L - 2 : mlo)];
   for (int m = V.L - 2; m >= mlo; --m) {
-    const LayerCoef cur = layer_coef(V, m, wvno, wvno2, omega, iom);
+    const float4 cur_ly = ly;
+    if (m > mlo) ly = V.lay[V.idx(m - 1)];
+    const LayerCoef cur = layer_coef(cur_ly, wvno, wvno2, omega, iom);
     apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
     if (++since >= NORM || m == mlo) {
       since = 0;
@@ -464,8 +467,12 @@ SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
   double e1 = rho1 * rb;
   double e2 = 1.0 / (beta1 * beta1);
   int since = 0;
-  for (int m = V.L - 2; m >= V.llw - 1; --m) {
-    const float4 ly = V.lay[V.idx(m)];
+  const int mlo = V.llw - 1;
+  // the next layer's float4 is loaded one layer ahead of its use
+  float4 nx = V.lay[V.idx(V.L - 2 >= mlo ? V.L - 2 : mlo)];
+  for (int m = V.L - 2; m >= mlo; --m) {
+    const float4 ly = nx;
+    if (m > mlo) nx = V.lay[V.idx(m - 1)];
     beta1 = ly.z;
     rho1 = ly.w;
     const double dpth = ly.x;
