@@ -242,6 +242,24 @@ int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, f
  * n device doubles; exported for its accuracy test. */
 int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream);
 
+/* One call of the device path captured as a CUDA graph and replayed.
+ * path: 0 get_1d_kernel, 1 get_2d_map, 2 root search only.  Capture first
+ * runs the call once eagerly (buffers, plans, depth upload, proposal
+ * networks), then records it on the context's stream; the graph keeps the
+ * given device pointers, so a replay recomputes from their current
+ * contents.  swdk_set_periods/set_depth/set_proposal and swdk_autotune drop
+ * the graph.  Replays update no statistics. */
+int swdk_graph_capture(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                       const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status);
+int swdk_graph_launch(swdk_ctx* ctx, void* stream);
+
+/* Autotuner of the persistent root-search kernel: times the root search on
+ * the given device model for 1..k resident blocks per SM (k = occupancy
+ * limit) and one oversubscribed grid, keeps the fastest in the context and
+ * returns it in *blocks (may be NULL). */
+int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
+                  int* blocks);
+
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 

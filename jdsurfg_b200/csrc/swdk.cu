@@ -982,6 +982,12 @@ struct swdk_ctx {
   DevBuf nodefeat, pfeat, prop;
   DevBuf retry_list, retry_ctr;  // deferred retries: records and {count, queue}
   int last_ncol = 0, last_path = -1;
+  // depth vector on the device (uploaded once per swdk_set_depth)
+  const void* depth_dev = nullptr;
+  // CUDA graph of one call (swdk_graph_capture / swdk_graph_launch)
+  bool capturing = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
   int launches = 0;  // kernels launched by the current call
   // stage marks: 0 start, 1 prep, 5 proposals, 2 roots, 3 eigen, 4 call done
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -1187,21 +1193,26 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(ctx->nevals.ensure(5 * sizeof(unsigned long long)));
   if (wantfeat) CK(ctx->nodefeat.ensure((size_t)ncol * FEAT_NODES * sizeof(float4)));
   CK(ctx->depth_d.ensure((size_t)nz * sizeof(float)));
-  CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (ctx->depth_dev != ctx->depth_d.p) {  // first call after swdk_set_depth (never inside a capture)
+    if (ctx->capturing) return fail(ctx, SWDK_E_ARG, "depth not on the device before graph capture");
+    CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
+    ctx->depth_dev = ctx->depth_d.p;
+  }
   CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
-  CK(cudaEventRecord(ctx->ev[0], st));
+  const bool timing = !ctx->capturing;  // stage events and statistics only on eager calls
+  if (timing) CK(cudaEventRecord(ctx->ev[0], st));
   ctx->launches = 1;
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                              ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(ctx->ev[1], st));
+  if (timing) CK(cudaEventRecord(ctx->ev[1], st));
   if (useprop) {
     r = run_proposals(ctx, P, ncol, st);
     if (r) return r;
   }
-  CK(cudaEventRecord(ctx->ev[5], st));
+  if (timing) CK(cudaEventRecord(ctx->ev[5], st));
   if (ctx->roots_blocks == 0) {
     int dev = 0, nsm = 0, per = 0;
     CK(cudaGetDevice(&dev));
@@ -1231,7 +1242,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
                                    ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
                                    ctx->nevals.as<unsigned long long>());
   CK(cudaGetLastError());
-  CK(cudaEventRecord(ctx->ev[2], st));
+  if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
     const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
     const int nslots = (int)P.slots.size();
@@ -1243,10 +1254,12 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
                                     d_vout, d_kernel, d_status);
     CK(cudaGetLastError());
   }
-  CK(cudaEventRecord(ctx->ev[3], st));
-  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(ctx->ev[4], st));
-  ctx->stats_pending = true;
+  if (timing) {
+    CK(cudaEventRecord(ctx->ev[3], st));
+    CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(ctx->ev[4], st));
+    ctx->stats_pending = true;
+  }
   ctx->stats.nchains = (int)P.chains.size();
   ctx->stats.nslots = P.kmax;
   ctx->stats.kernel_launches = ctx->launches;
@@ -1268,6 +1281,13 @@ void collect_stats(swdk_ctx* ctx) {
   cudaEventElapsedTime(&ctx->stats.ms_proposal, ctx->ev[1], ctx->ev[5]);
   cudaEventElapsedTime(&ctx->stats.ms_roots, ctx->ev[5], ctx->ev[2]);
   cudaEventElapsedTime(&ctx->stats.ms_eigen, ctx->ev[2], ctx->ev[3]);
+}
+
+void drop_graph(swdk_ctx* ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->gexec = nullptr;
+  ctx->graph = nullptr;
 }
 
 int run_host(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
@@ -1378,6 +1398,7 @@ void swdk_destroy(swdk_ctx* ctx) {
     ctx->plan[p].d_order.release();
     ctx->plan[p].d_rootfeat.release();
   }
+  drop_graph(ctx);
   for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
@@ -1401,6 +1422,7 @@ int swdk_set_periods(swdk_ctx* ctx, const double* tRc, int ntRc, int nmRc, const
   }
   ctx->have_periods = true;
   ctx->dirty = true;
+  drop_graph(ctx);
   cudaSetDevice(ctx->cfg.device);
   return ensure_plans(ctx);
 }
@@ -1409,6 +1431,8 @@ int swdk_set_depth(swdk_ctx* ctx, const float* depth, int nz) {
   if (!ctx || !depth || nz < 2) return SWDK_E_ARG;
   if (nz > SWDK_MAX_NZ) return fail(ctx, SWDK_E_LIMIT, "nz > SWDK_MAX_NZ");
   ctx->depth.assign(depth, depth + nz);
+  ctx->depth_dev = nullptr;
+  drop_graph(ctx);
   return SWDK_OK;
 }
 
@@ -1527,6 +1551,7 @@ int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, co
 int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double kappa_rayleigh, double kappa_love) {
   if (!ctx || !(kappa_rayleigh > 0.0) || !(kappa_rayleigh < 1.0e3) || !(kappa_love > 0.0) || !(kappa_love < 1.0e3))
     return fail(ctx, SWDK_E_ARG, "bad arguments");
+  drop_graph(ctx);
   ctx->net[0] = rayleigh;
   ctx->net[1] = love;
   ctx->kappa[0] = kappa_rayleigh;
@@ -1583,6 +1608,81 @@ int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, f
     k_targets<<<(n + 255) / 256, 256, 0, st>>>(n, rowmax, d_rows, ctx->croot.as<double>(), d_y);
     CK(cudaGetLastError());
   }
+  return SWDK_OK;
+}
+
+int swdk_graph_capture(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+                       const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status) {
+  if (!ctx || path < 0 || path > 2) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  CK(cudaSetDevice(ctx->cfg.device));
+  drop_graph(ctx);
+  cudaStream_t st = ctx->stream;
+  // one eager call sizes every buffer, builds the plans, uploads the depth
+  // vector and prepares the proposal networks, so the captured call
+  // allocates nothing and copies nothing from pageable memory
+  int r = run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  if (r) return r;
+  CK(cudaStreamSynchronize(st));
+  collect_stats(ctx);
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  ctx->capturing = true;
+  r = run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  ctx->capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (r) {
+    if (g) cudaGraphDestroy(g);
+    return r;
+  }
+  if (e != cudaSuccess) return fail(ctx, SWDK_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  ctx->graph = g;
+  CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
+  return SWDK_OK;
+}
+
+int swdk_graph_launch(swdk_ctx* ctx, void* stream) {
+  if (!ctx || !ctx->gexec) return fail(ctx, SWDK_E_ARG, "no captured graph");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaGraphLaunch(ctx->gexec, stream ? (cudaStream_t)stream : ctx->stream));
+  return SWDK_OK;
+}
+
+int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
+                  int* blocks_out) {
+  if (!ctx) return SWDK_E_ARG;
+  CK(cudaSetDevice(ctx->cfg.device));
+  drop_graph(ctx);
+  cudaStream_t st = ctx->stream;
+  int dev = 0, nsm = 0, per = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0));
+  per = std::max(1, per);
+  // candidates: resident blocks of the persistent root kernel, 1..per per SM
+  // plus one oversubscribed grid (queue items then also spread over waves)
+  std::vector<int> cand;
+  for (int k = 1; k <= per; ++k) cand.push_back(k * nsm);
+  cand.push_back(2 * per * nsm);
+  const int saved = ctx->cfg.block_roots;
+  int best = 0;
+  float best_ms = 1e30f;
+  // warm-up (plans, buffers), then each candidate timed on its own call
+  ctx->cfg.block_roots = cand.back();
+  int r = run_device(ctx, 2, nx, ny, nz, d_vs, d_vp, d_rho, nullptr, nullptr, nullptr, nullptr, st);
+  if (r) { ctx->cfg.block_roots = saved; return r; }
+  CK(cudaStreamSynchronize(st));
+  collect_stats(ctx);
+  for (int b : cand) {
+    ctx->cfg.block_roots = b;
+    r = run_device(ctx, 2, nx, ny, nz, d_vs, d_vp, d_rho, nullptr, nullptr, nullptr, nullptr, st);
+    if (r) { ctx->cfg.block_roots = saved; return r; }
+    CK(cudaStreamSynchronize(st));
+    collect_stats(ctx);
+    const float ms = ctx->stats.ms_roots;
+    if (ms < best_ms) { best_ms = ms; best = b; }
+  }
+  ctx->cfg.block_roots = best;
+  if (blocks_out) *blocks_out = best;
   return SWDK_OK;
 }
 

@@ -711,7 +711,8 @@ int swdk_mlp_propose(swdk_mlp* p, const void* d_xtiles, int nrows, double kappa,
   if (!p || !d_xtiles || !d_prop || nrows <= 0 || !(kappa > 0.0)) return SWDK_E_ARG;
   MCK(cudaSetDevice(p->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
-  if (st != p->stream) MCK(cudaStreamSynchronize(p->stream));  // weights written on the network's own stream
+  // every call that writes the weights (create, set_params, load, train_step)
+  // has finished its work on the network's stream before returning
   if (!p->wsw) {
     size_t bytes = 0;
     for (int l = 0; l < MLP_LAYERS; ++l) bytes += (size_t)p->nout[l] * p->kin[l] * 2;

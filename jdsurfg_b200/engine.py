@@ -69,6 +69,9 @@ def lib():
         L.swdk_root_slots.argtypes = [vp, C.POINTER(C.c_int), vp, vp, vp]
         L.swdk_last_roots.argtypes = [vp, vp, vp]
         L.swdk_training_rows.argtypes = [vp, vp, C.c_int, vp, vp, vp]
+        L.swdk_graph_capture.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int] + [vp] * 7
+        L.swdk_graph_launch.argtypes = [vp, vp]
+        L.swdk_autotune.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int)]
         L.swdk_last_error.argtypes = [vp]
         L.swdk_last_error.restype = C.c_char_p
         _LIB = L
@@ -248,6 +251,21 @@ class Engine:
         after roots_device; rows is an int64 device tensor."""
         self._check(lib().swdk_training_rows(self._h, _p(rows), rows.shape[0], _p(x), _p(y), stream),
                     "swdk_training_rows")
+
+    # -- CUDA graph of one device call, autotuner ------------------------------
+    PATHS = {"kernel": 0, "map": 1, "roots": 2}
+
+    def graph_capture(self, path, nx, ny, nz, vs, vp, rho, vc=None, vout=None, kernel=None, status=None):
+        self._check(lib().swdk_graph_capture(self._h, self.PATHS[path], nx, ny, nz, _p(vs), _p(vp), _p(rho), _p(vc),
+                                             _p(vout), _p(kernel), _p(status)), "swdk_graph_capture")
+
+    def graph_launch(self, stream=None):
+        self._check(lib().swdk_graph_launch(self._h, stream), "swdk_graph_launch")
+
+    def autotune(self, nx, ny, nz, vs, vp=None, rho=None):
+        b = C.c_int(0)
+        self._check(lib().swdk_autotune(self._h, nx, ny, nz, _p(vs), _p(vp), _p(rho), C.byref(b)), "swdk_autotune")
+        return b.value
 
     def stats(self):
         s = Stats()
