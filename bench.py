@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny"])
     ap.add_argument("--proposal", default="learned", choices=["learned", "none"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-scan comparison timing")
+    ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
     ap.add_argument("--ncols", type=int, default=0, help="use only the first N columns (profiling)")
     ap.add_argument("--refine", default="tight", choices=["tight", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -261,31 +262,48 @@ def main():
     ker = torch.empty((kmax, nz, ncol), dtype=torch.float64, device=dev)
     st = torch.empty((kmax, ncol), dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # one explicit stream for the flush, the engine's work and the timing
+    # events (a NULL stream handle would mean the engine's own stream)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step():
         flush.fill_(1)
         eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
 
+    roots_blocks = eng.autotune(nx, ny, nz, vs, vp, rho) if not args.no_graph else None
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
+    STAT_KEYS = ("ms_roots", "ms_proposal", "ms_eigen", "ms_prep", "secular_evals", "layer_evals_rayleigh",
+                 "layer_evals_love", "proposals_accepted", "proposals_rejected", "kernel_launches")
+
     def timed(nsteps):
-        """device time of nsteps steps (max over ranks) and summed stage stats"""
+        """device time of nsteps steps (max over ranks) and stage stats per step x nsteps.
+        The per-stage figures come from one eager probe call (CUDA events inside the
+        engine); the timed steps replay the captured CUDA graph of that call."""
+        step()
+        probe = eng.stats()
+        acc = {k: probe[k] * nsteps for k in STAT_KEYS}
+        use_graph = not args.no_graph
+        if use_graph:
+            eng.graph_capture("kernel", nx, ny, nz, vs, vp, rho, vc, vout, ker, st)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        acc = dict(ms_roots=0.0, ms_proposal=0.0, ms_eigen=0.0, ms_prep=0.0, secular_evals=0,
-                   layer_evals_rayleigh=0, layer_evals_love=0, proposals_accepted=0, proposals_rejected=0,
-                   kernel_launches=0)
         e0.record(stream)
         for _ in range(nsteps):
-            step()
-            s = eng.stats()  # synchronises on the engine's work; collects per-stage events
-            for k in acc:
-                acc[k] += s[k]
+            if use_graph:
+                flush.fill_(1)
+                eng.graph_launch(sptr)
+            else:
+                step()
         e1.record(stream)
         torch.cuda.synchronize()
         if pg:
@@ -312,7 +330,7 @@ def main():
     alg_lr, alg_ll = lr, ll  # algorithmic layer-evaluations: the plain method's count
     if args.proposal == "learned" and not args.no_plain:
         eng.set_proposal(None, None)
-        for _ in range(2):
+        for _ in range(1):
             step()
         torch.cuda.synchronize()
         if pg:
@@ -412,7 +430,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py); no public dataset exists for this path",
-                "config": case_desc(args, case, kmax), "clocks": clk, "e2e": e2e,
+                "config": dict(case_desc(args, case, kmax), timed_as="eager calls" if args.no_graph else
+                               "CUDA-graph replays of one get_1d_kernel_device call",
+                               roots_blocks_autotuned=roots_blocks), "clocks": clk, "e2e": e2e,
                 "gpu_launches": int(acc["kernel_launches"]), "roofline": roofline, "cpu_baseline": cb,
                 "plain": plain,
                 "detail": {"secular_evals_per_step": evals / args.steps,
