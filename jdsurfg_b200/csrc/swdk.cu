@@ -11,7 +11,8 @@
 //              surfdisp96 call (wave, period list, modes 1..M) with the
 //              reference's retry (surfdisp.cpp:94-109); identical chains of
 //              different slot types are computed once.
-//   k_eigen  : one block per column, one thread per output slot: sregn96 /
+//   k_eigen  : one block per (column, wave-type group of output slots), one
+//              thread per slot: sregn96 /
 //              sregnpu / slegn96 / slegnpu passes, sphericity, _ParamConvert
 //              and the empirical chain rule (SurfaceWave.cpp:491-500).
 #include <cuda_bf16.h>
@@ -52,6 +53,15 @@ struct ChainDesc {
   int iwave;    // 1 Love, 2 Rayleigh
   int igr;      // surfdisp96 igr
   int out_off;  // root slot of (mode 1, period 0)
+};
+
+// output slots grouped by wave type (Rc, Rg, Lc, Lg order); the eigen
+// kernel runs one block per (column, group), so a block's warps all do the
+// same kind of pass and finish together
+struct SlotGroups {
+  int n;         // non-empty groups
+  int start[4];  // first slot of group g in the plan's slot array
+  int count[4];  // slots of group g
 };
 
 struct SlotDesc {
@@ -676,7 +686,7 @@ __global__ void k_copy_last_mode(int nmodel, int kmax, int mode, const double* _
 }
 
 // ---------------------------------------------------------------------------
-// k_eigen: one block per column, threads over output slots
+// k_eigen: one block per (column, slot group), threads over the group's slots
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int worst_status(int a, int b) {
   // NO_ROOT / NAN dominate, then ITER_LIMIT, then RETRIED
@@ -695,7 +705,7 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
 
 __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                                const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
-                                               const SlotDesc* __restrict__ slots, int nslots,
+                                               const SlotDesc* __restrict__ slots, const SlotGroups groups,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
                                                int sphere, int path, double* __restrict__ vc, double* __restrict__ vout,
                                                double* __restrict__ kernel, int32_t* __restrict__ status) {
@@ -760,8 +770,9 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
   sink.L = L;
   sink.nw = ci.nw;
   const NodeSink nosink = {nullptr, crs, L, ci.nw};
-  for (int s = threadIdx.x; s < nslots; s += blockDim.x) {
-    const SlotDesc sd = slots[s];
+  const int g0 = groups.start[blockIdx.y], gn = groups.count[blockIdx.y];
+  for (int s = threadIdx.x; s < gn; s += blockDim.x) {
+    const SlotDesc sd = slots[g0 + s];
     const bool love = sd.wtype >= 2;
     const bool group = (sd.wtype == 1 || sd.wtype == 3);
     const double c0 = croot[(size_t)sd.r0 * ncol + col];
@@ -948,7 +959,8 @@ struct Plan {
   DevBuf d_order;
   std::vector<ChainDesc> chains;
   std::vector<double> periods;
-  std::vector<SlotDesc> slots;
+  std::vector<SlotDesc> slots;  // grouped by wave type
+  SlotGroups groups;
   std::vector<float4> rootfeat;  // per root slot: (log T / log 100, mode / 2, Rayleigh, 0)
   std::vector<int> rootwave, rootmode;
   std::vector<double> rootperiod;
@@ -1105,6 +1117,16 @@ int build_plan(swdk_ctx* ctx, int path) {
     P.slots.push_back(s);
   }
   if (P.chains.empty()) return fail(ctx, SWDK_E_NOPERIODS, "no periods");
+  std::stable_sort(P.slots.begin(), P.slots.end(), [](const SlotDesc& a, const SlotDesc& b) { return a.wtype < b.wtype; });
+  P.groups.n = 0;
+  for (size_t i = 0; i < P.slots.size(); ++i) {
+    if (i == 0 || P.slots[i].wtype != P.slots[i - 1].wtype) {
+      P.groups.start[P.groups.n] = (int)i;
+      P.groups.count[P.groups.n] = 0;
+      ++P.groups.n;
+    }
+    ++P.groups.count[P.groups.n - 1];
+  }
   P.order.clear();
   for (int w = 2; w >= 1; --w)
     for (size_t i = 0; i < P.chains.size(); ++i)
@@ -1245,11 +1267,12 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
     const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
-    const int nslots = (int)P.slots.size();
-    const int et = std::min(128, ((nslots + 31) / 32) * 32);
+    int gmax = 0;
+    for (int g = 0; g < P.groups.n; ++g) gmax = std::max(gmax, P.groups.count[g]);
+    const int et = std::min(128, ((gmax + 31) / 32) * 32);
     ctx->launches += 1;
-    k_eigen<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                    ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), nslots,
+    k_eigen<<<dim3(ncol, P.groups.n), et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                    ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), P.groups,
                                     ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
                                     d_vout, d_kernel, d_status);
     CK(cudaGetLastError());
