@@ -153,6 +153,15 @@ int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, co
                              const int32_t* d_row_slot, const float* d_fdm, int32_t* d_nnz, int32_t* d_indices,
                              float* d_values, void* stream);
 
+/* The same rows as CSR: d_rowptr[nrows+1] (int64, device) and the
+ * compacted indices/values of all rows in row order (capacity entries
+ * available).  Two passes: counts and their prefix sum, then the rows; the
+ * total number of nonzeros is returned in *nnz_total (the call waits for the
+ * count), SWDK_E_LIMIT if it exceeds capacity (call again with enough). */
+int swdk_frechet_csr_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, const double* d_kernel, int nrows,
+                            const int32_t* d_row_slot, const float* d_fdm, int64_t* d_rowptr, int32_t* d_indices,
+                            float* d_values, int64_t capacity, int64_t* nnz_total, void* stream);
+
 /* surfdisp96_ for callers that cannot allocate device memory.
  *
  * No counterpart in the reference: it is swdk_surfdisp96_batch on device
@@ -252,6 +261,25 @@ int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream);
 int swdk_graph_capture(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
                        const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status);
 int swdk_graph_launch(swdk_ctx* ctx, void* stream);
+
+/* Many models in one CUDA graph (uneven batches: different grids, depth
+ * vectors, period tables, modes).  Each model has its own context (its
+ * plans and buffers) and call; the graph forks one branch per context off a
+ * main stream and joins them, so small models run concurrently.  The
+ * contexts must be distinct and on one device.  As swdk_graph_capture, it
+ * first runs every call once eagerly.  A NULL stream launches on the
+ * graph's own stream. */
+typedef struct swdk_call {
+  int path; /* 0 get_1d_kernel, 1 get_2d_map, 2 root search only */
+  int nx, ny, nz;
+  const float *d_vs, *d_vp, *d_rho;
+  double *d_vc, *d_vout, *d_kernel;
+  int32_t* d_status;
+} swdk_call;
+typedef struct swdk_graph swdk_graph;
+int swdk_batch_graph_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swdk_graph** out);
+int swdk_batch_graph_launch(swdk_graph* graph, void* stream);
+void swdk_batch_graph_destroy(swdk_graph* graph);
 
 /* Autotuner of the persistent root-search kernel: times the root search on
  * the given device model for 1..k resident blocks per SM (k = occupancy

@@ -891,9 +891,11 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
 // ---------------------------------------------------------------------------
 // Frechet rows (SurfaceWave.cpp:630-659): one block per row
 // ---------------------------------------------------------------------------
+// rowptr == null: row r at r * n (padded rows); else at rowptr[r] (CSR).
+// count_only: only nnz[r] is written.
 __global__ void k_frechet(int nx, int ny, int nz, int kmax, const double* __restrict__ kernel, const int32_t* __restrict__ slot,
                           const float* __restrict__ fdm, int32_t* __restrict__ nnz, int32_t* __restrict__ idx,
-                          float* __restrict__ val) {
+                          float* __restrict__ val, const int64_t* __restrict__ rowptr, int count_only) {
   const int r = blockIdx.x;
   const int nxi = nx - 2, nyi = ny - 2;
   const int n = nxi * nyi * (nz - 1);
@@ -904,8 +906,9 @@ __global__ void k_frechet(int nx, int ny, int nz, int kmax, const double* __rest
     return;
   }
   const float* f = fdm + (size_t)r * ncol;
-  int32_t* oi = idx + (size_t)r * n;
-  float* ov = val + (size_t)r * n;
+  const size_t o0 = rowptr ? (size_t)rowptr[r] : (size_t)r * n;
+  int32_t* oi = count_only ? nullptr : idx + o0;
+  float* ov = count_only ? nullptr : val + o0;
   __shared__ int base;
   __shared__ int wsum[32];
   if (threadIdx.x == 0) base = 0;
@@ -927,12 +930,36 @@ __global__ void k_frechet(int nx, int ny, int nz, int kmax, const double* __rest
     __syncthreads();
     int off = 0, tot = 0;
     for (int w = 0; w < nw; ++w) { if (w < wid) off += wsum[w]; tot += wsum[w]; }
-    if (keep) { oi[base + off + wpre] = j; ov[base + off + wpre] = v; }
+    if (keep && !count_only) { oi[base + off + wpre] = j; ov[base + off + wpre] = v; }
     __syncthreads();
     if (threadIdx.x == 0) base += tot;
     __syncthreads();
   }
-  if (threadIdx.x == 0) nnz[r] = base;
+  if (threadIdx.x == 0 && nnz) nnz[r] = base;
+}
+
+// exclusive prefix sum of nnz[0..n) into rowptr[0..n] (one block)
+__global__ void k_rowptr(int n, const int32_t* __restrict__ nnz, int64_t* __restrict__ rowptr) {
+  __shared__ long long part[1024];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int a = 0; a < n; a += blockDim.x) {
+    const int i = a + threadIdx.x;
+    part[threadIdx.x] = (i < n) ? nnz[i] : 0;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {  // Hillis-Steele inclusive scan
+      const long long v = (threadIdx.x >= (unsigned)o) ? part[threadIdx.x - o] : 0;
+      __syncthreads();
+      part[threadIdx.x] += v;
+      __syncthreads();
+    }
+    if (i < n) rowptr[i + 1] = carry + part[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += part[threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rowptr[0] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1566,7 +1593,40 @@ int swdk_frechet_rows_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, co
   if (nrows == 0) return SWDK_OK;
   CK(cudaSetDevice(ctx->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, d_nnz, d_indices, d_values);
+  k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, d_nnz, d_indices, d_values, nullptr,
+                                   0);
+  CK(cudaGetLastError());
+  return SWDK_OK;
+}
+
+int swdk_frechet_csr_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, const double* d_kernel, int nrows,
+                            const int32_t* d_row_slot, const float* d_fdm, int64_t* d_rowptr, int32_t* d_indices,
+                            float* d_values, int64_t capacity, int64_t* nnz_total, void* stream) {
+  if (!ctx || nx < 3 || ny < 3 || nz < 2 || kmax <= 0 || nrows < 0 || !d_kernel || !d_row_slot || !d_fdm ||
+      !d_rowptr || capacity < 0 || (capacity > 0 && (!d_indices || !d_values)))
+    return fail(ctx, SWDK_E_ARG, "bad arguments");
+  CK(cudaSetDevice(ctx->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  if (nrows == 0) {
+    CK(cudaMemsetAsync(d_rowptr, 0, sizeof(int64_t), st));
+    if (nnz_total) *nnz_total = 0;
+    return SWDK_OK;
+  }
+  CK(ctx->in_misc.ensure((size_t)nrows * sizeof(int32_t)));
+  int32_t* cnt = ctx->in_misc.as<int32_t>();
+  // pass 1: entries per row; prefix sum into the row pointer
+  k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, cnt, nullptr, nullptr, nullptr, 1);
+  CK(cudaGetLastError());
+  k_rowptr<<<1, 1024, 0, st>>>(nrows, cnt, d_rowptr);
+  CK(cudaGetLastError());
+  int64_t total = 0;
+  CK(cudaMemcpyAsync(&total, d_rowptr + nrows, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (nnz_total) *nnz_total = total;
+  if (total > capacity) return fail(ctx, SWDK_E_LIMIT, "CSR capacity below the number of nonzeros");
+  // pass 2: the rows, compacted
+  k_frechet<<<nrows, 256, 0, st>>>(nx, ny, nz, kmax, d_kernel, d_row_slot, d_fdm, nullptr, d_indices, d_values,
+                                   d_rowptr, 0);
   CK(cudaGetLastError());
   return SWDK_OK;
 }
@@ -1661,6 +1721,97 @@ int swdk_graph_capture(swdk_ctx* ctx, int path, int nx, int ny, int nz, const fl
   ctx->graph = g;
   CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
   return SWDK_OK;
+}
+
+struct swdk_graph {
+  int device = 0;
+  cudaStream_t main = nullptr;
+  std::vector<cudaEvent_t> events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+void swdk_batch_graph_destroy(swdk_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (cudaEvent_t e : g->events)
+    if (e) cudaEventDestroy(e);
+  if (g->main) cudaStreamDestroy(g->main);
+  delete g;
+}
+
+int swdk_batch_graph_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swdk_graph** out) {
+  if (!out || n <= 0 || !ctxs || !calls) return SWDK_E_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i] || calls[i].path < 0 || calls[i].path > 2 || ctxs[i]->cfg.device != ctxs[0]->cfg.device)
+      return SWDK_E_ARG;
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return fail(ctxs[i], SWDK_E_ARG, "a context appears twice in one batch graph");
+  }
+  swdk_graph* g = new swdk_graph();
+  g->device = ctxs[0]->cfg.device;
+  auto bail = [&](swdk_ctx* c, int code, const std::string& msg) {
+    swdk_batch_graph_destroy(g);
+    return fail(c, code, msg);
+  };
+  swdk_ctx* ctx = ctxs[0];  // for CK's error text
+  cudaError_t e = cudaSetDevice(g->device);
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, cudaGetErrorString(e));
+  // eager pass: every context sizes its buffers, builds its plans, uploads
+  // its depth vector and prepares its proposal networks
+  for (int i = 0; i < n; ++i) {
+    const swdk_call& c = calls[i];
+    drop_graph(ctxs[i]);
+    const int r = run_device(ctxs[i], c.path, c.nx, c.ny, c.nz, c.d_vs, c.d_vp, c.d_rho, c.d_vc, c.d_vout, c.d_kernel,
+                             c.d_status, ctxs[i]->stream);
+    if (r) { swdk_batch_graph_destroy(g); return r; }
+  }
+  for (int i = 0; i < n; ++i) {
+    e = cudaStreamSynchronize(ctxs[i]->stream);
+    if (e != cudaSuccess) return bail(ctxs[i], SWDK_E_CUDA, cudaGetErrorString(e));
+    collect_stats(ctxs[i]);
+  }
+  // capture: fork every context's stream off one main stream, join them back
+  e = cudaStreamCreateWithFlags(&g->main, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, cudaGetErrorString(e));
+  g->events.assign(n + 1, nullptr);
+  for (int i = 0; i <= n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->events[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, cudaGetErrorString(e));
+  e = cudaStreamBeginCapture(g->main, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, cudaGetErrorString(e));
+  int r = SWDK_OK;
+  e = cudaEventRecord(g->events[n], g->main);
+  for (int i = 0; i < n && e == cudaSuccess && r == SWDK_OK; ++i) {
+    const swdk_call& c = calls[i];
+    e = cudaStreamWaitEvent(ctxs[i]->stream, g->events[n], 0);
+    if (e != cudaSuccess) break;
+    ctxs[i]->capturing = true;
+    r = run_device(ctxs[i], c.path, c.nx, c.ny, c.nz, c.d_vs, c.d_vp, c.d_rho, c.d_vc, c.d_vout, c.d_kernel, c.d_status,
+                   ctxs[i]->stream);
+    ctxs[i]->capturing = false;
+    if (r) break;
+    e = cudaEventRecord(g->events[i], ctxs[i]->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->main, g->events[i], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(g->main, &graph);
+  g->graph = graph;
+  if (r) { swdk_batch_graph_destroy(g); return r; }
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+  if (e2 != cudaSuccess) return bail(ctx, SWDK_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e2));
+  e = cudaGraphInstantiate(&g->exec, graph, 0);
+  if (e != cudaSuccess) return bail(ctx, SWDK_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  *out = g;
+  return SWDK_OK;
+}
+
+int swdk_batch_graph_launch(swdk_graph* g, void* stream) {
+  if (!g || !g->exec) return SWDK_E_ARG;
+  if (cudaSetDevice(g->device) != cudaSuccess) return SWDK_E_CUDA;
+  return cudaGraphLaunch(g->exec, stream ? (cudaStream_t)stream : g->main) == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
 }
 
 int swdk_graph_launch(swdk_ctx* ctx, void* stream) {

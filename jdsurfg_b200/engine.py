@@ -30,6 +30,13 @@ class Config(C.Structure):
                 ("sphere", C.c_int), ("block_roots", C.c_int)]
 
 
+class Call(C.Structure):
+    """swdk_call: one model's device call inside a batch graph."""
+    _fields_ = [("path", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("d_vs", C.c_void_p), ("d_vp", C.c_void_p), ("d_rho", C.c_void_p),
+                ("d_vc", C.c_void_p), ("d_vout", C.c_void_p), ("d_kernel", C.c_void_p), ("d_status", C.c_void_p)]
+
+
 class Stats(C.Structure):
     _fields_ = [("secular_evals", C.c_int64), ("layer_evals_rayleigh", C.c_int64), ("layer_evals_love", C.c_int64),
                 ("nchains", C.c_int32), ("nslots", C.c_int32),
@@ -72,6 +79,12 @@ def lib():
         L.swdk_graph_capture.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int] + [vp] * 7
         L.swdk_graph_launch.argtypes = [vp, vp]
         L.swdk_autotune.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int)]
+        L.swdk_frechet_csr_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp,
+                                              C.c_int64, C.POINTER(C.c_int64), vp]
+        L.swdk_batch_graph_create.argtypes = [C.c_int, vp, vp, C.POINTER(vp)]
+        L.swdk_batch_graph_launch.argtypes = [vp, vp]
+        L.swdk_batch_graph_destroy.argtypes = [vp]
+        L.swdk_batch_graph_destroy.restype = None
         L.swdk_last_error.argtypes = [vp]
         L.swdk_last_error.restype = C.c_char_p
         _LIB = L
@@ -251,6 +264,15 @@ class Engine:
         after roots_device; rows is an int64 device tensor."""
         self._check(lib().swdk_training_rows(self._h, _p(rows), rows.shape[0], _p(x), _p(y), stream),
                     "swdk_training_rows")
+
+    def frechet_csr_device(self, nx, ny, nz, kmax, kernel, row_slot, fdm, rowptr, indices, values, stream=None):
+        """Frechet rows as CSR on the device; returns the number of nonzeros."""
+        tot = C.c_int64(0)
+        cap = 0 if indices is None else indices.numel()
+        self._check(lib().swdk_frechet_csr_device(self._h, nx, ny, nz, kmax, _p(kernel), len(row_slot), _p(row_slot),
+                                                  _p(fdm), _p(rowptr), _p(indices), _p(values), cap, C.byref(tot),
+                                                  stream), "swdk_frechet_csr_device")
+        return tot.value
 
     # -- CUDA graph of one device call, autotuner ------------------------------
     PATHS = {"kernel": 0, "map": 1, "roots": 2}

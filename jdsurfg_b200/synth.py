@@ -145,3 +145,34 @@ def subset_columns(case, cols):
     out["vp"] = None if case["vp"] is None else np.ascontiguousarray(case["vp"][:, cols])
     out["rho"] = None if case["rho"] is None else np.ascontiguousarray(case["rho"][:, cols])
     return out
+
+
+def make_uneven_batch(nmodels=48, seed=5150, small=False, max_kernel_bytes=2 << 30):
+    """Independent models of one inversion iteration with uneven shapes:
+    grids 32x32..200x200 columns, 24..80 nodes (1 km to 20 km, then 2.5 km),
+    15..60 log-spaced periods inside 1..100 s, one or two of Rc/Rg/Lc/Lg,
+    modes 0..2; LVZ in 20 % and fluid nodes in 10 % of the columns of each
+    model.  small=True shrinks grids (8..20) and nodes (24..40) for tests.
+    The period count is lowered where a model's kernel would exceed
+    max_kernel_bytes."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(nmodels):
+        lo, hi = (8, 21) if small else (32, 201)
+        nx, ny = (int(v) for v in rng.integers(lo, hi, 2))
+        nz = int(rng.integers(24, 41 if small else 81))
+        depth = depth_grid(21, 1.0, nz, 2.5)
+        nt = int(rng.integers(15, 61))
+        tmin = float(np.exp(rng.uniform(np.log(1.0), np.log(5.0))))
+        tmax = float(np.exp(rng.uniform(np.log(30.0), np.log(100.0))))
+        k = int(rng.integers(1, 3))
+        waves = tuple(sorted((str(w) for w in rng.choice(WAVES, size=k, replace=False)), key=WAVES.index))
+        nmode = int(rng.integers(1, 4))
+        per_slot = nx * ny * nz * 8
+        nt = max(15, min(nt, max_kernel_bytes // max(1, per_slot * k * nmode)))
+        periods = np.geomspace(tmin, tmax, nt)
+        c = make_case(nx, ny, depth, 2.5, 4.7, 0.08, periods, waves, nmode, seed * 1000 + i, lvz_frac=0.2,
+                      water_frac=0.1)
+        c["waves"], c["nmode"] = waves, nmode
+        cases.append(c)
+    return cases

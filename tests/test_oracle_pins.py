@@ -194,3 +194,33 @@ def test_frechet_rows_layout():
     np.testing.assert_array_equal(val, (0.5 * ker[1, :nz - 1, 1 * nx + 2]).astype(np.float32))
     idx, val = rows[1]
     assert len(idx) == 2 * (nz - 1)
+
+
+def test_frechet_file_round_trip():
+    """The reference's row-file layout (SurfaceWave.cpp:596-603, 641-659) from
+    CSR rows of the oracle, read back record by record."""
+    import tempfile, os
+    from jdsurfg_b200.frechet_file import write_frechet, read_frechet
+    rng = np.random.default_rng(4)
+    nx, ny, nz, kmax = 6, 5, 4, 3
+    kernel = rng.standard_normal((kmax, nz, nx * ny))
+    kernel[:, :, ::7] = 0.0
+    row_slot = np.array([0, 2, 1, 2], np.int32)
+    fdm = rng.standard_normal((len(row_slot), nx * ny)).astype(np.float32)
+    fdm[1, :] = 0.0  # a row without entries
+    rows = O.frechet_rows(nx, ny, nz, kernel, row_slot, fdm)
+    rowptr = np.concatenate([[0], np.cumsum([len(i) for i, _ in rows])])
+    idx = np.concatenate([i for i, _ in rows]) if rowptr[-1] else np.zeros(0, np.int32)
+    val = np.concatenate([v for _, v in rows]) if rowptr[-1] else np.zeros(0, np.float32)
+    n = (nx - 2) * (ny - 2) * (nz - 1)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "frechet.0")
+        write_frechet(p, 17, n, np.arange(10, 10 + len(rows)), rowptr, idx, val)
+        assert os.path.getsize(p) == 8 + sum(8 + 8 * len(i) for i, _ in rows)
+        m, n2, back = read_frechet(p)
+    assert (m, n2) == (17, n)
+    for r, ((i0, v0), (rid, i1, v1)) in enumerate(zip(rows, back)):
+        assert rid == 10 + r
+        assert np.array_equal(i0, i1) and np.array_equal(v0, v1)
+        assert np.all(np.diff(i1) > 0) and np.all(np.abs(v1) > 0)
+    assert len(back[1][1]) == 0
