@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="swdk", choices=["swdk", "reference"])
-    ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny"])
+    ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny", "uneven"])
     ap.add_argument("--proposal", default="learned", choices=["learned", "none"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-scan comparison timing")
     ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
@@ -82,6 +82,8 @@ WORKLOAD_TEXT = {
     "production": "128x128 columns x 48 nodes, 40 periods 1-60 s, Rayleigh+Love modes 0-1 phase+group, water",
     "small": "16x16 columns x 20 nodes, 25 periods 2-40 s, Rayleigh mode 0 phase+group",
     "tiny": "4x3 columns x 12 nodes, 6 periods, all wave types",
+    "uneven": "48 models, grids 32x32..200x200, 24..80 nodes, 15..60 periods in 1..100 s, 1-2 of Rc/Rg/Lc/Lg, "
+              "modes 0..2, one CUDA graph",
 }
 
 
@@ -229,6 +231,59 @@ def run_reference(args):
     return 0
 
 
+def run_uneven(args, torch, dev, rank, world, pg):
+    """One step = one CUDA-graph launch over the 48-model uneven batch."""
+    from jdsurfg_b200 import synth
+    from jdsurfg_b200.batch import UnevenBatch
+    cases = synth.make_uneven_batch(48, seed=5150 + rank)
+    B = UnevenBatch(cases, learned=(args.proposal == "learned"))
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    B.capture()
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        B.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        flush.fill_(1)
+        B.launch(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    units = B.units
+    launches = sum(e.stats()["kernel_launches"] for e in B.engines)  # per model, from the eager pass
+    kb = sum(c["nx"] * c["ny"] * c["nz"] * e.kmax * 8 for c, e in zip(cases, B.engines))
+    if rank == 0:
+        line = {"metric": METRIC, "value": world * units / (ms / args.steps * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_uneven_batch)",
+                "config": {"workload": "uneven", "what": WORKLOAD_TEXT["uneven"], "models": len(cases),
+                           "slots_per_step": units, "kernel_bytes": kb, "proposal": args.proposal,
+                           "timed_as": "one CUDA graph launch per step (a branch per model)",
+                           "l2": "flushed between steps (256 MiB write)"},
+                "clocks": clk, "e2e": None, "gpu_launches": launches * args.steps, "roofline": None,
+                "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    B.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -243,6 +298,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
+    if args.workload == "uneven":
+        return run_uneven(args, torch, dev, rank, world, pg)
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
     eng = Engine(device=local, refine=args.refine)
