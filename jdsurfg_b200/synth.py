@@ -103,6 +103,8 @@ def make_config(name, seed=2024, nx=None, ny=None):
     large : 256x256, nz=64 (1 km to 20 km, then 2.5 km), vs 2.5->4.7 +-8 %,
             LVZ in 20 % of columns, 60 log-spaced periods 1-80 s, Rayleigh and
             Love mode 0 phase
+    mixed : the large grid with Rc, Rg, Lc and Lg mode 0 (phase and group),
+            the mixed-precision accuracy case
     """
     if name == "tiny":
         depth = np.arange(12, dtype=np.float32) * 2.0
@@ -115,6 +117,10 @@ def make_config(name, seed=2024, nx=None, ny=None):
         depth = depth_grid(21, 1.0, 48, 2.5)
         return make_case(nx or 128, ny or 128, depth, 2.5, 4.7, 0.08, np.geomspace(1.0, 60.0, 40), WAVES, 2, seed,
                          lvz_frac=0.2, water_frac=0.1)
+    if name == "mixed":  # the large grid with phase and group of Rayleigh and Love mode 0
+        depth = depth_grid(21, 1.0, 64, 2.5)
+        return make_case(nx or 256, ny or 256, depth, 2.5, 4.7, 0.08, np.geomspace(1.0, 80.0, 60), WAVES, 1,
+                         seed, lvz_frac=0.2)
     if name == "large":
         depth = depth_grid(21, 1.0, 64, 2.5)
         return make_case(nx or 256, ny or 256, depth, 2.5, 4.7, 0.08, np.geomspace(1.0, 80.0, 60), ("Rc", "Lc"), 1,

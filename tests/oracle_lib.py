@@ -203,3 +203,39 @@ def frechet_rows(nx, ny, nz, kernel, row_slot, fdm):
     for r in range(nrows):
         rows.append((idx[r * n:r * n + nnz[r]].copy(), val[r * n:r * n + nnz[r]].copy()))
     return rows
+
+
+def group_u_spread(case, col, group_wave, periods, k, rel=1e-15, steps=(-3, -1, 1, 3)):
+    """Conditioning of the reference's kernel-path group velocity: the range
+    of sregnpu_/slegnpu_'s U (flat) at period periods[k] when the phase
+    velocity input moves by a few `rel` relative steps.  group_wave: "Rg" or
+    "Lg".  Returns (U at the root, max |U(c(1+s*rel)) - U(c)|)."""
+    from jdsurfg_b200 import synth
+    vs = case["vs"][:, col]
+    if case["vp"] is None:
+        vp, rho = synth.brocher(vs)
+    else:
+        vp, rho = case["vp"][:, col], case["rho"][:, col]
+    th, a, b, r = grid2layer(case["depth"], vp, vs, rho)
+    iw = 2 if group_wave == "Rg" else 1
+    T = np.asarray(periods, np.float64)
+    c0 = surfdisp96(th, a, b, r, 1, iw, 1, 0, T, refine=1)[0][k]
+    c1 = surfdisp96(th, a, b, r, 1, iw, 1, 0, T * 1.005, refine=1)[0][k]
+    c2 = surfdisp96(th, a, b, r, 1, iw, 1, 0, T * 0.995, refine=1)[0][k]
+    n = len(th)
+    th, a, b, r = f32(th), f32(a), f32(b), f32(r)
+    out = []
+    for s in (0,) + tuple(steps):
+        bufs = [np.zeros(n) for _ in range(12)]
+        tt, cp, cg = C.c_double(T[k]), C.c_double(c0 * (1 + s * rel)), C.c_double(0)
+        t1, cc1, t2, cc2 = C.c_double(T[k] * 1.005), C.c_double(c1), C.c_double(T[k] * 0.995), C.c_double(c2)
+        if iw == 2:
+            lib().sregnpu_(_ptr(th), _ptr(a), _ptr(b), _ptr(r), n, C.byref(tt), C.byref(cp), C.byref(cg),
+                           *[_ptr(x) for x in bufs[:4]], C.byref(t1), C.byref(cc1), C.byref(t2), C.byref(cc2),
+                           *[_ptr(x) for x in bufs[4:]], 1)
+        else:
+            lib().slegnpu_(_ptr(th), _ptr(b), _ptr(r), n, C.byref(tt), C.byref(cp), C.byref(cg),
+                           *[_ptr(x) for x in bufs[:2]], C.byref(t1), C.byref(cc1), C.byref(t2), C.byref(cc2),
+                           *[_ptr(x) for x in bufs[2:8]], 1)
+        out.append(cg.value)
+    return out[0], max(abs(u - out[0]) for u in out[1:])
