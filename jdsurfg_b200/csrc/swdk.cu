@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const
 // current chain is finished, so lanes stay busy while long chains run.
 // queue[0] is the next item; the launch covers the GPU once.
 #ifndef SWDK_ROOTS_MINB
-#define SWDK_ROOTS_MINB 3  // 168 registers: 3 blocks of 128 per SM
+#define SWDK_ROOTS_MINB 5  // 96 registers with the chain state in shared memory: 5 blocks of 128 per SM
 #endif
 #ifndef SWDK_EIGEN_MINB
 #define SWDK_EIGEN_MINB 4  // 128 registers: 16 warps/SM measured faster than 2 blocks at 230
@@ -475,7 +475,10 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      unsigned long long* __restrict__ nevals) {
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
-  ChainState s;
+  // the chain's state machine lives in shared memory, so the registers go to
+  // the secular function: 96 registers, 5 blocks of 128 per SM
+  __shared__ ChainState sst[128];
+  ChainState& s = sst[threadIdx.x];
   ChainParams P;
   ChainIO io;
   LayerView V;
@@ -588,6 +591,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                const unsigned int* __restrict__ retry_count,
                                                                unsigned int retry_cap, unsigned int* __restrict__ queue,
                                                                unsigned long long* __restrict__ nevals) {
+  __shared__ ChainState sst[128];  // chain state in shared memory, as in k_roots_queue
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
   const unsigned int n = min(*retry_count, retry_cap);
@@ -600,7 +604,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     if (base >= n) break;
     const unsigned int r = base + lane;
     const bool active = r < n;
-    ChainState s;
+    ChainState& s = sst[threadIdx.x];
     ChainParams P;
     ChainIO io;
     LayerView V;
@@ -703,12 +707,18 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
   return group ? c * tm : c / tm;
 }
 
+// specialised per wave type WT (0 Rc, 1 Rg, 2 Lc, 3 Lg) and PATH (0
+// get_1d_kernel, 1 get_2d_map): one launch per slot group, so each kernel
+// carries only the passes it runs (the all-in-one kernel missed in the
+// instruction cache)
+template <int WT, int PATH>
 __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                                const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
-                                               const SlotDesc* __restrict__ slots, const SlotGroups groups,
+                                               const SlotDesc* __restrict__ slots, int g0, int gn,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
-                                               int sphere, int path, double* __restrict__ vc, double* __restrict__ vout,
+                                               int sphere, double* __restrict__ vc, double* __restrict__ vout,
                                                double* __restrict__ kernel, int32_t* __restrict__ status) {
+  constexpr int path = PATH;
   extern __shared__ double sm[];
   const int col = blockIdx.x;
   const ColInfo ci = info[col];
@@ -770,11 +780,10 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
   sink.L = L;
   sink.nw = ci.nw;
   const NodeSink nosink = {nullptr, crs, L, ci.nw};
-  const int g0 = groups.start[blockIdx.y], gn = groups.count[blockIdx.y];
   for (int s = threadIdx.x; s < gn; s += blockDim.x) {
     const SlotDesc sd = slots[g0 + s];
-    const bool love = sd.wtype >= 2;
-    const bool group = (sd.wtype == 1 || sd.wtype == 3);
+    constexpr bool love = WT >= 2;
+    constexpr bool group = (WT == 1 || WT == 3);
     const double c0 = croot[(size_t)sd.r0 * ncol + col];
     int st = cstat[(size_t)sd.r0 * ncol + col];
     double c1 = 0.0, c2 = 0.0;
@@ -798,7 +807,7 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
       continue;
     }
     const EigModel& M = love ? ML : MR;
-    if (path == 1) {  // get_2d_map: disp1D (SurfaceWave.cpp:177-255)
+    if constexpr (PATH == 1) {  // get_2d_map: disp1D (SurfaceWave.cpp:177-255)
       if (!group) {
         const double v = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
         vc[oo] = v;
@@ -816,8 +825,7 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
         }
         vout[oo] = ugr * tm;
       }
-      continue;
-    }
+    } else {
     // ---- get_1d_kernel: kernel1D (SurfaceWave.cpp:266-412) ----
     for (int i = 0; i < nz; ++i) kacc[i] = 0.0;
     if (!group) {
@@ -885,6 +893,7 @@ __global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz
       const double v = (i < ci.nw) ? 0.0 : kacc[i];
       kernel[((size_t)sd.oslot * nz + i) * ncol + col] = v;
     }
+    }  // get_1d_kernel
   }
 }
 
@@ -1294,15 +1303,21 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
     const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
-    int gmax = 0;
-    for (int g = 0; g < P.groups.n; ++g) gmax = std::max(gmax, P.groups.count[g]);
-    const int et = std::min(128, ((gmax + 31) / 32) * 32);
-    ctx->launches += 1;
-    k_eigen<<<dim3(ncol, P.groups.n), et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                    ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), P.groups,
-                                    ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, path, d_vc,
-                                    d_vout, d_kernel, d_status);
-    CK(cudaGetLastError());
+    using EigFn = void (*)(int, int, int, const float4*, const ColInfo*, const float2*, const SlotDesc*, int, int,
+                           const double*, const int32_t*, int, double*, double*, double*, int32_t*);
+    static const EigFn eig[4][2] = {{k_eigen<0, 0>, k_eigen<0, 1>}, {k_eigen<1, 0>, k_eigen<1, 1>},
+                                    {k_eigen<2, 0>, k_eigen<2, 1>}, {k_eigen<3, 0>, k_eigen<3, 1>}};
+    for (int g = 0; g < P.groups.n; ++g) {
+      const int g0 = P.groups.start[g], gn = P.groups.count[g];
+      const int wt = P.slots[g0].wtype;
+      const int et = std::min(128, ((gn + 31) / 32) * 32);
+      ctx->launches += 1;
+      eig[wt][path]<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                            ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), g0, gn,
+                                            ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, d_vc,
+                                            d_vout, d_kernel, d_status);
+      CK(cudaGetLastError());
+    }
   }
   if (timing) {
     CK(cudaEventRecord(ctx->ev[3], st));
