@@ -530,7 +530,7 @@ enum Phase : int {
   PH_CHAIN_START, PH_PERIOD_START, PH_GS_START, PH_GS_FIRST, PH_SCAN, PH_SCAN_GOT, PH_REFINE_START,
   PH_NEV_A, PH_NEV_TOP, PH_NEV_BODY_GOT, PH_NEV_BODY, PH_NEV_HALF_GOT, PH_NEV_NEV_GOT, PH_BRENT_STEP,
   PH_BRENT_GOT, PH_REFINE_DONE, PH_GS_OK, PH_GS_FAIL, PH_PERIOD_OUT, PH_FAIL, PH_MODE_END, PH_CHAIN_END,
-  PH_RETRY_NEXT, PH_PROP_LO, PH_PROP_HI, PH_PROP_CHECK, PH_PROP_DOWN, PH_PROP_DOWN_GOT, PH_DONE
+  PH_RETRY_NEXT, PH_PROP_LO, PH_PROP_HI, PH_PROP_CHECK, PH_PROP_DOWN, PH_PROP_DOWN_GOT, PH_PROP_C1_GOT, PH_DONE
 };
 
 struct ChainParams {
@@ -624,13 +624,14 @@ SWDK_HD void chain_init_retry(ChainState& s, int m, int k) {
 }
 
 // Learned proposals live on the reference's scan grid g_j = c1 + j*dc
-// (surfdisp96.f:452-470).  For period k > 1 of a mode, once the scan start
-// c1 has been evaluated and the scan goes upward, the network's anchored
-// estimate
+// (surfdisp96.f:452-470).  For period k > 1 of a mode, taking the scan to go
+// upward from c1 (f(c1) with the mode's polarity del1st; f(c1) itself is
+// evaluated only when the walk reaches c1 or the proposal is dropped), the
+// network's anchored estimate
 //   c* = c(k-1) + (mu(k) - mu(k-1))
 // (a bias of the network that is smooth in period cancels) names the grid
 // cell [g_m, g_m+1] expected to hold the root.  f is evaluated at both cell
-// ends: a sign change from the sign of f(c1) to the opposite one is the
+// ends: a sign change from the polarity del1st to the opposite one is the
 // cell the scan would have reached; otherwise the scan walks from that cell
 // up or down, one grid step at a time, to the sign change.  The cell and
 // hence the refinement are the plain scan's own.  The stretch [c1, g_m]
@@ -639,7 +640,7 @@ SWDK_HD void chain_init_retry(ChainState& s, int m, int k) {
 constexpr double PROP_GAP_PER_S = 0.01;
 
 SWDK_HD bool proposal_cell(const ChainState& s, const ChainParams& P, const ChainIO& io, int& m) {
-  if (!io.prop || s.sub || P.igr > 0 || P.refine != 1 || s.k < 2 || s.gpass != 0 || s.idir <= 0) return false;
+  if (!io.prop || s.sub || P.igr > 0 || P.refine != 1 || s.k < 2 || s.gpass != 0 || s.del1st == 0.0) return false;
   const size_t base = (size_t)(s.iq - 1) * io.stride;
   const float2 pr = io.prop[base + (size_t)(s.k - 1) * io.ostride];
   const float2 pp = io.prop[base + (size_t)(s.k - 2) * io.ostride];
@@ -708,6 +709,21 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
         }
         s.gpass = 0;
         s.phase = PH_GS_START;
+        int m;
+        if (proposal_cell(s, P, io, m)) {
+          // learned cell: f(c1) is evaluated only if the walk or a fallback
+          // needs it; until then the scan is taken to go up, i.e. f(c1) to
+          // have the mode's polarity del1st (surfdisp96.f:446-451)
+          s.omega = TWOPI / s.t1;
+          s.c1s = s.c1;
+          s.del1s = s.del1st;
+          s.idir = 1;
+          s.nscan = 0;
+          s.pm = m;
+          s.plo = scan_grid(s.c1, m);
+          s.phi = s.plo + DC;
+          s.phase = PH_PROP_LO;
+        }
         break;
       }
       case PH_PROP_LO: {
@@ -719,7 +735,7 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
       }
       case PH_PROP_CHECK: {
         const double fphi = s.last;
-        const bool lo_same = dsign1(s.fplo) == dsign1(s.del1), hi_same = dsign1(fphi) == dsign1(s.del1);
+        const bool lo_same = dsign1(s.fplo) == dsign1(s.del1s), hi_same = dsign1(fphi) == dsign1(s.del1s);
         if (lo_same && !hi_same) {  // the cell of the sign change
           s.nprop_ok++;
           s.c1 = s.plo; s.del1 = s.fplo; s.c2 = s.phi; s.del2 = fphi;
@@ -733,20 +749,30 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
           s.c2 = s.plo; s.del2 = s.fplo;
           s.pm = s.pm - 1;
           s.phase = PH_PROP_DOWN;
-        } else {  // two sign changes inside one cell: plain scan from c1
+        } else {  // two sign changes inside one cell: the plain search from c1
           s.nprop_fail++;
-          s.phase = PH_SCAN;
+          s.c1 = s.c1s;
+          s.phase = PH_GS_START;
         }
         break;
       }
       case PH_PROP_DOWN: {  // c2 = g_pm+1 has the opposite sign; try g_pm
-        if (s.pm <= 0) {  // cell [c1, g_1]; f(c1) is known
-          s.c1 = s.c1s; s.del1 = s.del1s;
-          s.phase = PH_REFINE_START;
-          break;
+        if (s.pm <= 0) {  // cell [c1, g_1]: f(c1) itself is needed now
+          SWDK_REQ(s.c1s, PH_PROP_C1_GOT);
         }
         s.plo = scan_grid(s.c1s, s.pm);
         SWDK_REQ(s.plo, PH_PROP_DOWN_GOT);
+      }
+      case PH_PROP_C1_GOT: {
+        if (dsign1(s.last) == dsign1(s.del1s)) {  // as assumed: the cell [c1, g_1]
+          s.c1 = s.c1s; s.del1 = s.last;
+          s.phase = PH_REFINE_START;
+        } else {  // f(c1) has the other polarity: the reference scans down from c1
+          s.nprop_fail++;
+          s.c1 = s.c1s;
+          s.phase = PH_GS_START;
+        }
+        break;
       }
       case PH_PROP_DOWN_GOT: {
         if (dsign1(s.last) == dsign1(s.del1s)) {  // sign change in [g_pm, g_pm+1]
@@ -772,15 +798,6 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
         else if (plmn >= 0.0) s.idir = 1;
         else s.idir = -1;
         s.phase = PH_SCAN;
-        int m;
-        if (proposal_cell(s, P, io, m)) {
-          s.c1s = s.c1;
-          s.del1s = s.del1;
-          s.pm = m;
-          s.plo = scan_grid(s.c1, m);
-          s.phi = s.plo + DC;
-          s.phase = PH_PROP_LO;
-        }
         break;
       }
       case PH_SCAN: {  // label 1000
