@@ -288,6 +288,16 @@ void swdk_batch_graph_destroy(swdk_graph* graph);
 int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
                   int* blocks);
 
+/* LSMR's matrix products on the device with the CSR rows of
+ * swdk_frechet_csr_device (replaces myaprod_csr, src/shared/parallel.cpp:
+ * 31-115, used by LSMR in src/shared/lsmrModule_csr.f90): mode 1 y += A x,
+ * mode 2 x += A^T y; A is m x n with int64 row pointers, int32 column
+ * indices and FP32 values, x and y are FP64 device vectors.  Asynchronous
+ * on `stream` (NULL: the legacy default stream).  Mode 2 accumulates with
+ * atomics, so its summation order (last bits) varies between calls. */
+int swdk_aprod_csr(int mode, int64_t m, int64_t n, const int64_t* d_rowptr, const int32_t* d_indices,
+                   const float* d_values, double* d_x, double* d_y, void* stream);
+
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 

@@ -947,6 +947,32 @@ __global__ void k_frechet(int nx, int ny, int nz, int kmax, const double* __rest
   if (threadIdx.x == 0 && nnz) nnz[r] = base;
 }
 
+// LSMR's products with the assembled sensitivity matrix (the reference's
+// myaprod_csr, src/shared/parallel.cpp:31-115): FP32 values, FP64 vectors.
+// mode 1: y += A x, one warp per row, lanes stride over the row's entries;
+// mode 2: x += A^T y, one warp per row scattering with FP64 atomics (the
+// reference uses an OpenMP atomic; the summation order is not fixed).
+__global__ void k_aprod1(int64_t m, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ idx,
+                         const float* __restrict__ val, const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= m) return;
+  double acc = 0.0;
+  for (int64_t j = rowptr[r] + lane; j < rowptr[r + 1]; j += 32) acc += (double)val[j] * x[idx[j]];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) y[r] += acc;
+}
+
+__global__ void k_aprod2(int64_t m, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ idx,
+                         const float* __restrict__ val, double* __restrict__ x, const double* __restrict__ y) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= m) return;
+  const double yr = y[r];
+  if (yr == 0.0) return;
+  for (int64_t j = rowptr[r] + lane; j < rowptr[r + 1]; j += 32) atomicAdd(&x[idx[j]], (double)val[j] * yr);
+}
+
 // exclusive prefix sum of nnz[0..n) into rowptr[0..n] (one block)
 __global__ void k_rowptr(int n, const int32_t* __restrict__ nnz, int64_t* __restrict__ rowptr) {
   __shared__ long long part[1024];
@@ -1879,6 +1905,18 @@ int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream) {
   if (n < 0 || (n > 0 && (!d_x || !d_r))) return SWDK_E_ARG;
   if (n == 0) return SWDK_OK;
   k_recip<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, d_x, d_r);
+  return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
+}
+
+int swdk_aprod_csr(int mode, int64_t m, int64_t n, const int64_t* d_rowptr, const int32_t* d_indices,
+                   const float* d_values, double* d_x, double* d_y, void* stream) {
+  if ((mode != 1 && mode != 2) || m < 0 || n < 0 || (m > 0 && (!d_rowptr || !d_x || !d_y))) return SWDK_E_ARG;
+  if (m == 0) return SWDK_OK;
+  const int64_t blocks = (m + 7) / 8;  // 8 rows (warps) per block of 256
+  if (blocks > 0x7fffffff) return SWDK_E_LIMIT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (mode == 1) k_aprod1<<<(unsigned)blocks, 256, 0, st>>>(m, d_rowptr, d_indices, d_values, d_x, d_y);
+  else k_aprod2<<<(unsigned)blocks, 256, 0, st>>>(m, d_rowptr, d_indices, d_values, d_x, d_y);
   return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
 }
 

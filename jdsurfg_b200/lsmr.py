@@ -1,0 +1,170 @@
+"""LSMR on the GPU over the assembled sensitivity rows.
+
+The reference solves the damped least-squares system of every inversion
+iteration with LSMR (csr_matrix::lsmr_solver, src/shared/csr_matrix.cpp,
+running src/shared/lsmrModule_csr.f90 in FP32 with OpenMP matrix products).
+Here the matrix stays on the device as the CSR rows swdk_frechet_csr_device
+produced (FP32 values, int32 columns, int64 row pointers); the two products
+per iteration are libswdk's k_aprod1/k_aprod2 (swdk_aprod_csr), the vectors
+are FP64 device tensors, and the scalar recurrences run on the host.
+
+The iteration follows Fong & Saunders, "LSMR: An iterative algorithm for
+sparse least-squares problems", SIAM J. Sci. Comput. 33 (2011): Golub-Kahan
+bidiagonalization, a first QR factorization of the lower bidiagonal matrix
+(with the damping rotation), a second QR factorization giving the
+minimization of ||A^T r||, and the paper's estimates of ||r||, ||A^T r||,
+||A|| and cond(A) for the stopping rules.  istop has the meaning of the
+reference's module:
+  1 ||r|| small enough (b-compatible system), 2 ||A^T r|| small (least
+  squares), 3 cond(A) above conlim, 4-6 the same three at machine
+  precision, 7 iteration limit.
+Local reorthogonalization (the reference's localSize) is not implemented.
+"""
+import ctypes as C
+import math
+
+from .engine import SwdkError, lib
+
+
+class DeviceCSR:
+    """m x n matrix as device CSR (torch tensors): rowptr int64 (m+1),
+    indices int32, values float32."""
+
+    def __init__(self, rowptr, indices, values, m, n):
+        self.rowptr, self.indices, self.values, self.m, self.n = rowptr, indices, values, m, n
+        L = lib()
+        L.swdk_aprod_csr.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]
+
+    def aprod(self, mode, x, y):
+        """mode 1: y += A x; mode 2: x += A^T y (x, y FP64 device tensors)."""
+        import torch
+        st = torch.cuda.current_stream(x.device).cuda_stream
+        rc = lib().swdk_aprod_csr(mode, self.m, self.n, self.rowptr.data_ptr(), self.indices.data_ptr(),
+                                  self.values.data_ptr(), x.data_ptr(), y.data_ptr(), st)
+        if rc != 0:
+            raise SwdkError(f"swdk_aprod_csr failed ({rc})")
+
+
+def lsmr(A, b, damp=0.0, atol=1e-6, btol=1e-6, conlim=1e8, itnlim=None):
+    """Solve min ||A x - b||^2 + damp^2 ||x||^2.  A: DeviceCSR; b: FP64 device
+    tensor (m).  Returns x (device) and dict(istop, itn, normA, condA, normr,
+    normAr, normx)."""
+    import torch
+    m, n = A.m, A.n
+    dev = b.device
+    itnlim = min(m, n) if itnlim is None else itnlim
+    ctol = 1.0 / conlim if conlim > 0 else 0.0
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    # Golub-Kahan start: beta_1 u_1 = b, alpha_1 v_1 = A^T u_1
+    u = b.clone()
+    beta = float(torch.linalg.vector_norm(u))
+    v = torch.zeros(n, dtype=torch.float64, device=dev)
+    alpha = 0.0
+    if beta > 0.0:
+        u /= beta
+        A.aprod(2, v, u)
+        alpha = float(torch.linalg.vector_norm(v))
+    if alpha > 0.0:
+        v /= alpha
+    normb = beta
+    info = dict(istop=0, itn=0, normA=0.0, condA=1.0, normr=beta, normAr=alpha * beta, normx=0.0)
+    if alpha * beta == 0.0:
+        return x, info
+
+    # state of the two QR factorizations
+    alpha_bar, zeta_bar = alpha, alpha * beta      # first column of the damped bidiagonal, rhs of the 2nd QR
+    rho_prev, rho_bar_prev, c_bar, s_bar = 1.0, 1.0, 1.0, 0.0
+    h = v.clone()
+    h_bar = torch.zeros(n, dtype=torch.float64, device=dev)
+    # residual-norm recurrences (Fong & Saunders, section 3.4)
+    beta_dd, beta_dot = beta, 0.0
+    rho_dot_prev, tau_tilde_prev, theta_tilde, zeta_prev = 1.0, 0.0, 0.0, 0.0
+    damp_sum = 0.0
+    normA2 = alpha * alpha
+    rho_bar_max, rho_bar_min = 0.0, 1e300
+    istop, itn = 0, 0
+    normr = beta
+    while itn < itnlim:
+        itn += 1
+        # bidiagonalization: beta u <- A v - alpha u ; alpha v <- A^T u - beta v
+        u *= -alpha
+        A.aprod(1, v, u)
+        beta = float(torch.linalg.vector_norm(u))
+        if beta > 0.0:
+            u /= beta
+            v *= -beta
+            A.aprod(2, v, u)
+            alpha = float(torch.linalg.vector_norm(v))
+            if alpha > 0.0:
+                v /= alpha
+        # damping rotation on (alpha_bar, damp)
+        alpha_hat = math.hypot(alpha_bar, damp)
+        c_hat, s_hat = alpha_bar / alpha_hat, damp / alpha_hat
+        # first QR rotation: (alpha_hat, beta)
+        rho = math.hypot(alpha_hat, beta)
+        c, s = alpha_hat / rho, beta / rho
+        theta_next = s * alpha
+        alpha_bar = c * alpha
+        # second QR rotation
+        theta_bar = s_bar * rho
+        rho_bar = math.hypot(c_bar * rho, theta_next)
+        c_bar, s_bar = c_bar * rho / rho_bar, theta_next / rho_bar
+        zeta = c_bar * zeta_bar
+        zeta_bar = -s_bar * zeta_bar
+        # search directions and solution
+        h_bar.mul_(-(theta_bar * rho) / (rho_prev * rho_bar_prev)).add_(h)
+        x.add_(h_bar, alpha=zeta / (rho * rho_bar))
+        h.mul_(-(theta_next / rho)).add_(v)
+        # ||r||: rotations applied to the right-hand side (beta_1, 0, ...)
+        beta_acute = c_hat * beta_dd
+        beta_check = -s_hat * beta_dd
+        beta_hat = c * beta_acute
+        beta_dd = -s * beta_acute
+        rho_tilde = math.hypot(rho_dot_prev, theta_bar)
+        c_t, s_t = rho_dot_prev / rho_tilde, theta_bar / rho_tilde
+        theta_tilde_old = theta_tilde
+        theta_tilde = s_t * rho_bar
+        rho_dot = c_t * rho_bar
+        beta_dot = -s_t * beta_dot + c_t * beta_hat
+        tau_tilde_prev = (zeta_prev - theta_tilde_old * tau_tilde_prev) / rho_tilde
+        tau_dot = (zeta - theta_tilde * tau_tilde_prev) / rho_dot
+        damp_sum += beta_check * beta_check
+        normr = math.sqrt(damp_sum + (beta_dot - tau_dot) ** 2 + beta_dd ** 2)
+        # ||A|| and cond(A) estimates
+        normA2 += beta * beta
+        normA = math.sqrt(normA2)
+        normA2 += alpha * alpha
+        rho_bar_max = max(rho_bar_max, rho_bar_prev)
+        if itn > 1:
+            rho_bar_min = min(rho_bar_min, rho_bar_prev)
+        condA = max(rho_bar_max, rho_bar) / min(rho_bar_min, rho_bar)
+        normAr = abs(zeta_bar)
+        normx = float(torch.linalg.vector_norm(x))
+        # roll the recurrences
+        rho_prev, rho_bar_prev, rho_dot_prev, zeta_prev = rho, rho_bar, rho_dot, zeta
+        # stopping rules
+        test1 = normr / normb
+        test2 = normAr / (normA * normr) if normA * normr > 0.0 else math.inf
+        test3 = 1.0 / condA
+        t1 = test1 / (1.0 + normA * normx / normb)
+        rtol = btol + atol * normA * normx / normb
+        if itn >= itnlim:
+            istop = 7
+        if 1.0 + test3 <= 1.0:
+            istop = 6
+        if 1.0 + test2 <= 1.0:
+            istop = 5
+        if 1.0 + t1 <= 1.0:
+            istop = 4
+        if test3 <= ctol:
+            istop = 3
+        if test2 <= atol:
+            istop = 2
+        if test1 <= rtol:
+            istop = 1
+        info.update(istop=istop, itn=itn, normA=normA, condA=condA, normr=normr, normAr=normAr, normx=normx)
+        if istop > 0:
+            break
+    return x, info

@@ -1,0 +1,63 @@
+"""LSMR on the device (jdsurfg_b200/lsmr.py) with libswdk's CSR products:
+the products against scipy's sparse matrix, and the solver against scipy's
+LSMR run on the same FP32-valued matrix in FP64."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(m, n, density, seed):
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    A = sp.random(m, n, density=density, format="csr", random_state=seed, dtype=np.float64)
+    A.data = (A.data - 0.5).astype(np.float32).astype(np.float64)  # FP32 values, as the Frechet rows
+    A.sort_indices()
+    b = A @ rng.standard_normal(n) + 1e-3 * rng.standard_normal(m)
+    return A, b
+
+
+def _device(A):
+    import torch
+    from jdsurfg_b200.lsmr import DeviceCSR
+    d = torch.device("cuda", 0)
+    return DeviceCSR(torch.from_numpy(A.indptr.astype(np.int64)).to(d),
+                     torch.from_numpy(A.indices.astype(np.int32)).to(d),
+                     torch.from_numpy(A.data.astype(np.float32)).to(d), A.shape[0], A.shape[1])
+
+
+def test_csr_products_match_scipy():
+    import torch
+    A, _ = _problem(3000, 2000, 0.01, 1)
+    D = _device(A)
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(2000)
+    y0 = rng.standard_normal(3000)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.from_numpy(y0.copy()).cuda()
+    D.aprod(1, xd, yd)
+    assert np.allclose(yd.cpu().numpy(), y0 + A @ x, rtol=1e-12, atol=1e-12)
+    x0 = rng.standard_normal(2000)
+    xd = torch.from_numpy(x0.copy()).cuda()
+    D.aprod(2, xd, torch.from_numpy(y0).cuda())
+    assert np.allclose(xd.cpu().numpy(), x0 + A.T @ y0, rtol=1e-11, atol=1e-11)
+
+
+@pytest.mark.parametrize("damp", [0.0, 0.3])
+def test_lsmr_matches_scipy(damp):
+    import torch
+    from scipy.sparse.linalg import lsmr as sp_lsmr
+    from jdsurfg_b200.lsmr import lsmr
+    A, b = _problem(2500, 1200, 0.02, 3)
+    D = _device(A)
+    x, info = lsmr(D, torch.from_numpy(b).cuda(), damp=damp, atol=1e-10, btol=1e-10, itnlim=300)
+    ref = sp_lsmr(A, b, damp=damp, atol=1e-10, btol=1e-10, maxiter=300)
+    xr = ref[0]
+    assert info["istop"] == ref[1]
+    assert abs(info["itn"] - ref[2]) <= 2
+    assert np.linalg.norm(x.cpu().numpy() - xr) <= 1e-6 * np.linalg.norm(xr)
+    assert abs(info["normr"] - ref[3]) <= 1e-6 * max(1.0, ref[3])
+    # the normal equations of the damped problem hold at the solution
+    xs = x.cpu().numpy()
+    g = A.T @ (A @ xs - b) + damp ** 2 * xs
+    assert np.linalg.norm(g) <= 1e-6 * np.linalg.norm(A.T @ b)
