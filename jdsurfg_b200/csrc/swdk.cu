@@ -460,7 +460,10 @@ __global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const
 #define SWDK_ROOTS_MINB 5  // 96 registers with the chain state in shared memory: 5 blocks of 128 per SM
 #endif
 #ifndef SWDK_EIGEN_MINB
-#define SWDK_EIGEN_MINB 4  // 128 registers: 16 warps/SM measured faster than 2 blocks at 230
+#define SWDK_EIGEN_MINB 5  // Rayleigh passes: 96 registers (4: 310 ms, 5: 293 ms, 6: 325 ms on the default workload)
+#endif
+#ifndef SWDK_EIGEN_MINB_LOVE
+#define SWDK_EIGEN_MINB_LOVE 5  // Love passes
 #endif
 __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, int nitems, const int* __restrict__ order,
                                                      const ChainDesc* __restrict__ chains,
@@ -712,7 +715,7 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
 // carries only the passes it runs (the all-in-one kernel missed in the
 // instruction cache)
 template <int WT, int PATH>
-__global__ void __launch_bounds__(128, SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+__global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                                const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
                                                const SlotDesc* __restrict__ slots, int g0, int gn,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
