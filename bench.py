@@ -305,6 +305,7 @@ def main():
     eng = Engine(device=local, refine=args.refine)
     nets = None
     from jdsurfg_b200 import learn
+    eng_nets_on = [args.proposal == "learned"]  # whether the timed engine has the proposal attached
     if args.proposal == "learned":
         nets, _ = learn.load_proposals(eng)
     eng.setup(case)
@@ -344,8 +345,19 @@ def main():
         The per-stage figures come from one eager probe call (CUDA events inside the
         engine); the timed steps replay the captured CUDA graph of that call."""
         step()
-        probe = eng.stats()
+        launches = eng.stats()["kernel_launches"]
+        # stage breakdown from one call of an unsplit engine with the same
+        # settings (the timed call runs as two overlapping column halves,
+        # whose stage times do not add up)
+        probe_eng = Engine(device=local, refine=args.refine, split_cols=-1)
+        if eng_nets_on[0]:
+            learn.load_proposals(probe_eng)
+        probe_eng.setup(case)
+        probe_eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
+        probe = probe_eng.stats()
+        probe_eng.close()
         acc = {k: probe[k] * nsteps for k in STAT_KEYS}
+        acc["kernel_launches"] = launches * nsteps
         use_graph = not args.no_graph
         if use_graph:
             eng.graph_capture("kernel", nx, ny, nz, vs, vp, rho, vc, vout, ker, st)
@@ -387,6 +399,7 @@ def main():
     alg_lr, alg_ll = lr, ll  # algorithmic layer-evaluations: the plain method's count
     if args.proposal == "learned" and not args.no_plain:
         eng.set_proposal(None, None)
+        eng_nets_on[0] = False
         for _ in range(1):
             step()
         torch.cuda.synchronize()
@@ -403,6 +416,7 @@ def main():
                  "learned_eval_reduction": pacc["secular_evals"] / max(1, evals),
                  "max_abs_dc_learned_vs_plain_km_s": dmax}
         nets, _ = learn.load_proposals(eng)  # the e2e leg runs the learned path again
+        eng_nets_on[0] = True
 
     # e2e: host-memory C-ABI call, pinned buffers, copies in the timed region
     e2e = None

@@ -74,7 +74,10 @@ typedef struct swdk_config {
   double rtol;     /* bracket width for SWDK_REFINE_TIGHT (default 1e-10)     */
   int sngl;        /* 1: roots rounded to REAL*4 as surfdisp96 does (default) */
   int sphere;      /* 1: spherical earth as SurfTime (default); 0: flat       */
-  int block_roots; /* threads per block of the root kernel, 0 = default       */
+  int block_roots; /* blocks of the persistent root kernel, 0 = occupancy
+                      default (swdk_autotune sets it)                       */
+  int split_cols;  /* calls with at least this many columns run as two
+                      concurrent column halves; 0 = 8192, < 0 = never       */
 } swdk_config;
 
 typedef struct swdk_stats {

@@ -194,7 +194,7 @@ __device__ void write_layers(int L, int ncol, int col, const float* th, const fl
 // ---------------------------------------------------------------------------
 // k_prep: node model -> layer models (one thread per column)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __restrict__ vs_in,
+__global__ void __launch_bounds__(128) k_prep(int ncol, int ldi, int nz, const float* __restrict__ vs_in,
                                               const float* __restrict__ vp_in, const float* __restrict__ rho_in,
                                               const float* __restrict__ depth, int sphere, int Lmax,
                                               float4* __restrict__ layR, float4* __restrict__ layL,
@@ -206,11 +206,11 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int nz, const float* __r
   float v[NZMAX], vp[NZMAX], rho[NZMAX], dep[NZMAX];
   bool valid = true;
   for (int k = 0; k < nz; ++k) {
-    v[k] = vs_in[col + (size_t)ncol * k];
+    v[k] = vs_in[col + (size_t)ldi * k];
     dep[k] = depth[k];
     if (vp_in) {
-      vp[k] = vp_in[col + (size_t)ncol * k];
-      rho[k] = rho_in[col + (size_t)ncol * k];
+      vp[k] = vp_in[col + (size_t)ldi * k];
+      rho[k] = rho_in[col + (size_t)ldi * k];
     } else {
       brocher(v[k], vp[k], rho[k]);
     }
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
                                                const SlotDesc* __restrict__ slots, int g0, int gn,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
                                                int sphere, double* __restrict__ vc, double* __restrict__ vout,
-                                               double* __restrict__ kernel, int32_t* __restrict__ status) {
+                                               double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
   constexpr int path = PATH;
   extern __shared__ double sm[];
   const int col = blockIdx.x;
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
       st = worst_status(st, cstat[(size_t)sd.r1 * ncol + col]);
       st = worst_status(st, cstat[(size_t)sd.r2 * ncol + col]);
     }
-    const size_t oo = (size_t)sd.oslot * ncol + col;
+    const size_t oo = (size_t)sd.oslot * ldo + col;  // outputs: row stride ldo (>= ncol)
     bool dead = !ci.valid || c0 == 0.0 || (three && (c1 == 0.0 || c2 == 0.0));
     if (!ci.valid) st = ST_NAN_INPUT;
     else if (dead) st = ST_NO_ROOT;
@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
       vc[oo] = 0.0;
       vout[oo] = 0.0;
       if (path == 0)
-        for (int i = 0; i < nz; ++i) kernel[((size_t)sd.oslot * nz + i) * ncol + col] = 0.0;
+        for (int i = 0; i < nz; ++i) kernel[((size_t)sd.oslot * nz + i) * ldo + col] = 0.0;
       continue;
     }
     const EigModel& M = love ? ML : MR;
@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
     // water / merged fluid nodes carry no kernel (SurfaceWave.cpp:495)
     for (int i = 0; i < nz; ++i) {
       const double v = (i < ci.nw) ? 0.0 : kacc[i];
-      kernel[((size_t)sd.oslot * nz + i) * ncol + col] = v;
+      kernel[((size_t)sd.oslot * nz + i) * ldo + col] = v;
     }
     }  // get_1d_kernel
   }
@@ -1061,6 +1061,13 @@ struct swdk_ctx {
   int last_ncol = 0, last_path = -1;
   // depth vector on the device (uploaded once per swdk_set_depth)
   const void* depth_dev = nullptr;
+  // large calls run as two column halves on two child contexts (own
+  // buffers and streams), forked from and joined back into the caller's
+  // stream, so each half's stage tails overlap the other half's work and,
+  // for host calls, the copies of one half overlap the other's compute
+  swdk_ctx* kids[2] = {nullptr, nullptr};
+  cudaEvent_t evfork = nullptr, evjoin[2] = {nullptr, nullptr};
+  bool last_split = false;
   // CUDA graph of one call (swdk_graph_capture / swdk_graph_launch)
   bool capturing = false;
   cudaGraph_t graph = nullptr;
@@ -1252,9 +1259,12 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
 
 // model preparation + (proposals) + roots + (eigen) for one call on device
 // pointers; path 0 get_1d_kernel, 1 get_2d_map, 2 roots of path 0 only
+// ldi / ldo: row strides (in columns) of the input model and of the outputs,
+// >= nx*ny; -1 = nx*ny (dense).  A column block of a larger model runs with
+// the pointers offset to its first column and the large model's strides.
 int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
                const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
-               cudaStream_t st) {
+               cudaStream_t st, int ldi = -1, int ldo = -1) {
   const bool roots_only = (path == 2);
   if (roots_only) path = 0;
   if (nx <= 0 || ny <= 0 || !d_vs || (!roots_only && (!d_vc || !d_vout || (path == 0 && !d_kernel))))
@@ -1266,6 +1276,9 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   if (r) return r;
   Plan& P = ctx->plan[path];
   const int ncol = nx * ny;
+  if (ldi < 0) ldi = ncol;
+  if (ldo < 0) ldo = ncol;
+  if (ldi < ncol || ldo < ncol) return fail(ctx, SWDK_E_ARG, "row stride below the column count");
   const int Lmax = 4 * nz - 3;
   const bool useprop = proposals_on(ctx);
   const bool wantfeat = useprop || roots_only;
@@ -1289,7 +1302,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   const bool timing = !ctx->capturing;  // stage events and statistics only on eager calls
   if (timing) CK(cudaEventRecord(ctx->ev[0], st));
   ctx->launches = 1;
-  k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
+  k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ldi, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                              ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr);
@@ -1333,7 +1346,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   if (!roots_only) {
     const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
     using EigFn = void (*)(int, int, int, const float4*, const ColInfo*, const float2*, const SlotDesc*, int, int,
-                           const double*, const int32_t*, int, double*, double*, double*, int32_t*);
+                           const double*, const int32_t*, int, double*, double*, double*, int32_t*, int);
     static const EigFn eig[4][2] = {{k_eigen<0, 0>, k_eigen<0, 1>}, {k_eigen<1, 0>, k_eigen<1, 1>},
                                     {k_eigen<2, 0>, k_eigen<2, 1>}, {k_eigen<3, 0>, k_eigen<3, 1>}};
     for (int g = 0; g < P.groups.n; ++g) {
@@ -1344,7 +1357,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       eig[wt][path]<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                             ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), g0, gn,
                                             ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, d_vc,
-                                            d_vout, d_kernel, d_status);
+                                            d_vout, d_kernel, d_status, ldo);
       CK(cudaGetLastError());
     }
   }
@@ -1364,6 +1377,30 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
 
 void collect_stats(swdk_ctx* ctx) {
   if (!ctx->stats_pending) return;
+  if (ctx->last_split) {  // sum of the two halves; stage times are the longer half's
+    ctx->stats_pending = false;
+    swdk_stats t;
+    memset(&t, 0, sizeof(t));
+    for (swdk_ctx* k : ctx->kids) {
+      if (!k) continue;
+      collect_stats(k);
+      const swdk_stats& a = k->stats;
+      t.secular_evals += a.secular_evals;
+      t.layer_evals_rayleigh += a.layer_evals_rayleigh;
+      t.layer_evals_love += a.layer_evals_love;
+      t.proposals_accepted += a.proposals_accepted;
+      t.proposals_rejected += a.proposals_rejected;
+      t.kernel_launches += a.kernel_launches;
+      t.nchains = a.nchains;
+      t.nslots = a.nslots;
+      t.ms_prep = std::max(t.ms_prep, a.ms_prep);
+      t.ms_proposal = std::max(t.ms_proposal, a.ms_proposal);
+      t.ms_roots = std::max(t.ms_roots, a.ms_roots);
+      t.ms_eigen = std::max(t.ms_eigen, a.ms_eigen);
+    }
+    ctx->stats = t;
+    return;
+  }
   cudaEventSynchronize(ctx->ev[4]);
   ctx->stats_pending = false;
   ctx->stats.secular_evals = (int64_t)ctx->h_nevals[0];
@@ -1384,39 +1421,148 @@ void drop_graph(swdk_ctx* ctx) {
   ctx->graph = nullptr;
 }
 
+constexpr int SPLIT_MIN_COLS = 8192;  // calls with fewer columns run as one piece
+
+void drop_kids(swdk_ctx* ctx) {
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->kids[i]) swdk_destroy(ctx->kids[i]);
+    ctx->kids[i] = nullptr;
+    if (ctx->evjoin[i]) cudaEventDestroy(ctx->evjoin[i]);
+    ctx->evjoin[i] = nullptr;
+  }
+  if (ctx->evfork) cudaEventDestroy(ctx->evfork);
+  ctx->evfork = nullptr;
+  ctx->last_split = false;
+}
+
+// child contexts with the parent's configuration, period tables, depth
+// vector and proposal networks
+int ensure_kids(swdk_ctx* ctx) {
+  if (ctx->kids[0] && ctx->kids[1]) return SWDK_OK;
+  drop_kids(ctx);
+  for (int i = 0; i < 2; ++i) {
+    swdk_ctx* k = nullptr;
+    const int r = swdk_create(&k, &ctx->cfg);
+    if (r) { drop_kids(ctx); return fail(ctx, r, "child context creation failed"); }
+    for (int w = 0; w < 4; ++w) { k->tab[w] = ctx->tab[w]; k->ntmax[w] = ctx->ntmax[w]; k->nmode[w] = ctx->nmode[w]; }
+    k->have_periods = ctx->have_periods;
+    k->dirty = true;
+    k->depth = ctx->depth;
+    k->net[0] = ctx->net[0];
+    k->net[1] = ctx->net[1];
+    k->kappa[0] = ctx->kappa[0];
+    k->kappa[1] = ctx->kappa[1];
+    ctx->kids[i] = k;
+    CK(cudaEventCreateWithFlags(&ctx->evjoin[i], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&ctx->evfork, cudaEventDisableTiming));
+  return SWDK_OK;
+}
+
+bool use_split(const swdk_ctx* ctx, int path, int ncol) {
+  const int lim = ctx->cfg.split_cols == 0 ? SPLIT_MIN_COLS : ctx->cfg.split_cols;
+  return path != 2 && lim > 0 && ncol >= lim && ncol >= 2;
+}
+
+// a device call, as two column halves when it is large enough
+int run_split(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
+              const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status, cudaStream_t st) {
+  const int ncol = nx * ny;
+  if (!use_split(ctx, path, ncol) || nx <= 0 || ny <= 0) {
+    ctx->last_split = false;
+    return run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  }
+  int r = ensure_plans(ctx);  // argument checks and the parent's plan (kmax) first
+  if (r) return r;
+  r = ensure_kids(ctx);
+  if (r) return r;
+  CK(cudaEventRecord(ctx->evfork, st));
+  for (int h = 0; h < 2; ++h) {
+    swdk_ctx* k = ctx->kids[h];
+    const int c0 = h ? ncol / 2 : 0, n = h ? ncol - ncol / 2 : ncol / 2;
+    CK(cudaStreamWaitEvent(k->stream, ctx->evfork, 0));
+    k->capturing = ctx->capturing;
+    r = run_device(k, path, n, 1, nz, d_vs + c0, d_vp ? d_vp + c0 : nullptr, d_rho ? d_rho + c0 : nullptr,
+                   d_vc + c0, d_vout + c0, d_kernel ? d_kernel + c0 : nullptr, d_status ? d_status + c0 : nullptr,
+                   k->stream, ncol, ncol);
+    k->capturing = false;
+    if (r) return fail(ctx, r, std::string("column half: ") + k->err);
+    CK(cudaEventRecord(ctx->evjoin[h], k->stream));
+    CK(cudaStreamWaitEvent(st, ctx->evjoin[h], 0));
+  }
+  ctx->last_split = true;
+  ctx->stats_pending = !ctx->capturing;
+  ctx->last_ncol = ncol;
+  ctx->last_path = path;
+  return SWDK_OK;
+}
+
+// host arrays -> device -> host for columns [c0, c0+n) of an ncol-column
+// model, on context k's stream and buffers (strided 2-D copies)
+int host_piece(swdk_ctx* ctx, swdk_ctx* k, int path, int ncol, int c0, int n, int nz, const float* vs,
+               const float* vp, const float* rho, double* vc, double* vout, double* kernel, int32_t* status) {
+  int r = ensure_plans(k);
+  if (r) return fail(ctx, r, k->err);
+  const int kmax = k->plan[path].kmax;
+  cudaStream_t st = k->stream;
+  CK(k->in_vs.ensure((size_t)n * nz * sizeof(float)));
+  if (vp) {
+    CK(k->in_vp.ensure((size_t)n * nz * sizeof(float)));
+    CK(k->in_rho.ensure((size_t)n * nz * sizeof(float)));
+  }
+  CK(k->out_vc.ensure((size_t)n * kmax * sizeof(double)));
+  CK(k->out_vout.ensure((size_t)n * kmax * sizeof(double)));
+  CK(k->out_status.ensure((size_t)n * kmax * sizeof(int32_t)));
+  if (path == 0) CK(k->out_kernel.ensure((size_t)n * nz * kmax * sizeof(double)));
+  const size_t fw = (size_t)n * sizeof(float), dw = (size_t)n * sizeof(double), iw = (size_t)n * sizeof(int32_t);
+  CK(cudaMemcpy2DAsync(k->in_vs.p, fw, vs + c0, ncol * sizeof(float), fw, nz, cudaMemcpyHostToDevice, st));
+  if (vp) {
+    CK(cudaMemcpy2DAsync(k->in_vp.p, fw, vp + c0, ncol * sizeof(float), fw, nz, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpy2DAsync(k->in_rho.p, fw, rho + c0, ncol * sizeof(float), fw, nz, cudaMemcpyHostToDevice, st));
+  }
+  r = run_device(k, path, n, 1, nz, k->in_vs.as<float>(), vp ? k->in_vp.as<float>() : nullptr,
+                 vp ? k->in_rho.as<float>() : nullptr, k->out_vc.as<double>(), k->out_vout.as<double>(),
+                 path == 0 ? k->out_kernel.as<double>() : nullptr, k->out_status.as<int32_t>(), st);
+  if (r) return fail(ctx, r, k->err);
+  CK(cudaMemcpy2DAsync(vc + c0, ncol * sizeof(double), k->out_vc.p, dw, dw, kmax, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpy2DAsync(vout + c0, ncol * sizeof(double), k->out_vout.p, dw, dw, kmax, cudaMemcpyDeviceToHost, st));
+  if (status)
+    CK(cudaMemcpy2DAsync(status + c0, ncol * sizeof(int32_t), k->out_status.p, iw, iw, kmax, cudaMemcpyDeviceToHost,
+                         st));
+  if (path == 0)
+    CK(cudaMemcpy2DAsync(kernel + c0, ncol * sizeof(double), k->out_kernel.p, dw, dw, (size_t)kmax * nz,
+                         cudaMemcpyDeviceToHost, st));
+  return SWDK_OK;
+}
+
 int run_host(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* vs, const float* vp, const float* rho,
              double* vc, double* vout, double* kernel, int32_t* status) {
   if (!ctx || nx <= 0 || ny <= 0 || !vs || !vc || !vout || (path == 0 && !kernel)) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  if ((vp == nullptr) != (rho == nullptr)) return fail(ctx, SWDK_E_ARG, "vp and rho must both be given or both NULL");
   CK(cudaSetDevice(ctx->cfg.device));
   int r = ensure_plans(ctx);
   if (r) return r;
-  const size_t ncol = (size_t)nx * ny;
-  const int kmax = ctx->plan[path].kmax;
-  cudaStream_t st = ctx->stream;
-  CK(ctx->in_vs.ensure(ncol * nz * sizeof(float)));
-  if (vp) {
-    CK(ctx->in_vp.ensure(ncol * nz * sizeof(float)));
-    CK(ctx->in_rho.ensure(ncol * nz * sizeof(float)));
+  const int ncol = nx * ny;
+  if (!use_split(ctx, path, ncol)) {
+    r = host_piece(ctx, ctx, path, ncol, 0, ncol, nz, vs, vp, rho, vc, vout, kernel, status);
+    if (r) return r;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->last_split = false;
+    collect_stats(ctx);
+    return SWDK_OK;
   }
-  CK(ctx->out_vc.ensure(ncol * kmax * sizeof(double)));
-  CK(ctx->out_vout.ensure(ncol * kmax * sizeof(double)));
-  CK(ctx->out_status.ensure(ncol * kmax * sizeof(int32_t)));
-  if (path == 0) CK(ctx->out_kernel.ensure(ncol * nz * kmax * sizeof(double)));
-  CK(cudaMemcpyAsync(ctx->in_vs.p, vs, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
-  if (vp) {
-    CK(cudaMemcpyAsync(ctx->in_vp.p, vp, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->in_rho.p, rho, ncol * nz * sizeof(float), cudaMemcpyHostToDevice, st));
-  }
-  r = run_device(ctx, path, nx, ny, nz, ctx->in_vs.as<float>(), vp ? ctx->in_vp.as<float>() : nullptr,
-                 vp ? ctx->in_rho.as<float>() : nullptr, ctx->out_vc.as<double>(), ctx->out_vout.as<double>(),
-                 path == 0 ? ctx->out_kernel.as<double>() : nullptr, ctx->out_status.as<int32_t>(), st);
+  r = ensure_kids(ctx);
   if (r) return r;
-  CK(cudaMemcpyAsync(vc, ctx->out_vc.p, ncol * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(vout, ctx->out_vout.p, ncol * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
-  if (status) CK(cudaMemcpyAsync(status, ctx->out_status.p, ncol * kmax * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  if (path == 0)
-    CK(cudaMemcpyAsync(kernel, ctx->out_kernel.p, ncol * nz * kmax * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  for (int h = 0; h < 2; ++h) {
+    const int c0 = h ? ncol / 2 : 0, n = h ? ncol - ncol / 2 : ncol / 2;
+    r = host_piece(ctx, ctx->kids[h], path, ncol, c0, n, nz, vs, vp, rho, vc, vout, kernel, status);
+    if (r) return r;
+  }
+  for (int h = 0; h < 2; ++h) CK(cudaStreamSynchronize(ctx->kids[h]->stream));
+  ctx->last_split = true;
+  ctx->stats_pending = true;
+  ctx->last_ncol = ncol;
+  ctx->last_path = path;
   collect_stats(ctx);
   return SWDK_OK;
 }
@@ -1450,6 +1596,7 @@ int swdk_config_default(swdk_config* cfg) {
   cfg->sngl = 1;
   cfg->sphere = 1;
   cfg->block_roots = 0;
+  cfg->split_cols = 0;
   return SWDK_OK;
 }
 
@@ -1493,6 +1640,7 @@ void swdk_destroy(swdk_ctx* ctx) {
     ctx->plan[p].d_rootfeat.release();
   }
   drop_graph(ctx);
+  drop_kids(ctx);
   for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
@@ -1517,6 +1665,7 @@ int swdk_set_periods(swdk_ctx* ctx, const double* tRc, int ntRc, int nmRc, const
   ctx->have_periods = true;
   ctx->dirty = true;
   drop_graph(ctx);
+  drop_kids(ctx);
   cudaSetDevice(ctx->cfg.device);
   return ensure_plans(ctx);
 }
@@ -1527,6 +1676,7 @@ int swdk_set_depth(swdk_ctx* ctx, const float* depth, int nz) {
   ctx->depth.assign(depth, depth + nz);
   ctx->depth_dev = nullptr;
   drop_graph(ctx);
+  drop_kids(ctx);
   return SWDK_OK;
 }
 
@@ -1554,7 +1704,7 @@ int swdk_get_1d_kernel_device(swdk_ctx* ctx, int nx, int ny, int nz, const float
   if (!ctx) return SWDK_E_ARG;
   CK(cudaSetDevice(ctx->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  return run_device(ctx, 0, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  return run_split(ctx, 0, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
 }
 
 int swdk_get_2d_map_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
@@ -1562,7 +1712,7 @@ int swdk_get_2d_map_device(swdk_ctx* ctx, int nx, int ny, int nz, const float* d
   if (!ctx) return SWDK_E_ARG;
   CK(cudaSetDevice(ctx->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  return run_device(ctx, 1, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, nullptr, d_status, st);
+  return run_split(ctx, 1, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, nullptr, d_status, st);
 }
 
 int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* thk, const float* vp, const float* vs,
@@ -1679,6 +1829,7 @@ int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double 
   if (!ctx || !(kappa_rayleigh > 0.0) || !(kappa_rayleigh < 1.0e3) || !(kappa_love > 0.0) || !(kappa_love < 1.0e3))
     return fail(ctx, SWDK_E_ARG, "bad arguments");
   drop_graph(ctx);
+  drop_kids(ctx);
   ctx->net[0] = rayleigh;
   ctx->net[1] = love;
   ctx->kappa[0] = kappa_rayleigh;
@@ -1710,6 +1861,7 @@ int swdk_root_slots(swdk_ctx* ctx, int* nslots, int32_t* wave, int32_t* mode, do
 
 int swdk_last_roots(swdk_ctx* ctx, double* h_c, int32_t* h_status) {
   if (!ctx || ctx->last_ncol <= 0 || ctx->last_path < 0) return fail(ctx, SWDK_E_ARG, "no root search ran yet");
+  if (ctx->last_split) return fail(ctx, SWDK_E_ARG, "the last call ran as column halves: use swdk_roots_device");
   CK(cudaSetDevice(ctx->cfg.device));
   const Plan& P = ctx->plan[ctx->last_path == 1 ? 1 : 0];
   const size_t n = (size_t)P.nroot * ctx->last_ncol;
@@ -1747,13 +1899,13 @@ int swdk_graph_capture(swdk_ctx* ctx, int path, int nx, int ny, int nz, const fl
   // one eager call sizes every buffer, builds the plans, uploads the depth
   // vector and prepares the proposal networks, so the captured call
   // allocates nothing and copies nothing from pageable memory
-  int r = run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  int r = run_split(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
   if (r) return r;
   CK(cudaStreamSynchronize(st));
   collect_stats(ctx);
   CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   ctx->capturing = true;
-  r = run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
+  r = run_split(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
   ctx->capturing = false;
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(st, &g);
@@ -1900,6 +2052,7 @@ int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, cons
     if (ms < best_ms) { best_ms = ms; best = b; }
   }
   ctx->cfg.block_roots = best;
+  drop_kids(ctx);  // the column halves are recreated with the tuned grid
   if (blocks_out) *blocks_out = best;
   return SWDK_OK;
 }

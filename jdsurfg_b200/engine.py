@@ -27,7 +27,7 @@ REFINE = {"reference": 0, "tight": 1}
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("refine", C.c_int), ("rtol", C.c_double), ("sngl", C.c_int),
-                ("sphere", C.c_int), ("block_roots", C.c_int)]
+                ("sphere", C.c_int), ("block_roots", C.c_int), ("split_cols", C.c_int)]
 
 
 class Call(C.Structure):
@@ -110,7 +110,7 @@ class SwdkError(RuntimeError):
 class Engine:
     """One GPU context (device buffers, plans, stream) of libswdk."""
 
-    def __init__(self, device=0, refine="tight", rtol=1e-10, sngl=True, sphere=True, block_roots=0):
+    def __init__(self, device=0, refine="tight", rtol=1e-10, sngl=True, sphere=True, block_roots=0, split_cols=0):
         L = lib()
         cfg = Config()
         L.swdk_config_default(C.byref(cfg))
@@ -120,6 +120,7 @@ class Engine:
         cfg.sngl = 1 if sngl else 0
         cfg.sphere = 1 if sphere else 0
         cfg.block_roots = block_roots
+        cfg.split_cols = split_cols
         h = C.c_void_p()
         rc = L.swdk_create(C.byref(h), C.byref(cfg))
         if rc != 0:

@@ -81,3 +81,31 @@ def test_autotune_keeps_results():
     for x, y in zip(ref[:3], got[:3]):
         assert np.array_equal(x, y)
     eng.close()
+
+
+@pytest.mark.parametrize("path", ["kernel", "map"])
+def test_column_halves_equal_one_piece(path):
+    """Large calls run as two concurrent column halves on child contexts; the
+    results must be the bits of the one-piece call, for device and host calls."""
+    import torch
+    dev = torch.device("cuda", 0)
+    a = synth.subset_columns(synth.make_config("production", seed=2024), np.arange(9000))
+    outs = []
+    for split in (-1, 0):
+        eng = Engine(device=0, split_cols=split)
+        keep = learn.load_proposals(eng)
+        eng.setup(a)
+        dvc = _eager(eng, a, torch, dev, path)
+        host = eng.get_1d_kernel(a["vs"], a["vp"], a["rho"], nx=a["nx"]) if path == "kernel" else \
+            eng.get_2d_map(a["vs"], a["vp"], a["rho"], nx=a["nx"])
+        st = eng.stats()
+        outs.append((dvc, host, st))
+        eng.close()
+    (d1, h1, s1), (d2, h2, s2) = outs
+    for x, y in zip(d1, d2):
+        if x is not None:
+            assert np.array_equal(x, y)
+    for k in h1:
+        assert np.array_equal(h1[k], h2[k]), k
+    assert np.array_equal(d1[0], h2["vc"])
+    assert s1["secular_evals"] == s2["secular_evals"] and s1["proposals_accepted"] == s2["proposals_accepted"]
