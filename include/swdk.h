@@ -37,6 +37,7 @@
 #ifndef SWDK_H_
 #define SWDK_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -306,6 +307,82 @@ int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 
 /* Human-readable text of the last error on this context. */
 const char* swdk_last_error(const swdk_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Fast-marching traveltimes and ray-path Frechet weights (FMST)
+ *
+ * Replaces the per-pair calls fmst_init / fmst_run / fmst_reset /
+ * fmst_raypath / fmst_finalize (src/SWD/SurfaceWave.hpp:8-50, implemented in
+ * src/SWD/fmst.f90 and src/SWD/fmm.f90) that SurfTime::travel_time
+ * (src/SWD/SurfaceWave.cpp:510-541) and SurfTime::frechet_matrix
+ * (:583-672) make for every station pair, with one batched call over all
+ * pairs of an inversion iteration.  Same algorithm and REAL*4 arithmetic:
+ * propagation grid diced 8x from the (nx, ny) model grid, a refined grid
+ * (8x finer, 8 nodes around the source) marched first, the mixed-order
+ * narrow-band fast marching with the reference's binary heap, bilinear
+ * receiver times, and rays traced back down the traveltime gradient with
+ * cubic B-spline Frechet weights and the group-velocity traveltime.
+ * ------------------------------------------------------------------------ */
+typedef struct swdk_fmst swdk_fmst;
+
+/* fmst_init's arguments (fmst.f90:9): model grid nx (latitude) x ny
+ * (longitude) nodes, upper-left corner latitude goxd and longitude gozd and
+ * spacings dvxd, dvzd, all in degrees (SurfTime's lat0, lon0, dlat, dlon). */
+typedef struct swdk_fmst_grid {
+    int nx, ny;
+    float goxd, gozd, dvxd, dvzd;
+} swdk_fmst_grid;
+
+/* per-receiver status of swdk_fmst_pairs (the reference prints and STOPs
+ * for the first three; its ray loop then reads an undefined point count) */
+#define SWDK_FMST_SOURCE_OUTSIDE 1    /* fmst.f90:159-167 */
+#define SWDK_FMST_RECEIVER_OUTSIDE 2  /* fmm.f90:1000-1007, fmst.f90:497-504 */
+#define SWDK_FMST_BAND_OVERFLOW 3     /* narrow band above snb*nnx*nnz nodes */
+#define SWDK_FMST_RAY_UNFINISHED 4    /* ray did not reach the source in nnx*nnz steps */
+
+/* Handle for one model grid on `device`: the grid constants (REAL*4, as
+ * fmst_init computes them) and the host-computed r*sin(colatitude) tables
+ * of the propagation grid and of every refined source grid. */
+int swdk_fmst_create(swdk_fmst** out, int device, const swdk_fmst_grid* grid);
+void swdk_fmst_destroy(swdk_fmst* fmst);
+const char* swdk_fmst_last_error(const swdk_fmst* fmst);
+
+/* Scratch budget for the per-pair marching grids (bytes; 0 keeps the
+ * current, 16 GiB by default), marching lanes per warp (1..32, a multiple of
+ * lanes_per_pair; default 8), resident marching warps per SM (0..64, default
+ * 12; 0 = one warp per group of pairs, all at once), heap entries per pair
+ * kept in shared memory (-1 = automatic, the default: 1.5 (nnx + nnz); 0 =
+ * heap in global memory; a pair whose band outgrows it is marched again with
+ * the full heap) and lanes per pair (1: one lane solves the four neighbours
+ * of each accepted node; 4, the default: four lanes solve one each).  None
+ * of them changes a result. */
+int swdk_fmst_set_options(swdk_fmst* fmst, size_t scratch_budget_bytes, int lanes_per_warp, int warps_per_sm,
+                          int smem_heap_entries, int lanes_per_pair);
+
+/* Propagation grid size; of the last swdk_fmst_pairs: device time, the
+ * largest narrow band (heap entries) and the pairs whose band outgrew the
+ * first pass's heap and were marched again with the reference's full heap.
+ * Any pointer may be NULL. */
+int swdk_fmst_info(const swdk_fmst* fmst, int* nnx, int* nnz, double* ms_last, int* max_band, int* overflow_pairs);
+
+/* All station pairs of one iteration.  HOST arrays (StationPair fields,
+ * SurfaceWave.hpp:53-82): pair p has period slot slot[p] (get_period_index,
+ * 0..kmax-1), source colatitude/longitude srcx[p], srcz[p] in radians,
+ * group[p] != 0 for Rg/Lg data, and receivers rcv_ptr[p]..rcv_ptr[p+1]-1 of
+ * rcx/rcz (radians).  DEVICE arrays: d_vc, d_vout are the phase and used
+ * velocity maps (nx*ny, kmax) column-major (vc and vout of get_2d_map /
+ * get_1d_kernel); outputs d_ttime[nrcv] (data[p.counter+i]: the receiver
+ * time of fmst_run, or for Rg/Lg pairs the ray's group traveltime), d_status
+ * [nrcv] (SWDK_FMST_*, NaN times where nonzero) and, if d_fdm is not NULL,
+ * the ray-path weights of every receiver as (nx, ny) column-major floats at
+ * d_fdm + r*nx*ny (fmst_raypath's fdm, the input of
+ * swdk_frechet_csr_device).  Without d_fdm only Rg/Lg receivers trace rays,
+ * as travel_time does.  Runs on `stream`; returns when the results are
+ * complete. */
+int swdk_fmst_pairs(swdk_fmst* fmst, int npairs, const int32_t* slot, const float* srcx, const float* srcz,
+                    const int32_t* group, const int64_t* rcv_ptr, const float* rcx, const float* rcz,
+                    const double* d_vc, const double* d_vout, int kmax, float* d_ttime, float* d_fdm,
+                    int32_t* d_status, void* stream);
 
 #ifdef __cplusplus
 }

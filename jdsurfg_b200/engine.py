@@ -267,12 +267,15 @@ class Engine:
                     "swdk_training_rows")
 
     def frechet_csr_device(self, nx, ny, nz, kmax, kernel, row_slot, fdm, rowptr, indices, values, stream=None):
-        """Frechet rows as CSR on the device; returns the number of nonzeros."""
+        """Frechet rows as CSR on the device; returns the number of nonzeros.
+        With indices None only the row pointer and the count are produced."""
         tot = C.c_int64(0)
         cap = 0 if indices is None else indices.numel()
-        self._check(lib().swdk_frechet_csr_device(self._h, nx, ny, nz, kmax, _p(kernel), len(row_slot), _p(row_slot),
-                                                  _p(fdm), _p(rowptr), _p(indices), _p(values), cap, C.byref(tot),
-                                                  stream), "swdk_frechet_csr_device")
+        rc = lib().swdk_frechet_csr_device(self._h, nx, ny, nz, kmax, _p(kernel), len(row_slot), _p(row_slot),
+                                           _p(fdm), _p(rowptr), _p(indices), _p(values), cap, C.byref(tot), stream)
+        if indices is None and rc == -5:  # SWDK_E_LIMIT: counted, nothing written
+            return tot.value
+        self._check(rc, "swdk_frechet_csr_device")
         return tot.value
 
     # -- CUDA graph of one device call, autotuner ------------------------------

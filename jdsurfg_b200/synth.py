@@ -182,3 +182,79 @@ def make_uneven_batch(nmodels=48, seed=5150, small=False, max_kernel_bytes=2 << 
         c["waves"], c["nmode"] = waves, nmode
         cases.append(c)
     return cases
+
+
+def make_survey(name="example", seed=7, nx=None, ny=None, nstation=None, nperiod=None, waves=("Rc", "Rg")):
+    """Seeded station pairs on a model grid, for the fast-marching path.
+
+    The reference's own data set cannot ship, so its shapes stand in:
+    example : 33 x 36 grid at 0.3 deg from (35.3 N, 99.7 E), 41 nodes every
+              2 km, 19 periods 4-40 s, Rayleigh phase and group, 80 stations
+              inside the grid; every station is a source for each (wave,
+              period) and records at ~18 % of the others (about 14
+              receivers per pair, ~3000 pairs, ~44 000 traveltimes)
+    production : the 128 x 128 production grid at 0.1 deg, 40 periods, 150
+              stations, the same fraction of receivers.
+    Returns dict(case=..., grid=(nx, ny, lat0, lon0, dlat, dlon), tables,
+    kmax_per_mode, pairs) with pairs as SurfTime holds them (colatitude and
+    longitude in radians, float32)."""
+    rng = np.random.default_rng(seed)
+    if name == "example":
+        nx, ny = nx or 33, ny or 36
+        lat0, lon0, d = 35.3, 99.7, 0.3
+        depth = (np.arange(41) * 2.0).astype(np.float32)
+        periods = np.arange(4.0, 41.0, 2.0)[: nperiod or 19]
+        nstation = nstation or 80
+        case = make_case(nx, ny, depth, 2.5, 4.6, 0.06, periods, waves, 1, seed)
+    elif name == "production":
+        nx, ny = nx or 128, ny or 128
+        lat0, lon0, d = 40.0, 100.0, 0.1
+        base = make_config("production", seed=seed, nx=nx, ny=ny)
+        periods = np.geomspace(1.0, 60.0, 40)[: nperiod or 40]
+        nstation = nstation or 150
+        case = make_case(nx, ny, base["depth"], 2.5, 4.7, 0.08, periods, waves, 1, seed, lvz_frac=0.2)
+    else:
+        raise ValueError(name)
+    # stations strictly inside the propagation grid (one model cell from each side)
+    lat = lat0 - d * rng.uniform(1.5, nx - 2.5, nstation)
+    lon = lon0 + d * rng.uniform(1.5, ny - 2.5, nstation)
+    d2r = np.float32(np.pi / 180.0)
+    colat = ((np.float32(90.0) - lat.astype(np.float32)) * d2r).astype(np.float32)
+    lonr = (lon.astype(np.float32) * d2r).astype(np.float32)
+    wt, modes, pidx, srcx, srcz, rptr, rcx, rcz = [], [], [], [], [], [0], [], []
+    for w in waves:
+        for ip in range(len(periods)):
+            for s in range(nstation):
+                others = np.flatnonzero(rng.random(nstation) < 0.18)
+                others = others[others != s]
+                if len(others) == 0:
+                    continue
+                wt.append(w)
+                modes.append(0)
+                pidx.append(ip)
+                srcx.append(colat[s])
+                srcz.append(lonr[s])
+                rcx.extend(colat[others])
+                rcz.extend(lonr[others])
+                rptr.append(rptr[-1] + len(others))
+    pairs = dict(wavetype=wt, mode=np.array(modes, np.int32), period_idx=np.array(pidx, np.int32),
+                 srcx=np.array(srcx, np.float32), srcz=np.array(srcz, np.float32),
+                 rcv_ptr=np.array(rptr, np.int64), rcx=np.array(rcx, np.float32), rcz=np.array(rcz, np.float32))
+    pairs["counter"] = pairs["rcv_ptr"][:-1].copy()
+    kmax_per_mode = [[len(periods)] if (case["tables"][i] is not None) else [] for i in range(4)]
+    return dict(case=case, grid=(nx, ny, lat0, lon0, d, d), tables=case["tables"], kmax_per_mode=kmax_per_mode,
+                pairs=pairs)
+
+
+def survey_slots(survey):
+    """(slot, group) per pair in get_period_index order."""
+    off, base = {}, 0
+    for w, km in zip(WAVES, survey["kmax_per_mode"]):
+        for m, k in enumerate(km):
+            off[(w, m)] = base
+            base += k
+    p = survey["pairs"]
+    slot = np.array([off[(w, int(m))] + int(i) for w, m, i in zip(p["wavetype"], p["mode"], p["period_idx"])],
+                    np.int32)
+    group = np.array([1 if w in ("Rg", "Lg") else 0 for w in p["wavetype"]], np.int32)
+    return slot, group

@@ -239,3 +239,66 @@ def group_u_spread(case, col, group_wave, periods, k, rel=1e-15, steps=(-3, -1, 
                            *[_ptr(x) for x in bufs[2:8]], 1)
         out.append(cg.value)
     return out[0], max(abs(u - out[0]) for u in out[1:])
+
+
+# ---------------------------------------------------------------------------
+# Fast-marching traveltimes and ray-path weights (oracle/fmst_oracle.cpp)
+
+def delsph(a, b, c, d):
+    f = lib().oracle_delsph
+    f.restype = C.c_float
+    f.argtypes = [C.c_float] * 4
+    return f(a, b, c, d)
+
+
+def ref_delsph(a, b, c, d):
+    """The reference's own src/shared/spherical.cpp delsph (oracle/_ref), or None."""
+    r = ref_cxx()
+    if r is None:
+        return None
+    r.delsph.restype = C.c_float
+    r.delsph.argtypes = [C.c_float] * 4
+    return r.delsph(a, b, c, d)
+
+
+def fmst_pairs(grid, pairs, vc, vout, want_fdm=False, nthreads=0):
+    """The per-pair loop of SurfTime::travel_time (want_fdm=False) or
+    frechet_matrix (want_fdm=True).  grid = (nx, ny, goxd, gozd, dvxd, dvzd);
+    pairs = dict(slot, srcx, srcz, rcv_ptr, rcx, rcz, group); vc, vout =
+    (kmax, nx*ny) float64 maps.  Returns ttime (nrcv) and fdm (nrcv, ny, nx)
+    float32 (None unless want_fdm)."""
+    nx, ny, goxd, gozd, dvxd, dvzd = grid
+    slot = np.ascontiguousarray(pairs["slot"], np.int32)
+    srcx, srcz = f32(pairs["srcx"]), f32(pairs["srcz"])
+    rptr = np.ascontiguousarray(pairs["rcv_ptr"], np.int64)
+    rcx, rcz = f32(pairs["rcx"]), f32(pairs["rcz"])
+    group = np.ascontiguousarray(pairs["group"], np.int32)
+    vc = np.ascontiguousarray(vc, np.float64)
+    vout = np.ascontiguousarray(vout, np.float64)
+    nrcv = int(rptr[-1])
+    tt = np.zeros(nrcv, np.float32)
+    fdm = np.zeros((nrcv, ny, nx), np.float32) if want_fdm else None
+    nthreads = nthreads or os.cpu_count()
+    lib().oracle_fmst_pairs(nx, ny, C.c_float(goxd), C.c_float(gozd), C.c_float(dvxd), C.c_float(dvzd), len(slot),
+                            _ptr(slot), _ptr(srcx), _ptr(srcz), _ptr(rptr), _ptr(rcx), _ptr(rcz), _ptr(group),
+                            _ptr(vc), _ptr(vout), _ptr(tt), _ptr(fdm), nthreads)
+    return tt, fdm
+
+
+def fmst_field(grid, vmap, srcx, srcz):
+    """Coarse traveltime field and node status after one fmst_run
+    ((nnz, nnx) arrays, column-major flattened as [ix][iz])."""
+    nx, ny, goxd, gozd, dvxd, dvzd = grid
+    L = lib()
+    L.fmst_init(nx, ny, C.c_float(goxd), C.c_float(gozd), C.c_float(dvxd), C.c_float(dvzd))
+    rc = np.array([srcx], np.float32)
+    rz = np.array([srcz], np.float32)
+    tt = np.zeros(1, np.float32)
+    L.fmst_run(_ptr(np.ascontiguousarray(vmap, np.float64)), C.c_float(srcx), C.c_float(srcz), _ptr(rc), _ptr(rz), 1,
+               _ptr(tt))
+    nnx, nnz = (nx - 3) * 8 + 1, (ny - 3) * 8 + 1
+    t = np.zeros(nnx * nnz, np.float32)
+    s = np.zeros(nnx * nnz, np.int32)
+    L.oracle_fmst_field(_ptr(t), _ptr(s), nnx * nnz)
+    L.fmst_finalize()
+    return t.reshape(nnx, nnz), s.reshape(nnx, nnz)

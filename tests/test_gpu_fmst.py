@@ -1,0 +1,213 @@
+"""Fast marching, receiver times, rays and ray-path Frechet weights on the
+GPU (swdk_fmst_pairs) against the CPU oracle's restatement of fmst.f90 /
+fmm.f90, on the same velocity maps.
+
+Tolerances: the marching itself is REAL*4 in the reference's order with the
+reference's heap, so receiver times of phase pairs must be bit-identical.
+Rays step with sin(colatitude) of each ray point; the device computes it as
+sin in double rounded to float while the C library's sinf (which the oracle,
+like the reference, calls) is off by one ulp for about 1 % of arguments, so
+ray times are held to 2e-6 relative and the weights to 1e-4 of each row's
+largest weight."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from jdsurfg_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+TOL_RAY_T = 2e-6
+TOL_FDM = 1e-4
+
+
+def _maps(survey, torch, dev):
+    m = O.get_2d_map(survey["case"])
+    vc = torch.from_numpy(m["vc"]).to(dev)
+    vout = torch.from_numpy(m["vout"]).to(dev)
+    return m, vc, vout
+
+
+def _subset(survey, idx):
+    p = survey["pairs"]
+    slot, group = synth.survey_slots(survey)
+    idx = np.asarray(idx)
+    rp = p["rcv_ptr"]
+    rcx = np.concatenate([p["rcx"][rp[i]:rp[i + 1]] for i in idx])
+    rcz = np.concatenate([p["rcz"][rp[i]:rp[i + 1]] for i in idx])
+    cnt = np.array([rp[i + 1] - rp[i] for i in idx])
+    return dict(slot=slot[idx], srcx=p["srcx"][idx], srcz=p["srcz"][idx], group=group[idx],
+                rcv_ptr=np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64), rcx=rcx, rcz=rcz)
+
+
+@pytest.fixture(scope="module")
+def example():
+    import torch
+    dev = torch.device("cuda", 0)
+    s = synth.make_survey("example")
+    m, vc, vout = _maps(s, torch, dev)
+    return s, m, vc, vout
+
+
+def test_receiver_times_bit_identical(example):
+    from jdsurfg_b200.fmst import FMST
+    s, m, vc, vout = example
+    rng = np.random.default_rng(0)
+    idx = np.sort(rng.choice(len(s["pairs"]["srcx"]), 300, replace=False))
+    pairs = _subset(s, idx)
+    pairs["group"] = np.zeros_like(pairs["group"])
+    ref, _ = O.fmst_pairs(s["grid"], pairs, m["vc"], m["vout"])
+    f = FMST(*s["grid"])
+    r = f.pairs(pairs, vc, vout)
+    tt, st = r["ttime"].cpu().numpy(), r["status"].cpu().numpy()
+    f.close()
+    assert (st == 0).all()
+    assert not np.isnan(ref).any()
+    bad = np.flatnonzero(tt != ref)
+    print(f"{len(tt)} receiver times, {len(bad)} differ; max rel "
+          f"{np.max(np.abs(tt - ref) / ref) if len(bad) else 0.0:.3g}")
+    assert len(bad) == 0
+
+
+def test_rays_weights_and_group_times(example):
+    from jdsurfg_b200.fmst import FMST
+    s, m, vc, vout = example
+    rng = np.random.default_rng(1)
+    idx = np.sort(rng.choice(len(s["pairs"]["srcx"]), 200, replace=False))
+    pairs = _subset(s, idx)
+    ref_t, ref_f = O.fmst_pairs(s["grid"], pairs, m["vc"], m["vout"], want_fdm=True)
+    f = FMST(*s["grid"])
+    r = f.pairs(pairs, vc, vout, want_fdm=True)
+    tt, st, fdm = r["ttime"].cpu().numpy(), r["status"].cpu().numpy(), r["fdm"].cpu().numpy()
+    f.close()
+    assert (st == 0).all()
+    grp = np.repeat(pairs["group"], np.diff(pairs["rcv_ptr"])).astype(bool)
+    # phase pairs: receiver times, bit-identical
+    assert np.array_equal(tt[~grp], ref_t[~grp])
+    # group pairs: times along the ray
+    rel = np.abs(tt[grp] - ref_t[grp]) / ref_t[grp]
+    scale = np.abs(ref_f).reshape(len(tt), -1).max(axis=1)
+    err = np.abs(fdm - ref_f).reshape(len(tt), -1).max(axis=1) / scale
+    same = np.mean([np.array_equal(a, b) for a, b in zip(fdm, ref_f)])
+    print(f"group times: max rel {rel.max():.3g}, identical {np.mean(rel == 0):.3f}; weights: max rel "
+          f"{err.max():.3g}, rows identical {same:.3f}")
+    assert rel.max() <= TOL_RAY_T
+    assert err.max() <= TOL_FDM
+
+
+def test_lanes_per_warp_do_not_change_results(example):
+    """One or several pairs per warp, one or four lanes per pair: the same bits."""
+    from jdsurfg_b200.fmst import FMST
+    s, m, vc, vout = example
+    pairs = _subset(s, np.arange(0, 3000, 37))
+    out = []
+    for lanes, per in ((1, 1), (8, 1), (32, 1), (4, 4), (32, 4)):
+        f = FMST(*s["grid"])
+        f.set_options(lanes_per_warp=lanes, warps_per_sm=0, lanes_per_pair=per)
+        r = f.pairs(pairs, vc, vout, want_fdm=True)
+        out.append((r["ttime"].cpu().numpy(), r["fdm"].cpu().numpy()))
+        f.close()
+    for t, w in out[1:]:
+        assert np.array_equal(t, out[0][0]) and np.array_equal(w, out[0][1])
+
+
+def test_heap_placement_does_not_change_results(example):
+    """Heap in global or shared memory, and a shared-memory heap too small for
+    the narrow band (every such pair is marched again with the reference's
+    full heap), give the same bits."""
+    from jdsurfg_b200.fmst import FMST
+    s, m, vc, vout = example
+    pairs = _subset(s, np.arange(3, 3000, 29))
+    out, info = [], []
+    for wps, heap, lanes, per in ((8, 0, 1, 1), (12, 1024, 1, 1), (4, 64, 1, 1), (16, 768, 8, 4), (8, 64, 4, 4)):
+        f = FMST(*s["grid"])
+        f.set_options(warps_per_sm=wps, smem_heap=heap, lanes_per_warp=lanes, lanes_per_pair=per)
+        r = f.pairs(pairs, vc, vout, want_fdm=True)
+        out.append((r["ttime"].cpu().numpy(), r["fdm"].cpu().numpy(), r["status"].cpu().numpy()))
+        info.append(f.last_info())
+        f.close()
+    print(info)
+    assert info[2]["overflow_pairs"] > 0 and info[4]["overflow_pairs"] > 0 and info[0]["overflow_pairs"] == 0
+    for t, w, st in out:
+        assert (st == 0).all()
+        assert np.array_equal(t, out[0][0]) and np.array_equal(w, out[0][1])
+
+
+def test_small_scratch_budget_chunks_pairs(example):
+    """Pairs split into many chunks (scratch budget of a few pairs) give the
+    same bits as one chunk."""
+    from jdsurfg_b200.fmst import FMST
+    s, m, vc, vout = example
+    pairs = _subset(s, np.arange(5, 2900, 61))
+    f = FMST(*s["grid"])
+    a = f.pairs(pairs, vc, vout, want_fdm=True)
+    f.set_options(scratch_budget_bytes=4 << 20)
+    b = f.pairs(pairs, vc, vout, want_fdm=True)
+    f.close()
+    assert np.array_equal(a["ttime"].cpu().numpy(), b["ttime"].cpu().numpy())
+    assert np.array_equal(a["fdm"].cpu().numpy(), b["fdm"].cpu().numpy())
+
+
+def test_outside_points_are_flagged(example):
+    from jdsurfg_b200.fmst import FMST, FMST_RECEIVER_OUTSIDE, FMST_SOURCE_OUTSIDE
+    s, m, vc, vout = example
+    pairs = _subset(s, [0, 1])
+    far = np.float32(np.pi / 2)  # the equator: outside the grid
+    pairs["rcx"] = pairs["rcx"].copy()
+    pairs["rcx"][0] = far
+    pairs["srcx"] = pairs["srcx"].copy()
+    pairs["srcx"][1] = far
+    f = FMST(*s["grid"])
+    r = f.pairs(pairs, vc, vout)
+    tt, st = r["ttime"].cpu().numpy(), r["status"].cpu().numpy()
+    f.close()
+    n0 = int(pairs["rcv_ptr"][1])
+    assert st[0] == FMST_RECEIVER_OUTSIDE and np.isnan(tt[0])
+    assert (st[1:n0] == 0).all() and not np.isnan(tt[1:n0]).any()
+    assert (st[n0:] == FMST_SOURCE_OUTSIDE).all() and np.isnan(tt[n0:]).all()
+
+
+def test_surftime_frechet_matrix_against_oracle(tmp_path):
+    """SurfTime.frechet_matrix end to end (device kernels, FMST, CSR rows,
+    the reference's row file) against the oracle's kernel, rays and rows."""
+    from jdsurfg_b200 import frechet_file
+    from jdsurfg_b200.surftime import SurfTime
+    s = synth.make_survey("example", nstation=14, nperiod=3, seed=3)
+    case = s["case"]
+    nx, ny, lat0, lon0, dlat, dlon = s["grid"]
+    st = SurfTime(device=0)
+    st.set_model(case["depth"], lat0, lon0, dlat, dlon, nx, ny)
+    st.set_data(s["tables"], s["kmax_per_mode"], s["pairs"])
+    out = str(tmp_path / "frechet.bin")
+    data, nnz, dev = st.frechet_matrix(case["vs"], out, return_device=True)
+    status = dev["fmst"]["status"].cpu().numpy()
+    tt_only = st.travel_time(case["vs"])
+    st.close()
+    bad = np.flatnonzero(status != 0)
+    assert len(bad) == 0, f"{len(bad)} receivers with status {np.unique(status[bad])}, first {bad[:5]}"
+    # oracle: kernels and maps, rays and weights, rows
+    ker = O.get_1d_kernel(case)
+    slot, group = synth.survey_slots(s)
+    p = s["pairs"]
+    pairs = dict(slot=slot, srcx=p["srcx"], srcz=p["srcz"], group=group, rcv_ptr=p["rcv_ptr"], rcx=p["rcx"],
+                 rcz=p["rcz"])
+    ref_t, ref_f = O.fmst_pairs(s["grid"], pairs, ker["vc"], ker["vout"], want_fdm=True)
+    ref_m = O.get_2d_map(case)
+    ref_tt, _ = O.fmst_pairs(s["grid"], pairs, ref_m["vc"], ref_m["vout"])
+    row_slot = np.repeat(slot, np.diff(p["rcv_ptr"])).astype(np.int32)
+    rows = O.frechet_rows(nx, ny, len(case["depth"]), ker["kernel"], row_slot,
+                          ref_f.reshape(len(ref_t), -1))
+    assert np.allclose(data, ref_t, rtol=1e-5, atol=0)
+    assert np.allclose(tt_only, ref_tt, rtol=1e-5, atol=0)
+    m, n, got = frechet_file.read_frechet(out)
+    assert m == len(ref_t) and n == (nx - 2) * (ny - 2) * (len(case["depth"]) - 1)
+    assert len(got) == len(rows) and sum(len(a) for _, a, _ in got) == nnz
+    same_pattern = 0
+    for (rid, gi, gv), (ri, rv) in zip(got, rows):
+        if np.array_equal(gi, ri):
+            same_pattern += 1
+            scale = np.abs(rv).max() if len(rv) else 1.0
+            assert np.abs(gv - rv).max(initial=0.0) <= 1e-3 * scale
+    print(f"{len(rows)} rows, {same_pattern} with the oracle's sparsity pattern, {nnz} nonzeros")
+    assert same_pattern >= 0.97 * len(rows)
+    assert [g[0] for g in got] == list(range(len(rows)))
