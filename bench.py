@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="swdk", choices=["swdk", "reference"])
-    ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny", "uneven"])
+    ap.add_argument("--workload", default="large", choices=["production", "large", "small", "tiny", "uneven", "fmst"])
     ap.add_argument("--proposal", default="learned", choices=["learned", "none"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-scan comparison timing")
     ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
@@ -199,9 +199,71 @@ def cpu_baseline(case, args, target_s):
                       f"reference-faithful refinement)"}, n2, dt
 
 
+FMST_METRIC = "fast-marching receivers/s (traveltime + ray-path Frechet weights, all station pairs)"
+FMST_UNIT = "receivers/s"
+
+
+def fmst_survey(rank=0):
+    from jdsurfg_b200 import synth
+    s = synth.make_survey("example", seed=7 + rank)
+    slot, group = synth.survey_slots(s)
+    p = s["pairs"]
+    pairs = dict(slot=slot, srcx=p["srcx"], srcz=p["srcz"], group=group, rcv_ptr=p["rcv_ptr"], rcx=p["rcx"],
+                 rcz=p["rcz"])
+    return s, pairs
+
+
+def fmst_config(s, pairs):
+    nx, ny = s["grid"][:2]
+    return {"workload": "fmst", "what": "station pairs shaped like the reference's example: 33x36 grid at 0.3 deg, "
+                                        "41 nodes, 19 periods 4-40 s, Rayleigh phase+group, 80 stations, "
+                                        "propagation grid 241x265 (8x dicing) plus 129x129 refined source grid",
+            "pairs": int(len(pairs["slot"])), "receivers": int(pairs["rcv_ptr"][-1]), "nx": nx, "ny": ny}
+
+
+def fmst_cpu_baseline(s, pairs, vc, vout, seconds):
+    """The oracle's per-pair loop (travel_time / frechet_matrix restated) on
+    every host core over the first pairs, sized to about `seconds`."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    cores = os.cpu_count() or 1
+    rp = pairs["rcv_ptr"]
+
+    def sub(n):
+        return dict(slot=pairs["slot"][:n], srcx=pairs["srcx"][:n], srcz=pairs["srcz"][:n], group=pairs["group"][:n],
+                    rcv_ptr=rp[:n + 1], rcx=pairs["rcx"], rcz=pairs["rcz"])
+    n = min(len(pairs["slot"]), 4 * cores)
+    t0 = time.perf_counter()
+    O.fmst_pairs(s["grid"], sub(n), vc, vout, want_fdm=True, nthreads=cores)
+    dt = time.perf_counter() - t0
+    n2 = int(min(len(pairs["slot"]), max(n, n * seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    O.fmst_pairs(s["grid"], sub(n2), vc, vout, want_fdm=True, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": int(rp[n2]) / dt, "unit": FMST_UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {n2} of {len(pairs['slot'])} pairs ({int(rp[n2])} receivers), rays and weights for "
+                      f"every receiver, OpenMP over pairs as SurfaceWave.cpp:583-672"}, n2
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
+        return 0
+    if args.workload == "fmst":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as O
+        s, pairs = fmst_survey(0)
+        m = O.get_2d_map(s["case"])
+        per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+        cb, n2 = fmst_cpu_baseline(s, pairs, m["vc"], m["vout"], per_step_s)
+        line = {"impl": "reference", "metric": FMST_METRIC, "value": cb["value"], "unit": FMST_UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * int(pairs["rcv_ptr"][-1]) / cb["value"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_survey)",
+                "config": fmst_config(s, pairs), "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": FMST_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return 0
     case = workload(args, 0)
     from jdsurfg_b200 import synth
@@ -228,6 +290,112 @@ def run_reference(args):
             "data": "synthetic (seeded generator, jdsurfg_b200/synth.py)", "config": case_desc(args, case, kmax),
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_fmst(args, torch, dev, rank, world, pg):
+    """One step = fast marching, receiver times, rays and ray-path Frechet
+    weights of every station pair of the example-shaped survey, with the
+    phase/group maps (from the GPU engine) resident in HBM; e2e = the whole
+    SurfTime.frechet_matrix (dispersion kernels, fast marching, CSR rows)
+    from the host model to the host data vector."""
+    from jdsurfg_b200 import Engine
+    from jdsurfg_b200.fmst import FMST
+    from jdsurfg_b200.surftime import SurfTime
+    s, pairs = fmst_survey(rank)
+    case = s["case"]
+    nx, ny = s["grid"][:2]
+    nz = len(case["depth"])
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    eng = Engine(device=dev.index)
+    eng.setup(case)
+    vs = torch.from_numpy(case["vs"]).to(dev)
+    vc = torch.empty((eng.kmax, nx * ny), dtype=torch.float64, device=dev)
+    vout = torch.empty_like(vc)
+    ker = torch.empty((eng.kmax, nz, nx * ny), dtype=torch.float64, device=dev)
+    st = torch.empty((eng.kmax, nx * ny), dtype=torch.int32, device=dev)
+    eng.get_1d_kernel_device(nx, ny, nz, vs, None, None, vc, vout, ker, st, stream=sp)
+    torch.cuda.synchronize()
+    f = FMST(*s["grid"], device=dev.index)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        r = f.pairs(pairs, vc, vout, want_fdm=True, stream=sp)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    ms, dev_ms = 0.0, 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = f.pairs(pairs, vc, vout, want_fdm=True, stream=sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        dev_ms += f.last_info()["ms"]
+    clk = clocks.stop()
+    info = f.last_info()
+    ok = int((r["status"] == 0).sum().item())
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    nrcv = int(pairs["rcv_ptr"][-1])
+    # e2e through the public API: host model in, host data out
+    stt = SurfTime(device=dev.index)
+    stt.set_model(case["depth"], *s["grid"][2:], nx, ny)
+    stt.set_data(s["tables"], s["kmax_per_mode"], s["pairs"])
+    stt.frechet_matrix(case["vs"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        data, nnz = stt.frechet_matrix(case["vs"])
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    stt.close()
+    # algorithmic bytes of the marching kernel per pair: the propagation grid
+    # (8-byte time+status per node) written and read once, its slowness read
+    # once, and the same for the 129x129 refined grid
+    N = f.nnx * f.nnz
+    alg = len(pairs["slot"]) * (N * 20 + 129 * 129 * 20)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            peaks = json.load(fp)
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    achieved = alg / (dev_ms / args.steps * 1e-3) / 1e9
+    if rank == 0:
+        cb, _ = fmst_cpu_baseline(s, pairs, vc.cpu().numpy(), vout.cpu().numpy(), args.cpu_seconds)
+        line = {"metric": FMST_METRIC, "value": world * nrcv / (ms / args.steps * 1e-3), "unit": FMST_UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_survey)",
+                "config": dict(fmst_config(s, pairs), l2="flushed between steps (256 MiB write)",
+                               max_band=info["max_band"], receivers_ok=ok),
+                "clocks": clk,
+                "e2e": {"value": world * nrcv / e2e_s, "unit": FMST_UNIT,
+                        "h2d_bytes_per_step": int(case["vs"].nbytes), "d2h_bytes_per_step": int(nrcv * 4),
+                        "what": "SurfTime.frechet_matrix: host model -> get_1d_kernel, fast marching, rays, "
+                                "CSR rows on the device -> host data vector", "nonzeros": int(nnz)},
+                "gpu_launches": 5 * args.steps,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": None,
+                             "note": "the marching is one dependent chain per pair (heap order); latency-bound, "
+                                     "the HBM fraction only states how far from bandwidth it is"},
+                "cpu_baseline": cb}
+        print(json.dumps(line), flush=True)
+    f.close()
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
     return 0
 
 
@@ -300,6 +468,8 @@ def main():
         pg = dist
     if args.workload == "uneven":
         return run_uneven(args, torch, dev, rank, world, pg)
+    if args.workload == "fmst":
+        return run_fmst(args, torch, dev, rank, world, pg)
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
     eng = Engine(device=local, refine=args.refine)
