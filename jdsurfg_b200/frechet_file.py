@@ -35,3 +35,19 @@ def read_frechet(path):
         pos += 4 * nnz
         rows.append((int(rid), idx.copy(), val.copy()))
     return int(m), int(n), rows
+
+
+def merge_frechet(parts, outfile, remove=True):
+    """The reference's merge_csr_files (src/shared/csr_matrix.cpp:205-242):
+    per-rank row files outfile.0, outfile.1, ... (each with its own m, n
+    header) concatenated into one file with the first header."""
+    import os
+    with open(outfile, "wb") as out:
+        for i, part in enumerate(parts):
+            with open(part, "rb") as f:
+                head = f.read(8)
+                if i == 0:
+                    out.write(head)
+                out.write(f.read())
+            if remove:
+                os.remove(part)

@@ -12,9 +12,17 @@ Blocks follow the reference's own task split (allocate_tasks,
 src/shared/parallel.cpp:3-19): the first ntasks % nprocs ranks get one
 extra column.
 
-The per-block computation is injected (`compute`), so the host logic --
-block bounds, padding, gather and reassembly -- is tested on CPU with gloo
-ranks; on GPUs the default computes with the rank's Engine.
+Station pairs shard the same way for fast marching: frechet_matrix gives
+each worker a contiguous block of pairs (allocate_tasks over pairs,
+SurfaceWave.cpp:583-600), each writes its own row file and the files are
+merged in rank order (merge_csr_files); the traveltimes of all pairs are
+all-gathered.  Every rank needs the whole vc/vout maps for that, which the
+column gather provides.
+
+The per-block computations are injected (`compute`, `march`), so the host
+logic -- block bounds, padding, gather and reassembly -- is tested on CPU
+with gloo ranks; on GPUs the defaults compute with the rank's Engine and
+FMST.
 """
 import numpy as np
 
@@ -30,14 +38,28 @@ def column_block(ncol, world, rank):
     return start, start + sub
 
 
-class ShardedSurfTime:
-    """get_2d_map / get_1d_kernel of one model split by columns across the
-    ranks of a torch.distributed process group."""
+def pair_subset(pairs, p0, p1):
+    """Pairs [p0, p1) with their receivers, receiver offsets from 0."""
+    rp = np.asarray(pairs["rcv_ptr"], np.int64)
+    r0, r1 = int(rp[p0]), int(rp[p1])
+    out = {k: np.asarray(pairs[k])[p0:p1] for k in ("slot", "srcx", "srcz", "group")}
+    out["rcv_ptr"] = rp[p0:p1 + 1] - r0
+    out["rcx"] = np.asarray(pairs["rcx"])[r0:r1]
+    out["rcz"] = np.asarray(pairs["rcz"])[r0:r1]
+    return out
 
-    def __init__(self, rank, world, group=None, engine=None, compute=None):
+
+class ShardedSurfTime:
+    """get_2d_map / get_1d_kernel of one model split by columns, and the
+    station pairs' fast marching split by pairs, across the ranks of a
+    torch.distributed process group."""
+
+    def __init__(self, rank, world, group=None, engine=None, compute=None, fmst=None, march=None):
         self.rank, self.world, self.group = rank, world, group
         self.engine = engine
         self.compute = compute
+        self.fmst = fmst
+        self.march = march
 
     def _block(self, arr, c0, c1):
         return None if arr is None else np.ascontiguousarray(arr[:, c0:c1])
@@ -87,3 +109,53 @@ class ShardedSurfTime:
         r = self._local("kernel", vs, vp, rho, c0, c1)
         vc, vout, st = self._gather_maps(r["vc"], r["vout"], r["status"], ncol)
         return dict(vc=vc, vout=vout, status=st, kernel=r["kernel"], columns=(c0, c1))
+
+    # -- fast marching over a block of the station pairs ---------------------
+    def _march(self, sub, vc, vout, want_fdm):
+        if self.march is not None:
+            return self.march(sub, vc, vout, want_fdm)
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        r = self.fmst.pairs(sub, torch.as_tensor(vc, device=dev), torch.as_tensor(vout, device=dev),
+                            want_fdm=want_fdm)
+        return (r["ttime"].cpu().numpy(), None if r["fdm"] is None else r["fdm"].cpu().numpy())
+
+    def _gather_times(self, tt, nrcv, rp):
+        """All-gather each rank's receiver times into the full data vector."""
+        import torch
+        import torch.distributed as dist
+        npairs = len(rp) - 1
+        rmax = max(int(rp[column_block(npairs, self.world, r)[1]] - rp[column_block(npairs, self.world, r)[0]])
+                   for r in range(self.world))
+        pad = np.full(rmax, np.nan, np.float32)
+        pad[:len(tt)] = tt
+        t = torch.from_numpy(pad)
+        if dist.get_backend(self.group) == "nccl":
+            t = t.cuda()
+        outs = [torch.empty_like(t) for _ in range(self.world)]
+        dist.all_gather(outs, t, group=self.group)
+        data = np.empty(nrcv, np.float32)
+        for r, o in enumerate(outs):
+            p0, p1 = column_block(npairs, self.world, r)
+            a, b = int(rp[p0]), int(rp[p1])
+            data[a:b] = o.cpu().numpy()[:b - a]
+        return data
+
+    def travel_time(self, pairs, vc, vout):
+        """SurfaceWave.cpp:510-541 over this rank's block of pairs; the full
+        data vector on every rank."""
+        rp = np.asarray(pairs["rcv_ptr"], np.int64)
+        p0, p1 = column_block(len(rp) - 1, self.world, self.rank)
+        tt, _ = self._march(pair_subset(pairs, p0, p1), vc, vout, False)
+        return self._gather_times(tt, int(rp[-1]), rp)
+
+    def frechet_pairs(self, pairs, vc, vout):
+        """This rank's pairs [p0, p1): receiver times and ray-path weights
+        (rows of frechet_matrix before the depth kernel multiplies them), and
+        the full data vector on every rank."""
+        rp = np.asarray(pairs["rcv_ptr"], np.int64)
+        p0, p1 = column_block(len(rp) - 1, self.world, self.rank)
+        tt, fdm = self._march(pair_subset(pairs, p0, p1), vc, vout, True)
+        return dict(data=self._gather_times(tt, int(rp[-1]), rp), fdm=fdm, pairs=(p0, p1),
+                    receivers=(int(rp[p0]), int(rp[p1])))
+
