@@ -354,8 +354,8 @@ const char* swdk_fmst_last_error(const swdk_fmst* fmst);
  * kept in shared memory (-1 = automatic, the default: 1.5 (nnx + nnz); 0 =
  * heap in global memory; a pair whose band outgrows it is marched again with
  * the full heap) and lanes per pair (1: one lane solves the four neighbours
- * of each accepted node; 4, the default: four lanes solve one each).  None
- * of them changes a result. */
+ * of each accepted node; 4, the default: four lanes solve one each; 8: a
+ * fifth lane keeps the heap meanwhile).  None of them changes a result. */
 int swdk_fmst_set_options(swdk_fmst* fmst, size_t scratch_budget_bytes, int lanes_per_warp, int warps_per_sm,
                           int smem_heap_entries, int lanes_per_pair);
 

@@ -85,7 +85,8 @@ __global__ void k_fmst_refvel(Grid G, int npair, const int32_t* __restrict__ cp,
 
 // fmst.f90:108-310: each warp marches `lanes / per` pairs at a time, `per`
 // lanes per pair (1: one lane solves all four neighbours of an accepted
-// node; 4: four lanes solve one each, lane 0 of the four owns the heap), and
+// node; 4: four lanes solve one each, lane 0 of the four owns the heap; 8:
+// lane 0 owns the heap and lanes 1-4 solve), and
 // loops over the pairs; the grid holds the number of warps per SM that keeps
 // the marching fronts in L1.
 __global__ void __launch_bounds__(128) k_fmst_travel(Grid G, int npair, int lanes, int per,
@@ -98,8 +99,9 @@ __global__ void __launch_bounds__(128) k_fmst_travel(Grid G, int npair, int lane
     const int lane = threadIdx.x & 31;
     if (lane >= lanes) return;
     const int ppw = lanes / per, slot = lane / per;
-    const int g4 = per == 4 ? (lane & 3) : 0;
-    const unsigned gmask = per == 4 ? (0xFu << (lane & ~3)) : (1u << lane);
+    const int g4 = lane % per;        // lane within the pair's group
+    if (per == 8 && g4 > 4) return;   // groups of eight use five lanes
+    const unsigned gmask = per == 1 ? (1u << lane) : per == 4 ? (0xFu << (lane & ~3)) : (0x1Fu << (lane & ~7));
     // with smem_cap > 0 each pair's heap (1..smem_cap) lives in shared memory;
     // a band that outgrows it flags the pair for a second pass with the full
     // heap in global memory
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(128) k_fmst_travel(Grid G, int npair, int lane
         const int p = warp * ppw + slot;
         if (p >= npair) return;  // the same for the lanes of one pair
         march_pair(G, p, cp[p], srcx, srcz, pslot, slwn, risti_c, risti_r, S, n_overflow, hp, smem_cap,
-                   per == 4 ? 2 : 0, g4, gmask);
+                   per == 1 ? 0 : per == 4 ? 2 : 3, g4, gmask);
     }
 }
 
@@ -437,7 +439,8 @@ extern "C" const char* swdk_fmst_last_error(const swdk_fmst* f) { return f ? f->
 extern "C" int swdk_fmst_set_options(swdk_fmst* f, size_t scratch_budget_bytes, int lanes_per_warp,
                                      int warps_per_sm, int smem_heap_entries, int lanes_per_pair) {
     if (!f || lanes_per_warp < 1 || lanes_per_warp > 32 || warps_per_sm < 0 || warps_per_sm > 64 ||
-        smem_heap_entries < -1 || (lanes_per_pair != 1 && lanes_per_pair != 4) || lanes_per_warp % lanes_per_pair ||
+        smem_heap_entries < -1 || (lanes_per_pair != 1 && lanes_per_pair != 4 && lanes_per_pair != 8) ||
+        lanes_per_warp % lanes_per_pair ||
         (size_t)(lanes_per_warp / lanes_per_pair) * ((smem_heap_entries + 2) & ~1) * sizeof(FHeap) > 200 * 1024)
         return SWDK_E_ARG;
     f->smem_heap = smem_heap_entries;

@@ -388,8 +388,9 @@ struct March {
         const int z = iz + dz, x = ix + dx;
         if (z < 1 || z > nnz || x < 1 || x > nnx) return -2;
         const int n = idx(z, x);
+        // the neighbour's status, its stencil and slowness in one round of loads
         const int s = nd[n].s;
-        if (!(s == -1 || s > 0)) return s;
+        const float sl = slw[n];
         FNode w[7][7];
         w[3][2] = wload(z, x, 0, -1);
         w[3][4] = wload(z, x, 0, 1);
@@ -404,7 +405,7 @@ struct March {
         else if (dx == 1) w[3][2] = FNode{tacc, 0};
         else if (dz == -1) w[4][3] = FNode{tacc, 0};
         else w[2][3] = FNode{tacc, 0};
-        *t = fouds2w<0, 0>(w, z, x, slw[n], risti_at(x));
+        if (s == -1 || s > 0) *t = fouds2w<0, 0>(w, z, x, sl, risti_at(x));
         return s;
     }
 
@@ -432,14 +433,18 @@ struct March {
     }
 
 #if defined(__CUDA_ARCH__)
-    // march() by the four lanes of a group (g4 = lane & 3, mask gmask): lane
-    // g4 solves neighbour g4 (x-1, x+1, z-1, z+1); lane 0 of the group owns
-    // the heap, sifts it down meanwhile and applies the four updates in the
-    // reference's order.  Every lane of the group runs this with the same
-    // March state; only lane 0's heap fields are live.
-    __device__ void march_coop(bool refined, const PairGeo& g, int g4, unsigned gmask) {
-        const int lead = (int)(threadIdx.x & 31) & ~3;
-        const int dz = g4 == 2 ? -1 : (g4 == 3 ? 1 : 0), dx = g4 == 0 ? -1 : (g4 == 1 ? 1 : 0);
+    // march() by the lanes of a group (lane g4 of the group, mask gmask): the
+    // lanes base .. base+3 solve the trial times of the neighbours x-1, x+1,
+    // z-1, z+1; lane 0 of the group owns the heap, sifts it down meanwhile
+    // and applies the four updates in the reference's order.  base = 0: lane
+    // 0 also solves x-1 (groups of four lanes); base = 1: lane 0 only keeps
+    // the heap, so its sift-down overlaps the solves (groups of eight lanes,
+    // five of them active).  Every lane runs this with the same March state;
+    // only lane 0's heap fields are live.
+    __device__ void march_coop(bool refined, const PairGeo& g, int g4, unsigned gmask, int base) {
+        const int lead = __ffs(gmask) - 1;
+        const int q = g4 - base;  // neighbour this lane solves (0..3), or none
+        const int dz = q == 2 ? -1 : (q == 3 ? 1 : 0), dx = q == 0 ? -1 : (q == 1 ? 1 : 0);
         for (;;) {
             int go = 0, pk = 0;
             float tacc = 0.0f;
@@ -458,14 +463,15 @@ struct March {
             __syncwarp(gmask);
             const int iz = (pk & 0xFFFF) + 1, ix = (pk >> 16) + 1;
             float t = 0.0f;
-            const int s = solve_neighbour(iz, ix, tacc, dz, dx, &t);
+            int s = -2;
+            if (q >= 0 && q < 4) s = solve_neighbour(iz, ix, tacc, dz, dx, &t);
             if (g4 == 0) downtree();
-            const int s1 = __shfl_sync(gmask, s, lead + 1), s2 = __shfl_sync(gmask, s, lead + 2),
-                      s3 = __shfl_sync(gmask, s, lead + 3);
-            const float t1 = __shfl_sync(gmask, t, lead + 1), t2 = __shfl_sync(gmask, t, lead + 2),
-                        t3 = __shfl_sync(gmask, t, lead + 3);
+            const int s0 = __shfl_sync(gmask, s, lead + base), s1 = __shfl_sync(gmask, s, lead + base + 1),
+                      s2 = __shfl_sync(gmask, s, lead + base + 2), s3 = __shfl_sync(gmask, s, lead + base + 3);
+            const float t0 = __shfl_sync(gmask, t, lead + base), t1 = __shfl_sync(gmask, t, lead + base + 1),
+                        t2 = __shfl_sync(gmask, t, lead + base + 2), t3 = __shfl_sync(gmask, t, lead + base + 3);
             if (g4 == 0) {
-                apply(iz, ix - 1, s, t);
+                apply(iz, ix - 1, s0, t0);
                 apply(iz, ix + 1, s1, t1);
                 apply(iz - 1, ix, s2, t2);
                 apply(iz + 1, ix, s3, t3);
@@ -567,19 +573,20 @@ FM_HD void march_pair(const Grid& G, int p, int gp, const float* __restrict__ sr
                            FHeap* hp, int smem_cap, int mode, int g4, unsigned gmask) {
     // mode 0: one lane, window march; 1: one lane, neighbours one by one;
     // 2: the four lanes g4 = 0..3 of mask gmask march the pair together
-    // (lane 0 writes the grids and owns the heap).
+    // (lane 0 writes the grids and owns the heap); 3: five lanes, lane 0 only
+    // owns the heap and lanes 1..4 solve.
     PairGeo g = S.geo[p];
     if (g.status) return;
     const bool lead = g4 == 0;
     auto group_sync = [&]() {
 #if defined(__CUDA_ARCH__)
-        if (mode == 2) __syncwarp(gmask);
+        if (mode >= 2) __syncwarp(gmask);
 #endif
     };
     auto run = [&](March& M, bool refined) {
         if (mode == 1) M.march_nb(refined, g);
 #if defined(__CUDA_ARCH__)
-        else if (mode == 2) M.march_coop(refined, g, g4, gmask);
+        else if (mode == 2 || mode == 3) M.march_coop(refined, g, g4, gmask, mode == 3 ? 1 : 0);
 #endif
         else M.march(refined, g);
     };

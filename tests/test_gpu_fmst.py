@@ -96,12 +96,12 @@ def test_rays_weights_and_group_times(example):
 
 
 def test_lanes_per_warp_do_not_change_results(example):
-    """One or several pairs per warp, one or four lanes per pair: the same bits."""
+    """One or several pairs per warp, one, four or eight lanes per pair: the same bits."""
     from jdsurfg_b200.fmst import FMST
     s, m, vc, vout = example
     pairs = _subset(s, np.arange(0, 3000, 37))
     out = []
-    for lanes, per in ((1, 1), (8, 1), (32, 1), (4, 4), (32, 4)):
+    for lanes, per in ((1, 1), (8, 1), (32, 1), (4, 4), (32, 4), (8, 8), (32, 8)):
         f = FMST(*s["grid"])
         f.set_options(lanes_per_warp=lanes, warps_per_sm=0, lanes_per_pair=per)
         r = f.pairs(pairs, vc, vout, want_fdm=True)
@@ -211,3 +211,39 @@ def test_surftime_frechet_matrix_against_oracle(tmp_path):
     print(f"{len(rows)} rows, {same_pattern} with the oracle's sparsity pattern, {nnz} nonzeros")
     assert same_pattern >= 0.97 * len(rows)
     assert [g[0] for g in got] == list(range(len(rows)))
+
+
+def test_surftime_compute_grad_against_oracle():
+    """SurfTime.compute_grad (SurfaceWave.cpp:697-782): the Frechet rows times
+    (t - obs), summed, times vs at the interior nodes, against the same sum
+    over the oracle's rows (FP64 sums on both sides; rows within the kernel
+    and weight tolerances, so the gradient within 1e-4 of its largest entry)."""
+    from jdsurfg_b200.surftime import SurfTime
+    s = synth.make_survey("example", nstation=12, nperiod=2, seed=5)
+    case = s["case"]
+    nx, ny, lat0, lon0, dlat, dlon = s["grid"]
+    nz = len(case["depth"])
+    rng = np.random.default_rng(0)
+    nrcv = int(s["pairs"]["rcv_ptr"][-1])
+    obst = (rng.uniform(20.0, 200.0, nrcv)).astype(np.float32)
+    st = SurfTime(device=0)
+    st.set_model(case["depth"], lat0, lon0, dlat, dlon, nx, ny)
+    st.set_data(s["tables"], s["kmax_per_mode"], s["pairs"], obst=obst)
+    data, grad = st.compute_grad(case["vs"])
+    st.close()
+    ker = O.get_1d_kernel(case)
+    slot, group = synth.survey_slots(s)
+    p = s["pairs"]
+    pairs = dict(slot=slot, srcx=p["srcx"], srcz=p["srcz"], group=group, rcv_ptr=p["rcv_ptr"], rcx=p["rcx"],
+                 rcz=p["rcz"])
+    ref_t, ref_f = O.fmst_pairs(s["grid"], pairs, ker["vc"], ker["vout"], want_fdm=True)
+    row_slot = np.repeat(slot, np.diff(p["rcv_ptr"])).astype(np.int32)
+    rows = O.frechet_rows(nx, ny, nz, ker["kernel"], row_slot, ref_f.reshape(nrcv, -1))
+    n = (nx - 2) * (ny - 2) * (nz - 1)
+    g = np.zeros(n)
+    for r, (ii, vv) in enumerate(rows):
+        g[ii] += vv.astype(np.float64) * (float(ref_t[r]) - float(obst[r]))
+    vs3 = case["vs"].reshape(nz, ny, nx)[:nz - 1, 1:-1, 1:-1].reshape(-1)
+    g *= vs3
+    assert np.allclose(data, ref_t, rtol=1e-5, atol=0)
+    assert np.abs(grad - g).max() <= 1e-4 * np.abs(g).max()
