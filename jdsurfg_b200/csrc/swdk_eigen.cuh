@@ -521,6 +521,7 @@ SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, doub
   double exr = 0.0;
   int exi = 0;
   double ca[5][5];
+#pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = L - 2; m >= 0; --m) {
     const double zam = M.za[m], zbm = M.zb[m], zdm = M.zd[m];
     const int iw = (zbm > 0.0) ? 0 : 1;
@@ -559,6 +560,7 @@ SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, doub
   EnergyAcc acc = {0.0, 0.0, 0.0, 0.0};
   const double c = omega / wvno;
   double AA[4][4];
+#pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = 0; m < L; ++m) {
     const double zbm = M.zb[m];
     const int iw = (zbm > 0.0) ? 0 : 1;
@@ -619,6 +621,7 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
     }
     s0[2] = 0.0;
   }
+#pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = L - 2; k >= 0; --k) {
     double* sk = scr + 3 * k;
     const double zb = M.zb[k];
@@ -657,6 +660,7 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
   double ext = 0.0;
   double umax = scr[0];
   scr[1] = 0.0;  // tt(1) = 0
+#pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = 1; k < L; ++k) {
     double* sk = scr + 3 * k;
     if (M.zb[k] > 0.0) {
@@ -675,6 +679,7 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
   const double c = omega / wvno;
   double sumi0 = 0.0, sumi1 = 0.0;
   double prev_uu = scr[0] * iumax, prev_tt = scr[1] * iumax;
+#pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = 0; k < L; ++k) {
     const double uu = prev_uu, tt = prev_tt;
     double nuu = 0.0, ntt = 0.0;
