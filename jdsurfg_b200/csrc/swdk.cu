@@ -580,8 +580,55 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
   }
 }
 
+// One round of the getsol scan (surfdisp96.f:452-486) by a whole warp.  The
+// chain machine has just asked for f at the next scan point c2 = s.creq (the
+// point counted in s.nscan).  Lane j evaluates the point j steps further on,
+// accumulated step by step exactly as the scan does; lanes past a point the
+// scan would not evaluate (below clow going down, beyond the scan cap) stay
+// idle.  The first point, in scan order, with a sign change from its
+// predecessor or failing the range test ends the round: the state becomes the
+// one the sequential scan reaches there (refinement bracket or failure), so
+// the root is the sequential scan's.  Without such a point the scan goes on
+// from the last evaluated point.  Every lane holds the same state and leaves
+// with the same state.  Returns the evaluations the sequential scan makes.
+__device__ int retry_scan(ChainState& s, const ChainParams& P, const LayerView& V, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const double step = s.idir > 0 ? DC : -DC;
+  double p = s.creq;
+  for (int i = 0; i < lane; ++i) p = p + step;
+  const bool valid = lane == 0 || ((s.idir > 0 || p > s.clow) && s.nscan + lane <= SCAN_CAP);
+  const double f = valid ? secular_fast(V, P.iwave, P.refine, s.omega / p, s.omega) : 0.0;
+  double fprev = __shfl_up_sync(FULL, f, 1);
+  if (lane == 0) fprev = s.del1;
+  const bool sc = valid && dsign1(fprev) != dsign1(f);
+  const bool fail = valid && !sc && (p < s.cm || p >= ((double)P.betmx + DC) || !(p == p));
+  const unsigned ev = __ballot_sync(FULL, sc || fail);
+  const int nvalid = __popc(__ballot_sync(FULL, valid));  // the valid lanes are a prefix
+  const int e = ev ? __ffs(ev) - 1 : nvalid - 1;          // the point the round ends at
+  const double pe = __shfl_sync(FULL, p, e), fe = __shfl_sync(FULL, f, e);
+  const double pb = __shfl_sync(FULL, p, e > 0 ? e - 1 : 0), fb = __shfl_sync(FULL, f, e > 0 ? e - 1 : 0);
+  const bool sce = __shfl_sync(FULL, sc ? 1 : 0, e) != 0;
+  s.nscan += e;
+  s.last = fe;
+  if (ev && sce) {  // sign change between the previous point and pe: refine
+    if (e > 0) { s.c1 = pb; s.del1 = fb; }
+    s.c2 = pe;
+    s.del2 = fe;
+    s.phase = PH_REFINE_START;
+  } else {  // the scan moved on to pe: failed there, or continues from it
+    s.c1 = pe; s.del1 = fe;
+    s.c2 = pe; s.del2 = fe;
+    s.phase = ev ? PH_GS_FAIL : PH_SCAN;
+  }
+  return e + 1;
+}
+
 // k_retry: the deferred single-period retries (surfdisp.cpp:94-109), one
-// per thread; a warp takes 32 records at a time
+// record per warp.  A retry re-runs the reference's search for one period
+// from its start value, a scan of often several hundred dc steps; the warp's
+// lanes hold the same chain state and take the scan 32 points at a time
+// (retry_scan), the other requests (start point, refinement) are evaluated
+// by all lanes alike.
 __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const int* __restrict__ order,
                                                                const ChainDesc* __restrict__ chains,
                                                                const double* __restrict__ periods,
@@ -594,32 +641,24 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                const unsigned int* __restrict__ retry_count,
                                                                unsigned int retry_cap, unsigned int* __restrict__ queue,
                                                                unsigned long long* __restrict__ nevals) {
-  __shared__ ChainState sst[128];  // chain state in shared memory, as in k_roots_queue
+  __shared__ ChainState sst[128];  // one copy of the warp's chain state per lane
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
   const unsigned int n = min(*retry_count, retry_cap);
   const int lane = threadIdx.x & 31;
   unsigned long long ev_r = 0, lay_r = 0, lay_l = 0;
   for (;;) {
-    unsigned int base = 0;
-    if (lane == 0) base = atomicAdd(queue, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    const unsigned int r = base + lane;
-    const bool active = r < n;
+    unsigned int r = 0;
+    if (lane == 0) r = atomicAdd(queue, 1u);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= n) break;
     ChainState& s = sst[threadIdx.x];
     ChainParams P;
     ChainIO io;
     LayerView V;
-    ChainDesc cd = chains[order[0]];
-    int col = 0, m = 1, k = 1;
-    if (active) {
-      const int2 rec = retry_list[r];
-      cd = chains[order[rec.x / ncol]];
-      col = rec.x % ncol;
-      m = rec.y >> 16;
-      k = rec.y & 0xffff;
-    }
+    const int2 rec = retry_list[r];
+    const ChainDesc cd = chains[order[rec.x / ncol]];
+    const int col = rec.x % ncol, m = rec.y >> 16, k = rec.y & 0xffff;
     const ColInfo ci = info[col];
     V.lay = (cd.iwave == 2) ? layR : layL;
     V.fast = 1;
@@ -645,24 +684,23 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     io.stride = cd.np * ncol;
     io.ostride = ncol;
     io.prop = nullptr;
-    // run_chain's warp loop with a retry start state
     chain_init_retry(s, m, k);
-    bool act = active;
-    for (;;) {
-      const bool need = act && chain_advance(s, P, io);
-      if (!need) act = false;
-      if (__ballot_sync(0xffffffffu, need) == 0u) break;
-      if (need) {
-        s.last = secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega);
-        s.nevals++;
-        s.phase = s.next;
+    unsigned long long nev = 0;
+    while (chain_advance(s, P, io)) {  // the same decision in every lane
+      if (s.next == PH_SCAN_GOT) {
+        nev += retry_scan(s, P, V, lane);
+        continue;
       }
+      s.last = secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega);
+      nev++;
+      s.phase = s.next;
     }
-    if (active) {
+    __syncwarp();
+    if (lane == 0) {
       if (s.iterlim && st_at(io, m, k) != ST_NO_ROOT) st_at(io, m, k) = ST_ITER_LIMIT;
-      ev_r += s.nevals;
-      if (cd.iwave == 2) lay_r += (unsigned long long)s.nevals * V.L;
-      else lay_l += (unsigned long long)s.nevals * V.L;
+      ev_r += nev;
+      if (cd.iwave == 2) lay_r += nev * V.L;
+      else lay_l += nev * V.L;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
