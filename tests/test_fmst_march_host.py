@@ -75,3 +75,46 @@ def test_gpu_marching_code_matches_oracle(kw, mode):
     rt, rs = O.fmst_field(s["grid"], m["vc"][pairs["slot"][1]], float(pairs["srcx"][1]), float(pairs["srcz"][1]))
     assert np.array_equal(fs == 0, rs == 0) and (fs == 0).all()
     assert np.array_equal(ft, rt)
+
+
+def _edge_pairs(grid, d2r=np.float32(np.pi / 180)):
+    """Sources on propagation-grid nodes (a homogeneous model then gives
+    exactly equal times in symmetric directions, so the heap's order among
+    ties decides the result) and next to each side and corner of the grid
+    (the refined source grid then reaches the model's sides)."""
+    nx, ny, lat0, lon0, dl, _ = grid
+    # the propagation grid spans model nodes 1 .. nx-2 (lat) and 1 .. ny-2 (lon)
+    lat_lo, lat_hi = lat0 - (nx - 2) * dl, lat0 - dl
+    lon_lo, lon_hi = lon0 + dl, lon0 + (ny - 2) * dl
+    e = 0.02 * dl
+    srcs = [(lat0 - 5 * dl, lon0 + 6 * dl), (lat0 - 5 * dl - dl / 8, lon0 + 6 * dl + dl / 8),
+            (lat_hi - e, lon0 + 5 * dl), (lat_lo + e, lon0 + 5 * dl), (lat0 - 4 * dl, lon_lo + e),
+            (lat0 - 4 * dl, lon_hi - e), (lat_hi - e, lon_lo + e), (lat_lo + e, lon_hi - e)]
+    rng = np.random.default_rng(3)
+    rlat = np.concatenate([rng.uniform(lat_lo + e, lat_hi - e, 10), [lat_lo + e, lat_hi - e, lat0 - 5 * dl]])
+    rlon = np.concatenate([rng.uniform(lon_lo + e, lon_hi - e, 10), [lon_hi - e, lon_lo + e, lon0 + 6 * dl]])
+    col = lambda lat: np.float32((np.float32(90.0) - np.float32(lat)) * d2r)
+    lon = lambda x: np.float32(np.float32(x) * d2r)
+    pairs = dict(slot=np.zeros(len(srcs), np.int32), srcx=np.array([col(a) for a, _ in srcs], np.float32),
+                 srcz=np.array([lon(b) for _, b in srcs], np.float32), group=np.zeros(len(srcs), np.int32),
+                 rcv_ptr=np.arange(len(srcs) + 1, dtype=np.int64) * len(rlat),
+                 rcx=np.tile([col(a) for a in rlat], len(srcs)).astype(np.float32),
+                 rcz=np.tile([lon(b) for b in rlon], len(srcs)).astype(np.float32))
+    return pairs
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_ties_and_grid_sides_match_oracle(mode):
+    grid = (14, 16, 40.0, 100.0, 0.3, 0.3)
+    nx, ny = grid[:2]
+    pairs = _edge_pairs(grid)
+    for v in (np.full((1, nx * ny), 3.0), 3.0 + 0.3 * np.sin(np.arange(nx * ny))[None, :]):
+        tt, _, _, band = _run(grid, pairs, v, field_pair=0, mode=mode)
+        assert band > 0
+        ref, _ = O.fmst_pairs(grid, pairs, v, v)
+        assert not np.isnan(ref).any()
+        assert np.array_equal(tt, ref)
+        for p in (0, 1, 2, 6):
+            _, ft, fs, _ = _run(grid, pairs, v, field_pair=p, mode=mode)
+            rt, rs = O.fmst_field(grid, v[0], float(pairs["srcx"][p]), float(pairs["srcz"][p]))
+            assert np.array_equal(ft, rt) and (fs == 0).all()
