@@ -23,6 +23,7 @@ using std::max;
 using std::min;
 inline int __float_as_int(float x) { int i; std::memcpy(&i, &x, 4); return i; }
 inline float __double2float_rn(double x) { return (float)x; }
+inline float __int_as_float(int i) { float x; std::memcpy(&x, &i, 4); return x; }
 struct float4 { float x, y, z, w; };
 #endif
 
@@ -786,6 +787,187 @@ FM_HD float srtimes(const Grid& G, const RayIn& in, const PairGeo& g, float scx,
     return trr;
 }
 
+
+// src/shared/spherical.cpp:9-27
+FM_HD FM_INLINE float delsph(float colatrad1, float lonrad1, float colatrad2, float lonrad2) {
+    const float R = 6371.0f;
+    float dlat = colatrad2 - colatrad1;
+    float dlon = lonrad2 - lonrad1;
+    float lat1 = __double2float_rn(M_PI * 0.5 - (double)colatrad1);
+    float lat2 = __double2float_rn(M_PI * 0.5 - (double)colatrad2);
+    double s1 = sin((double)dlat * 0.5), s2 = sin((double)dlon * 0.5);
+    float a = __double2float_rn(s1 * s1 + s2 * s2 * cos((double)lat1) * cos((double)lat2));
+    float c = __double2float_rn(2.0 * atan2(sqrt((double)a), sqrt((double)(1.0f - a))));
+    return R * c;
+}
+
+// fmst.f90:350-976 for one receiver: returns tsyn; fdm (if not null) gets the
+// (nx, ny) column-major weights, accumulated in the reference's order.
+// sin_f(x) gives sin(colatitude) of a ray point (the reference: the C
+// library's sinf); sin_rcx is that of the receiver.
+template <class Sin>
+FM_HD float raypath(const Grid& G, const RayIn& in, const PairGeo& g, float scx, float scz, float rcx, float rcz,
+                    float sin_rcx, float* fdm, int* status, Sin sin_f) {
+    const float dpl = 0.5f * G.dpl;
+    const float dnxr = G.drnx, dnzr = G.drnz, goxr = g.gorx, gozr = g.gorz;
+    const int nnxr = g.nrnx, nnzr = g.nrnz;
+    auto TT = [&](int iz, int ix) { return in.coarse[(iz - 1) + (size_t)(ix - 1) * G.nnz].t; };
+    auto TR = [&](int iz, int ix) { return in.fine[(iz - 1) + (size_t)(ix - 1) * RMAX].t; };
+    auto SR = [&](int iz, int ix) { return in.fine[(iz - 1) + (size_t)(ix - 1) * RMAX].s; };
+    const int isx = (int)((scx - goxr) / dnxr) + 1;
+    const int isz = (int)((scz - gozr) / dnzr) + 1;
+    int ipx = (int)((rcx - G.gox) / G.dnx) + 1;
+    int ipz = (int)((rcz - G.goz) / G.dnz) + 1;
+    if (ipx < 1 || ipx >= G.nnx || ipz < 1 || ipz >= G.nnz) {
+        *status = SWDK_FMST_RECEIVER_OUTSIDE;
+        return __int_as_float(0x7fc00000);
+    }
+    float px = rcx, pz = rcz;  // rgx(j), rgz(j)
+    float sin_px = sin_rcx;
+    int sw = 0;
+    float sred = sq((scx - px) * EARTH);
+    sred = sred + sq((scz - pz) * EARTH * sin_px);
+    sred = sqrtf(sred);
+    if (sred < 2.0f * dpl) sw = 1;
+    auto in_refined = [&](float qx, float qz, int& ixr, int& izr) {
+        ixr = (int)((qx - goxr) / dnxr) + 1;
+        izr = (int)((qz - gozr) / dnzr) + 1;
+        if (ixr < 1 || ixr >= nnxr || izr < 1 || izr >= nnzr) return 0;
+        if (SR(izr, ixr) != 0 || SR(izr + 1, ixr) != 0) return 0;
+        if (SR(izr, ixr + 1) != 0 || SR(izr + 1, ixr + 1) != 0) return 0;
+        return 1;
+    };
+    int ipxr, ipzr;
+    int igref = in_refined(rcx, rcz, ipxr, ipzr);
+    if (sw == 0 && igref == 1 && ipxr == isx && ipzr == isz) sw = 1;
+    float tsyn = 0.0f;
+    // traveltime along the ray (fmst.f90:916-946), accumulated segment by
+    // segment once both ends are final
+    auto seg_time = [&](float ax, float az, float bx, float bz) {
+        float dinc = delsph(ax, az, bx, bz);
+        int ipxo = (int)((ax - G.gox) / G.dnx) + 1, ipzo = (int)((az - G.goz) / G.dnz) + 1;
+        float velo = vel_at(G, in.velg, ax, az, ipxo, ipzo);
+        ipxo = (int)((bx - G.gox) / G.dnx) + 1;
+        ipzo = (int)((bz - G.goz) / G.dnz) + 1;
+        float vel = vel_at(G, in.velg, bx, bz, ipxo, ipzo);
+        tsyn = tsyn + dinc * 0.5f * (1.0f / vel + 1.0f / velo);
+    };
+    if (sw == 1) {
+        seg_time(px, pz, scx, scz);
+        return tsyn;
+    }
+    const long maxrp = (long)G.nnx * G.nnz;
+    for (long j = 1; j <= maxrp; ++j) {
+        float dtx, dtz;
+        if (igref == 1) {
+            dtx = TR(ipzr, ipxr + 1) - TR(ipzr, ipxr);
+            dtx = dtx + TR(ipzr + 1, ipxr + 1) - TR(ipzr + 1, ipxr);
+            dtx = dtx / (2.0f * EARTH * dnxr);
+            dtz = TR(ipzr + 1, ipxr) - TR(ipzr, ipxr);
+            dtz = dtz + TR(ipzr + 1, ipxr + 1) - TR(ipzr, ipxr + 1);
+            dtz = dtz / (2.0f * EARTH * sin_px * dnzr);
+        } else {
+            dtx = TT(ipz, ipx + 1) - TT(ipz, ipx);
+            dtx = dtx + TT(ipz + 1, ipx + 1) - TT(ipz + 1, ipx);
+            dtx = dtx / (2.0f * EARTH * G.dnx);
+            dtz = TT(ipz + 1, ipx) - TT(ipz, ipx);
+            dtz = dtz + TT(ipz + 1, ipx + 1) - TT(ipz, ipx + 1);
+            dtz = dtz / (2.0f * EARTH * sin_px * G.dnz);
+        }
+        const float rd1 = sqrtf(sq(dtx) + sq(dtz));
+        float nx_ = px - dpl * dtx / (EARTH * rd1);
+        float nz_ = pz - dpl * dtz / (EARTH * sin_px * rd1);
+        const int ipxo = ipx, ipzo = ipz;
+        igref = in_refined(nx_, nz_, ipxr, ipzr);
+        ipx = (int)((nx_ - G.gox) / G.dnx) + 1;
+        ipz = (int)((nz_ - G.goz) / G.dnz) + 1;
+        const float sin_n = sin_f(nx_);
+        sred = sq((scx - nx_) * EARTH);
+        sred = sred + sq((scz - nz_) * EARTH * sin_n);
+        sred = sqrtf(sred);
+        sw = 0;
+        if (sred < 2.0f * dpl) sw = 1;
+        if (sw == 0 && igref == 1 && ipxr == isx && ipzr == isz) sw = 1;
+        float sin_next = sin_n;
+        if (ipx < 1) { nx_ = G.gox; ipx = 1; sin_next = sin_f(nx_); }
+        if (ipx >= G.nnx) { nx_ = G.gox + (float)(G.nnx - 1) * G.dnx; ipx = G.nnx - 1; sin_next = sin_f(nx_); }
+        if (ipz < 1) { nz_ = G.goz; ipz = 1; }
+        if (ipz >= G.nnz) { nz_ = G.goz + (float)(G.nnz - 1) * G.dnz; ipz = G.nnz - 1; }
+        // the clamped point's refined-grid flag stays as computed above (fmst.f90:616-665)
+        if (fdm) {
+            // Frechet weights of segment (px,pz) -> (nx_,nz_) (fmst.f90:734-906)
+            const int ivx = (ipx - 1) / GDX + 1, ivz = (ipz - 1) / GDZ + 1;
+            const int ivxo = (ipxo - 1) / GDX + 1, ivzo = (ipzo - 1) / GDZ + 1;
+            int nhp = 0, chp[3];
+            float vrat[3];
+            if (ivx != ivxo) {
+                nhp = nhp + 1;
+                float xi = (ivx > ivxo) ? G.gox + (float)(ivx - 1) * G.dvx : G.gox + (float)ivx * G.dvx;
+                vrat[nhp - 1] = (xi - px) / (nx_ - px);
+                chp[nhp - 1] = 1;
+            }
+            if (ivz != ivzo) {
+                nhp = nhp + 1;
+                float zi = (ivz > ivzo) ? G.goz + (float)(ivz - 1) * G.dvz : G.goz + (float)ivz * G.dvz;
+                float r = (zi - pz) / (nz_ - pz);
+                if (nhp == 1) { vrat[0] = r; chp[0] = 2; }
+                else if (r >= vrat[nhp - 2]) { vrat[nhp - 1] = r; chp[nhp - 1] = 2; }
+                else {
+                    vrat[nhp - 1] = vrat[nhp - 2];
+                    chp[nhp - 1] = chp[nhp - 2];
+                    vrat[nhp - 2] = r;
+                    chp[nhp - 2] = 2;
+                }
+            }
+            nhp = nhp + 1;
+            vrat[nhp - 1] = 1.0f;
+            chp[nhp - 1] = 0;
+            float vel = vel_at(G, in.velg, px, pz, ipxo, ipzo);
+            float vi[4], wi[4], vio[4], wio[4];
+            basis(((px - G.gox) - (float)(ivxo - 1) * G.dvx) / G.dvx, vi);
+            basis(((pz - G.goz) - (float)(ivzo - 1) * G.dvz) / G.dvz, wi);
+            int ivxt = ivxo, ivzt = ivzo;
+            for (int k = 1; k <= nhp; ++k) {
+                const float velo = vel;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) { vio[q] = vi[q]; wio[q] = wi[q]; }
+                if (k > 1) {
+                    if (chp[k - 2] == 1) ivxt = ivx;
+                    else if (chp[k - 2] == 2) ivzt = ivz;
+                }
+                const float rigz = pz + vrat[k - 1] * (nz_ - pz);
+                const float rigx = px + vrat[k - 1] * (nx_ - px);
+                const int ipxt = (int)((rigx - G.gox) / G.dnx) + 1;
+                const int ipzt = (int)((rigz - G.goz) / G.dnz) + 1;
+                vel = vel_at(G, in.velg, rigx, rigz, ipxt, ipzt);
+                basis(((rigx - G.gox) - (float)(ivxt - 1) * G.dvx) / G.dvx, vi);
+                basis(((rigz - G.goz) - (float)(ivzt - 1) * G.dvz) / G.dvz, wi);
+                const float dinc = (k == 1) ? vrat[k - 1] * dpl : (vrat[k - 1] - vrat[k - 2]) * dpl;
+                if (ivzt < 1 || ivzt > G.nvz - 1 || ivxt < 1 || ivxt > G.nvx - 1) continue;  // cannot happen
+#pragma unroll
+                for (int l = 1; l <= 4; ++l)
+#pragma unroll
+                    for (int m = 1; m <= 4; ++m) {
+                        float r1 = vi[m - 1] * wi[l - 1] / sq(vel);
+                        float r2 = vio[m - 1] * wio[l - 1] / sq(velo);
+                        r1 = -(r1 + r2) * dinc / 2.0f;
+                        float* f = fdm + (size_t)(ivxt - 2 + m) + (size_t)(ivzt - 2 + l) * G.nx;
+                        *f = r1 + *f;
+                    }
+            }
+        }
+        seg_time(px, pz, nx_, nz_);
+        px = nx_;
+        pz = nz_;
+        sin_px = sin_next;
+        if (sw == 1) {
+            seg_time(px, pz, scx, scz);
+            return tsyn;
+        }
+    }
+    *status = SWDK_FMST_RAY_UNFINISHED;
+    return __int_as_float(0x7fc00000);
+}
 
 // fmst_init (fmst.f90:27-64) on the host, REAL*4 throughout.
 inline Grid make_grid(int nx, int ny, float goxdf, float gozdf, float dvxdf, float dvzdf) {

@@ -2,8 +2,8 @@
 fmst_march_host.cpp includes jdsurfg_b200/csrc/swdk_fmst_march.cuh): its
 propagation-grid times and statuses and its receiver times must equal the
 oracle's restatement of fmst.f90 / fmm.f90 bit for bit.  This checks the
-marching logic (window solve, heap, refined grid, resampling) without a
-GPU; tests/test_gpu_fmst.py checks the device build."""
+marching logic (window solve, heap, refined grid, resampling) and the ray
+tracer without a GPU; tests/test_gpu_fmst.py checks the device build."""
 import ctypes as C
 import os
 import subprocess
@@ -118,3 +118,46 @@ def test_ties_and_grid_sides_match_oracle(mode):
             _, ft, fs, _ = _run(grid, pairs, v, field_pair=p, mode=mode)
             rt, rs = O.fmst_field(grid, v[0], float(pairs["srcx"][p]), float(pairs["srcz"][p]))
             assert np.array_equal(ft, rt) and (fs == 0).all()
+
+
+def _rays(grid, pairs, vc, vout, sine):
+    L = _lib()
+    nx, ny, goxd, gozd, dvxd, dvzd = grid
+    a32 = lambda k: np.ascontiguousarray(pairs[k], np.int32)
+    f32 = lambda k: np.ascontiguousarray(pairs[k], np.float32)
+    slot, group, rptr = a32("slot"), a32("group"), np.ascontiguousarray(pairs["rcv_ptr"], np.int64)
+    srcx, srcz, rcx, rcz = f32("srcx"), f32("srcz"), f32("rcx"), f32("rcz")
+    vc, vout = np.ascontiguousarray(vc, np.float64), np.ascontiguousarray(vout, np.float64)
+    nrcv = int(rptr[-1])
+    tt = np.zeros(nrcv, np.float32)
+    fdm = np.zeros((nrcv, ny, nx), np.float32)
+    L.fm_host_rays.restype = C.c_int
+    rc = L.fm_host_rays(sine, nx, ny, C.c_float(goxd), C.c_float(gozd), C.c_float(dvxd), C.c_float(dvzd), len(slot),
+                        _p(slot), _p(srcx), _p(srcz), _p(group), _p(rptr), _p(rcx), _p(rcz), _p(vc), _p(vout),
+                        _p(tt), _p(fdm))
+    assert rc == 0
+    return tt, fdm
+
+
+def test_gpu_ray_code_matches_oracle_up_to_the_sine():
+    """The GPU's ray tracer (srtimes, raypath with its Frechet weights and the
+    group traveltime along the ray) on the CPU: with the C library's sinf for
+    the ray points, as the reference and the oracle use, its times and
+    weights are the oracle's bit for bit; with the device's sine (double,
+    rounded) they stay within the tolerances tests/test_gpu_fmst.py states
+    for the GPU (2e-6 of a ray time, 1e-4 of a row's largest weight)."""
+    s = synth.make_survey("example", nx=14, ny=16, nstation=10, nperiod=2, seed=11)
+    slot, group = synth.survey_slots(s)
+    p = s["pairs"]
+    pairs = dict(slot=slot, srcx=p["srcx"], srcz=p["srcz"], group=group, rcv_ptr=p["rcv_ptr"], rcx=p["rcx"],
+                 rcz=p["rcz"])
+    m = O.get_2d_map(s["case"])
+    ref_t, ref_f = O.fmst_pairs(s["grid"], pairs, m["vc"], m["vout"], want_fdm=True)
+    t0, f0 = _rays(s["grid"], pairs, m["vc"], m["vout"], sine=0)
+    assert np.array_equal(t0, ref_t) and np.array_equal(f0, ref_f)
+    t1, f1 = _rays(s["grid"], pairs, m["vc"], m["vout"], sine=1)
+    grp = np.repeat(group, np.diff(p["rcv_ptr"])).astype(bool)
+    assert np.array_equal(t1[~grp], ref_t[~grp])
+    assert np.max(np.abs(t1[grp] - ref_t[grp]) / ref_t[grp]) <= 2e-6
+    scale = np.abs(ref_f).reshape(len(ref_t), -1).max(axis=1)
+    assert np.max(np.abs(f1 - ref_f).reshape(len(ref_t), -1).max(axis=1) / scale) <= 1e-4
