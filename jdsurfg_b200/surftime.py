@@ -122,6 +122,28 @@ def _delsph(a, b, c, d):
     return np.float32(np.float32(6371.0) * cc)
 
 
+def write_syn(outfile, pairs, tables, sta_dist, obst, dsyn):
+    """SurfTime::write_syn (SurfaceWave.cpp:785-815): one line per datum,
+    "dist obs syn evlat evlon stlat stlon period mode wavetype", the floats
+    in printf's %f, coordinates back to degrees as the reference converts
+    them (REAL*4 values of double expressions)."""
+    rad2deg = 180.0 / math.pi
+    T = {"Rc": tables[0], "Rg": tables[1], "Lc": tables[2], "Lg": tables[3]}
+    with open(outfile, "w") as f:
+        c = 0
+        for k, w in enumerate(pairs["wavetype"]):
+            elat = np.float32((math.pi * 0.5 - float(pairs["srcx"][k])) * rad2deg)
+            elon = np.float32(float(pairs["srcz"][k]) * rad2deg)
+            per = np.float32(T[w][pairs["period_idx"][k], pairs["mode"][k]])
+            for i in range(int(pairs["rcv_ptr"][k]), int(pairs["rcv_ptr"][k + 1])):
+                slat = np.float32((math.pi * 0.5 - float(pairs["rcx"][i])) * rad2deg)
+                slon = np.float32(float(pairs["rcz"][i]) * rad2deg)
+                f.write(f"{float(sta_dist[c]):f} {float(obst[c]):f} {float(dsyn[c]):f} ")
+                f.write(f"{float(elat):f} {float(elon):f} {float(slat):f} {float(slon):f} ")
+                f.write(f"{float(per):f} {int(pairs['mode'][k])} {w}\n")
+                c += 1
+
+
 def period_offsets(kmax_per_mode):
     """Slot offset of each (wave, mode) in get_period_index order."""
     off, base = {}, 0
@@ -273,23 +295,8 @@ class SurfTime:
         return data.cpu().numpy(), grad.astype(np.float32)
 
     def write_syn(self, dsyn, outfile):
-        """SurfaceWave.cpp:785-815."""
-        rad2deg = 180.0 / math.pi
-        p = self.pairs
-        T = {"Rc": self.tables[0], "Rg": self.tables[1], "Lc": self.tables[2], "Lg": self.tables[3]}
-        with open(outfile, "w") as f:
-            c = 0
-            for k, w in enumerate(p["wavetype"]):
-                elat = np.float32((math.pi * 0.5 - float(p["srcx"][k])) * rad2deg)
-                elon = np.float32(float(p["srcz"][k]) * rad2deg)
-                per = np.float32(T[w][p["period_idx"][k], p["mode"][k]])
-                for i in range(int(p["rcv_ptr"][k]), int(p["rcv_ptr"][k + 1])):
-                    slat = np.float32((math.pi * 0.5 - float(p["rcx"][i])) * rad2deg)
-                    slon = np.float32(float(p["rcz"][i]) * rad2deg)
-                    f.write(f"{self.sta_dist[c]:f} {self.obst[c]:f} {dsyn[c]:f} ")
-                    f.write(f"{elat:f} {elon:f} {slat:f} {slon:f} ")
-                    f.write(f"{per:f} {int(p['mode'][k])} {w}\n")
-                    c += 1
+        """SurfaceWave.cpp:785-815 (see write_syn below)."""
+        write_syn(outfile, self.pairs, self.tables, self.sta_dist, self.obst, dsyn)
 
     def close(self):
         if self.fmst is not None:

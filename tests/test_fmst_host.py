@@ -148,3 +148,26 @@ def test_read_reference_example_file():
     assert d["tables"][2] is None and d["tables"][3] is None
     assert int(p["rcv_ptr"][-1]) == len(d["obst"]) > 10 * nsrc
     assert set(p["wavetype"]) <= {"Rc", "Rg"}
+
+
+def test_write_syn_round_trip(tmp_path):
+    """write_syn (SurfaceWave.cpp:785-815) after read_swd_data: one line per
+    datum with distance, observed and synthetic times, event and station
+    coordinates back in degrees, period, mode and wave type."""
+    tR = np.array([[4.0], [6.0]])
+    srcs = [((31.5, 102.0, 0, 2, 2, 1), [(32.0, 103.0, 3.1), (30.5, 101.5, 3.05)]),
+            ((30.0, 101.0, 0, 1, 2, 0), [(31.0, 102.5, 3.4)])]
+    path = tmp_path / "surfdata.dat"
+    _write_data(path, [tR, tR.copy(), None, None], srcs)
+    d = surftime.read_swd_data(str(path))
+    dsyn = np.array([10.5, 20.25, 30.125], np.float32)
+    out = tmp_path / "syn.dat"
+    surftime.write_syn(str(out), d["pairs"], d["tables"], d["dist"], d["obst"], dsyn)
+    lines = [l.split() for l in open(out).read().splitlines()]
+    assert len(lines) == 3 and [l[-1] for l in lines] == ["Rg", "Rg", "Rc"]
+    assert [float(l[2]) for l in lines] == [10.5, 20.25, 30.125]
+    assert [float(l[7]) for l in lines] == [6.0, 6.0, 4.0] and [int(l[8]) for l in lines] == [0, 0, 0]
+    assert abs(float(lines[0][3]) - 31.5) < 1e-4 and abs(float(lines[0][4]) - 102.0) < 1e-4
+    assert abs(float(lines[1][5]) - 30.5) < 1e-4 and abs(float(lines[1][6]) - 101.5) < 1e-4
+    assert np.allclose([float(l[0]) for l in lines], d["dist"], rtol=1e-6)
+    assert np.allclose([float(l[1]) for l in lines], d["obst"], rtol=1e-6)
