@@ -48,3 +48,24 @@ def test_config_defaults_and_arg_checks():
     assert lib.swdk_config_default(None) == -1
     assert lib.swdk_create(None, None) == -1
     assert lib.swdk_kmax(None) == 0
+
+
+def test_fmst_entry_points_check_arguments_without_gpu():
+    """swdk_fmst_*: bad arguments are refused with SWDK_E_ARG before any CUDA
+    call, and creating a handle without a GPU fails instead of falling back."""
+    import torch
+    lib = _lib()
+    from jdsurfg_b200.fmst import Grid
+    vp = C.c_void_p
+    lib.swdk_fmst_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(Grid)]
+    lib.swdk_fmst_set_options.argtypes = [vp, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.swdk_fmst_pairs.argtypes = [vp, C.c_int] + [vp] * 9 + [C.c_int] + [vp] * 4
+    h = vp()
+    assert lib.swdk_fmst_create(None, 0, None) == -1
+    assert lib.swdk_fmst_create(C.byref(h), 0, C.byref(Grid(3, 10, 40.0, 100.0, 0.3, 0.3))) == -1
+    assert lib.swdk_fmst_create(C.byref(h), 0, C.byref(Grid(10, 10, 40.0, 100.0, 0.0, 0.3))) == -1
+    assert lib.swdk_fmst_set_options(None, 0, 8, 12, -1, 4) == -1
+    assert lib.swdk_fmst_pairs(None, 1, *([None] * 9), 1, None, None, None, None) == -1
+    if not torch.cuda.is_available():
+        rc = lib.swdk_fmst_create(C.byref(h), 0, C.byref(Grid(10, 12, 40.0, 100.0, 0.3, 0.3)))
+        assert rc != 0 and not h.value
