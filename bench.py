@@ -637,13 +637,8 @@ def main():
     peak = fp64_peak_tflops(torch, dev)
     flops = alg_lr * F_SEC_RAYLEIGH + alg_ll * F_SEC_LOVE
     achieved = flops / (roots_ms * 1e-3) / 1e12 if roots_ms > 0 else 0.0
-    # DRAM bytes of one root-search launch: ncu capture at 16384 columns of this
-    # workload (50.7 GB, learned proposal), scaled by the columns processed
-    traffic = 50.70e9 * ncol / 16384 if args.workload == "large" and args.proposal == "learned" else None
     roofline = {"kernel": "k_roots_queue+k_retry", "bound": "fp64", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read+write of k_roots_queue at 16384 columns, scaled by columns"
-                if traffic else None,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
                 "peak_source": "measured in this run: cuBLAS float64 GEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_layer_eval": {"rayleigh": F_SEC_RAYLEIGH, "love": F_SEC_LOVE},
                 "work": "plain-method secular evaluations x layers x flops per layer (the learned "

@@ -188,7 +188,12 @@ int swdk_frechet_csr_device(swdk_ctx* ctx, int nx, int ny, int nz, int kmax, con
  * per model); larger calls return SWDK_E_LIMIT and do nothing.  The first
  * call on each device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current, so make that first call
- * before any stream capture.  All calls on one device share the array and
+ * before any stream capture.  The address is kept for the life of the
+ * process: cudaDeviceReset on a device after its first call here is not
+ * supported (the library's module, and with it the array, is reloaded at a
+ * new address).  A CUDA error already pending on the calling thread is
+ * reported as SWDK_E_CUDA before anything is launched, and left pending for
+ * the caller.  All calls on one device share the array and
  * it keeps the last call's contents: calls whose GPU work overlaps (other
  * streams, other host threads) race and corrupt each other's results, so
  * serialise them.  The previously current device is restored on return. */

@@ -2140,6 +2140,9 @@ int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_t
   const size_t o_cstat = align256(o_croot + nroot * sizeof(double));
   const size_t need = align256(o_cstat + nroot * sizeof(int32_t));
   if (need > SWDK_NOALLOC_SCRATCH_BYTES) return SWDK_E_LIMIT;
+  // an error the caller's thread left pending is the caller's: report it
+  // without clearing it, and launch nothing
+  if (cudaPeekAtLastError() != cudaSuccess) return SWDK_E_CUDA;
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return SWDK_E_CUDA;
   if (prev != device && cudaSetDevice(device) != cudaSuccess) return SWDK_E_CUDA;
@@ -2163,13 +2166,22 @@ int swdk_surfdisp96_noalloc(int device, int nmodel, int nlayer, const float* d_t
     int32_t* cstat = (int32_t*)(base + o_cstat);
     ChainDesc cd;
     cd.t_off = 0; cd.np = kmax; cd.nmode = mode; cd.iwave = iwave; cd.igr = igr; cd.out_off = 0;
+    // each launch is checked as it is made, so the result reflects only
+    // this call's own launches
     k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_thk, d_vp, d_vs, d_rho, iflsph, layR, layL,
                                                          info);
-    k_roots_one<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(cd, nmodel, d_t, layR, layL, info, refine,
-                                                               rtol > 0.0 ? rtol : 1e-10, sngl, croot, cstat, d_ierr);
-    const int n = nmodel * kmax;
-    k_copy_last_mode<<<(n + 255) / 256, 256, 0, st>>>(nmodel, kmax, mode, croot, d_cg);
     if (cudaGetLastError() != cudaSuccess) rc = SWDK_E_CUDA;
+    if (rc == SWDK_OK) {
+      k_roots_one<<<dim3((nmodel + 127) / 128, 1), 128, 0, st>>>(cd, nmodel, d_t, layR, layL, info, refine,
+                                                                 rtol > 0.0 ? rtol : 1e-10, sngl, croot, cstat,
+                                                                 d_ierr);
+      if (cudaGetLastError() != cudaSuccess) rc = SWDK_E_CUDA;
+    }
+    if (rc == SWDK_OK) {
+      const int n = nmodel * kmax;
+      k_copy_last_mode<<<(n + 255) / 256, 256, 0, st>>>(nmodel, kmax, mode, croot, d_cg);
+      if (cudaGetLastError() != cudaSuccess) rc = SWDK_E_CUDA;
+    }
   }
   if (prev != device) cudaSetDevice(prev);
   return rc;

@@ -302,6 +302,21 @@ static int grow(swdk_fmst* f, void** p, size_t* have, size_t need) {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// makes the handle's device current for the scope of a call and restores the
+// caller's current device on every return path
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int device) {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+        else if (err == cudaSuccess) prev = -1;  // already current: nothing to restore
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 extern "C" int swdk_fmst_pairs(swdk_fmst* f, int npairs, const int32_t* slot, const float* srcx, const float* srcz,
                                const int32_t* group, const int64_t* rcv_ptr, const float* rcx, const float* rcz,
                                const double* d_vc, const double* d_vout, int kmax, float* d_ttime, float* d_fdm,
@@ -310,7 +325,8 @@ extern "C" int swdk_fmst_pairs(swdk_fmst* f, int npairs, const int32_t* slot, co
         !d_ttime || !d_status || kmax < 1)
         return SWDK_E_ARG;
     if (npairs == 0) return SWDK_OK;
-    cudaSetDevice(f->device);
+    DeviceScope dev(f->device);
+    if (dev.err != cudaSuccess) return fail(f, "cudaSetDevice", dev.err);
     cudaStream_t st = (cudaStream_t)stream;
     const Grid& G = f->G;
     const int64_t nrcv = rcv_ptr[npairs];

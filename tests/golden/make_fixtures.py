@@ -6,7 +6,8 @@
    modes) on that model and on small seeded synthetic columns, frozen so later
    changes to the oracle are caught.
 
-Run from the repository root with the reference present at /root/reference:
+Run from the repository root with the reference checkout named by the
+environment variable JDSURFG_REFERENCE (default: /root/reference):
     python tests/golden/make_fixtures.py
 """
 import os
@@ -21,7 +22,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 
 def main():
-    src = "/root/reference/test/swd/model.txt"
+    ref = os.environ.get("JDSURFG_REFERENCE", "/root/reference")
+    src = os.path.join(ref, "test", "swd", "model.txt")
     with open(src) as f:
         txt = f.read()
     with open(os.path.join(HERE, "swd_model.txt"), "w") as f:

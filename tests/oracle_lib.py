@@ -46,6 +46,20 @@ def ref_cxx():
     return _REF
 
 
+def reference_dir():
+    """The reference checkout, or None: the environment variable
+    JDSURFG_REFERENCE, else the default oracle/Makefile's recipe uses."""
+    ref = os.environ.get("JDSURFG_REFERENCE")
+    if not ref:
+        try:
+            ref = subprocess.run(["make", "-s", "-C", ORACLE_DIR, "--eval",
+                                  "print-var: ; @echo $(JDSURFG_REFERENCE)", "print-var"], check=True,
+                                 capture_output=True, text=True).stdout.strip()
+        except Exception:
+            ref = None
+    return ref if ref and os.path.isdir(ref) else None
+
+
 def load_swd_model():
     d = np.loadtxt(os.path.join(ROOT, "tests", "golden", "swd_model.txt"), skiprows=1).astype(np.float32)
     return [np.ascontiguousarray(d[:, i]) for i in range(4)]  # z, vs, vp, rho

@@ -11,7 +11,10 @@ import oracle_lib as O
 from jdsurfg_b200 import surftime, synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-EXAMPLE = "/root/reference/example/surfdataSC.dat"
+# the reference's example data file, read when a reference checkout is
+# present (JDSURFG_REFERENCE, or oracle/Makefile's default); skipped otherwise
+_REF = O.reference_dir()
+EXAMPLE = os.path.join(_REF, "example", "surfdataSC.dat") if _REF else ""
 
 
 def test_delsph_matches_reference_build():

@@ -15,12 +15,13 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle_lib as O
 from jdsurfg_b200 import Engine
 from jdsurfg_b200.engine import lib
 
 pytestmark = pytest.mark.gpu
 
-TOL_C = 1e-6  # km/s, as the other parity tests
+TOL_C = 1e-6  # km/s against the oracle, as the other parity tests
 
 
 def _models(n, L, seed):
@@ -52,23 +53,45 @@ def _noalloc(thk, vp, vs, rho, iwave, mode, t, refine=1):
     return rc, cg.cpu().numpy(), ierr.cpu().numpy()
 
 
-def test_noalloc_matches_batch_entry_point_twice():
-    # first call: Rayleigh, two modes
+def _oracle(thk, vp, vs, rho, iwave, mode, t):
+    """surfdisp96_ of every model by the CPU oracle (tight refinement, sngl output)."""
+    cg = np.zeros((thk.shape[0], len(t)))
+    ierr = np.zeros(thk.shape[0], np.int32)
+    for i in range(thk.shape[0]):
+        cg[i], ierr[i], _ = O.surfdisp96(thk[i], vp[i], vs[i], rho[i], 1, iwave, mode, 0, t, refine=1, rtol=1e-10,
+                                         sngl=1)
+    return cg, ierr
+
+
+def test_noalloc_matches_batch_entry_point_and_oracle_twice():
+    # first call: Rayleigh, two modes; one model with a NaN layer
     thk, vp, vs, rho = _models(96, 61, seed=1)
+    vs[17, 9] = np.nan
     t = np.geomspace(2.0, 50.0, 14)
     rc, cg, ierr = _noalloc(thk, vp, vs, rho, 2, 2, t)
     assert rc == 0
     ref, rerr = Engine(refine=1).surfdisp96_batch(thk, vp, vs, rho, 1, 2, 2, 0, t)
-    assert np.abs(cg - ref).max() <= TOL_C
+    # the same chain code as the batch entry point: identical results
+    np.testing.assert_array_equal(cg, ref)
     np.testing.assert_array_equal(ierr, rerr)
+    # the NaN model: ierr set, every period zero
+    assert ierr[17] == 1 and (cg[17] == 0.0).all()
+    ok = np.ones(len(thk), bool)
+    ok[17] = False
+    oc, oerr = _oracle(thk[ok], vp[ok], vs[ok], rho[ok], 2, 2, t)
+    np.testing.assert_array_equal(ierr[ok], oerr)
+    assert np.abs(cg[ok] - oc).max() <= TOL_C
     # second call in a row, different sizes and wave type: nothing stale
     thk, vp, vs, rho = _models(40, 37, seed=2)
     t = np.geomspace(3.0, 30.0, 9)
     rc, cg, ierr = _noalloc(thk, vp, vs, rho, 1, 1, t)
     assert rc == 0
     ref, rerr = Engine(refine=1).surfdisp96_batch(thk, vp, vs, rho, 1, 1, 1, 0, t)
-    assert np.abs(cg - ref).max() <= TOL_C
+    np.testing.assert_array_equal(cg, ref)
     np.testing.assert_array_equal(ierr, rerr)
+    oc, oerr = _oracle(thk, vp, vs, rho, 1, 1, t)
+    np.testing.assert_array_equal(ierr, oerr)
+    assert np.abs(cg - oc).max() <= TOL_C
 
 
 def test_noalloc_rejects_calls_beyond_its_scratch():
