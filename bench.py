@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
     ap.add_argument("--ncols", type=int, default=0, help="use only the first N columns (profiling)")
     ap.add_argument("--refine", default="tight", choices=["tight", "reference"])
+    ap.add_argument("--split-cols", type=int, default=0,
+                    help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
+    ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
@@ -474,7 +477,7 @@ def main():
         return run_fmst(args, torch, dev, rank, world, pg)
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
-    eng = Engine(device=local, refine=args.refine)
+    eng = Engine(device=local, refine=args.refine, split_cols=args.split_cols, block_roots=args.roots_blocks)
     nets = None
     from jdsurfg_b200 import learn
     eng_nets_on = [args.proposal == "learned"]  # whether the timed engine has the proposal attached
@@ -502,7 +505,7 @@ def main():
         flush.fill_(1)
         eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
 
-    roots_blocks = eng.autotune(nx, ny, nz, vs, vp, rho) if not args.no_graph else None
+    roots_blocks = eng.autotune(nx, ny, nz, vs, vp, rho) if not args.no_graph and not args.roots_blocks else None
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

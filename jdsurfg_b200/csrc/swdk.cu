@@ -24,6 +24,7 @@
 #include <mutex>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "swdk.h"
@@ -760,58 +761,52 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
                                                int sphere, double* __restrict__ vc, double* __restrict__ vout,
                                                double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
   constexpr int path = PATH;
+  constexpr bool love = WT >= 2;
+  using Layer = typename std::conditional<love, LoveLayer, RayLayer>::type;
   extern __shared__ double sm[];
   const int col = blockIdx.x;
   const ColInfo ci = info[col];
   const int L = ci.L;
-  double* drs = sm;
-  double* zd = drs + L;
-  double* za = zd + L;
-  double* zb = za + L;
-  double* zrR = zb + L;
-  double* zrL = zrR + L;
-  double* vtp = zrL + L;
-  double* rtR = vtp + L;
-  double* rtL = rtR + L;
-  float2* crs = (float2*)(rtL + L);  // nz chain-rule factors
+  Layer* lay = reinterpret_cast<Layer*>(sm);
+  float2* crs = reinterpret_cast<float2*>(lay + L);  // nz chain-rule factors
   const float4* lc = lay0 + (size_t)col * Lmax;
-  // bldsph (sregn96.f90:130-184 / slegn96.f90:107-167), ar = 6371
-  if (threadIdx.x == 0) {
-    double dr = 0.0;
-    for (int i = 0; i < L; ++i) {
-      dr = dr + ((i == L - 1) ? 1.0 : (double)lc[i].x);
-      drs[i] = dr;
-    }
-  }
   for (int i = threadIdx.x; i < nz; i += blockDim.x) crs[i] = chainrule[(size_t)i * ncol + col];
-  __syncthreads();
+  // bldsph (sregn96.f90:130-184 / slegn96.f90:107-167), ar = 6371: the layer
+  // records every slot of the column reads.  Each thread sums the
+  // thicknesses above its layers itself, in the same order as one running
+  // sum, so the depths are those of the sequential loop.
   const double ar = 6371.0;
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
     const float4 l = lc[i];
+    double zd, za, zb, zr, vtp, rt;
     if (sphere) {
-      const double r0 = (i == 0) ? ar : ar - drs[i - 1];
-      const double r1 = ar - drs[i];
+      double dr = 0.0;
+      for (int j = 0; j < i; ++j) dr = dr + (double)lc[j].x;
+      const double r0 = (i == 0) ? ar : ar - dr;
+      dr = dr + ((i == L - 1) ? 1.0 : (double)l.x);
+      const double r1 = ar - dr;
       const double z0 = ar * log(ar / r0), z1 = ar * log(ar / r1);
       const double tmp = (2.0 * ar) / (r0 + r1);
-      vtp[i] = tmp;
-      rtR[i] = pow(tmp, (double)(-2.275f));
-      const double t2 = tmp * tmp, t4 = t2 * t2, t5 = t4 * tmp;
-      rtL[i] = 1.0 / t5;
-      za[i] = (double)l.y * tmp;
-      zb[i] = (double)l.z * tmp;
-      zrR[i] = (double)l.w * rtR[i];
-      zrL[i] = (double)l.w * rtL[i];
-      zd[i] = (i == L - 1) ? 0.0 : z1 - z0;
+      vtp = tmp;
+      if (love) {
+        const double t2 = tmp * tmp, t4 = t2 * t2, t5 = t4 * tmp;
+        rt = 1.0 / t5;
+      } else {
+        rt = pow(tmp, (double)(-2.275f));
+      }
+      za = (double)l.y * tmp;
+      zb = (double)l.z * tmp;
+      zr = (double)l.w * rt;
+      zd = (i == L - 1) ? 0.0 : z1 - z0;
     } else {
-      vtp[i] = 1.0; rtR[i] = 1.0; rtL[i] = 1.0;
-      za[i] = l.y; zb[i] = l.z; zrR[i] = l.w; zrL[i] = l.w;
-      zd[i] = l.x;
+      vtp = 1.0; rt = 1.0;
+      za = l.y; zb = l.z; zr = l.w;
+      zd = l.x;
     }
+    if constexpr (love) make_love_layer(lay[i], zd, zb, zr, vtp, rt);
+    else make_ray_layer(lay[i], zd, za, zb, zr, vtp, rt);
   }
   __syncthreads();
-  EigModel MR, ML;
-  MR.zd = zd; MR.za = za; MR.zb = zb; MR.zrho = zrR; MR.vtp = vtp; MR.rtp = rtR; MR.L = L;
-  ML.zd = zd; ML.za = za; ML.zb = zb; ML.zrho = zrL; ML.vtp = vtp; ML.rtp = rtL; ML.L = L;
 
   double scr[LMAX * 6];
   double kacc[NZMAX], kp[NZMAX];
@@ -823,7 +818,6 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
   const NodeSink nosink = {nullptr, crs, L, ci.nw};
   for (int s = threadIdx.x; s < gn; s += blockDim.x) {
     const SlotDesc sd = slots[g0 + s];
-    constexpr bool love = WT >= 2;
     constexpr bool group = (WT == 1 || WT == 3);
     const double c0 = croot[(size_t)sd.r0 * ncol + col];
     int st = cstat[(size_t)sd.r0 * ncol + col];
@@ -847,7 +841,6 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
         for (int i = 0; i < nz; ++i) kernel[((size_t)sd.oslot * nz + i) * ldo + col] = 0.0;
       continue;
     }
-    const EigModel& M = love ? ML : MR;
     if constexpr (PATH == 1) {  // get_2d_map: disp1D (SurfaceWave.cpp:177-255)
       if (!group) {
         const double v = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
@@ -857,8 +850,8 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
         vc[oo] = sphere ? flat2sphere(sd.t, c0, love, 0) : c0;
         const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
         double ugr, norm;
-        if (love) love_pass(M, omega, wvno, scr, ugr, norm, nosink);
-        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, nosink);
+        if constexpr (love) love_pass(lay, L, omega, wvno, scr, ugr, norm, nosink);
+        else rayleigh_pass(lay, L, omega, wvno, scr, ugr, norm, nosink);
         double tm = 1.0;
         if (sphere) {
           const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
@@ -873,8 +866,8 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
       const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
       double ugr, norm;
       for (int i = 0; i < nz; ++i) kp[i] = 0.0;
-      if (love) love_pass(M, omega, wvno, scr, ugr, norm, sink);
-      else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, sink);
+      if constexpr (love) love_pass(lay, L, omega, wvno, scr, ugr, norm, sink);
+      else rayleigh_pass(lay, L, omega, wvno, scr, ugr, norm, sink);
       double tm = 1.0;
       if (sphere) {
         const double x = (love ? 3.0 : 1.0) * c0 / (2. * ar * omega);
@@ -896,8 +889,8 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
         const double omega = twopi / tt, wvno = omega / cc;
         double ugr, norm;
         for (int i = 0; i < nz; ++i) kp[i] = 0.0;
-        if (love) love_pass(M, omega, wvno, scr, ugr, norm, sink);
-        else rayleigh_pass(M, false, omega, wvno, scr, ugr, norm, sink);
+        if constexpr (love) love_pass(lay, L, omega, wvno, scr, ugr, norm, sink);
+        else rayleigh_pass(lay, L, omega, wvno, scr, ugr, norm, sink);
         double coef;
         if (pass == 0) {
           cg = ugr;
@@ -1382,7 +1375,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
-    const size_t smem = (size_t)9 * Lmax * sizeof(double) + (size_t)nz * sizeof(float2);
+
     using EigFn = void (*)(int, int, int, const float4*, const ColInfo*, const float2*, const SlotDesc*, int, int,
                            const double*, const int32_t*, int, double*, double*, double*, int32_t*, int);
     static const EigFn eig[4][2] = {{k_eigen<0, 0>, k_eigen<0, 1>}, {k_eigen<1, 0>, k_eigen<1, 1>},
@@ -1391,6 +1384,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       const int g0 = P.groups.start[g], gn = P.groups.count[g];
       const int wt = P.slots[g0].wtype;
       const int et = std::min(128, ((gn + 31) / 32) * 32);
+      const size_t smem = (size_t)Lmax * (wt >= 2 ? sizeof(LoveLayer) : sizeof(RayLayer)) + (size_t)nz * sizeof(float2);
       ctx->launches += 1;
       eig[wt][path]<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
                                             ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), g0, gn,

@@ -35,6 +35,12 @@
 
 namespace swdk {
 
+#ifndef __CUDACC__
+// host builds of these headers (CPU test harnesses): the device's rsqrt
+inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+using std::signbit;
+#endif
+
 // ---------------------------------------------------------------------------
 // status codes (per output slot)
 // ---------------------------------------------------------------------------

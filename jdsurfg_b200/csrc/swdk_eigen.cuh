@@ -8,6 +8,20 @@
 //           energy (447-629), splove (631-670).
 // Node kernels: SurfaceWave.cpp _ParamConvert (59-101) with the reference's
 //           4.875x half-space weight of the last node kept.
+//
+// Arithmetic layout (same mathematics as the Fortran):
+//   * everything that depends on the layer only (1/alpha^2, 1/beta^2, 1/rho,
+//     the REAL*4 rho and 2 b^2 that dnka/hska take, the sphere factors) is
+//     formed once per column in a RayLayer / LoveLayer record that every
+//     slot of the column reads (shared memory on the device);
+//   * every division by a slot constant (wvno, wvno^2, omega^2, rho omega^2)
+//     is a multiplication by its reciprocal; 1/sqrt comes from rsqrt;
+//   * per layer and sweep the vertical wavenumbers and exp(-r d) (or
+//     cos/sin(r d)) are computed once and shared by varsv, dnka / hska and
+//     the energy integrals (the Fortran evaluates them up to three times);
+//     exp(-2 r d) is exp(-r d)^2 and exp(-(p+q)) is exp(-p) exp(-q);
+//   * the energy integrals are formed without E and E^-1 (energy_lean);
+//   * the up/down vectors are normalised by exact powers of two.
 #pragma once
 #include "swdk_core.cuh"
 
@@ -17,11 +31,46 @@ constexpr int LMAX = 320;   // sublayers per column (4*80-3 = 317)
 constexpr int NZMAX = 96;   // grid nodes per column
 constexpr double LN2 = 0.69314718055994530942;
 
-// flattened eigen model of one column (bldsph), top-down index m
-struct EigModel {
-  const double *zd, *za, *zb, *zrho, *vtp, *rtp;
-  int L;
+// per-layer constants of one column's flattened Rayleigh model (bldsph of
+// sregn96.f90:130-184); rf, rf2 and gq carry the REAL*4 rounding of dnka's
+// and hska's arguments (rho, rho*rho and 2 b^2 are REAL*4 there)
+struct RayLayer {
+  double d, za, zb, zr;  // thickness, alpha, beta, rho
+  double izr, ia2, ib2;  // 1/rho, 1/alpha^2, 1/beta^2 (0 for a fluid layer)
+  double rf, irf;        // (double)(float)rho and its reciprocal
+  double rf2, irf2;      // (double)(rhof*rhof) and its reciprocal
+  double gq;             // (double)(2.0f*bf*bf)
+  double vtp, rtp;       // _ParamConvert factors of the velocity / density transform
 };
+
+// per-layer constants of one column's flattened Love model (slegn96.f90:107-167)
+struct LoveLayer {
+  double d, zb, zr, ib2;  // thickness, beta, rho, 1/beta^2 (0 for a fluid layer)
+  double mu, imu;         // rho beta^2 and its reciprocal
+  double vtp, rtp;
+};
+
+SWDK_HD void make_ray_layer(RayLayer& y, double d, double za, double zb, double zr, double vtp, double rtp) {
+  y.d = d; y.za = za; y.zb = zb; y.zr = zr;
+  y.izr = 1.0 / zr;
+  y.ia2 = 1.0 / (za * za);
+  y.ib2 = (zb > 0.0) ? 1.0 / (zb * zb) : 0.0;
+  const float rhof = (float)zr, bf = (float)zb;
+  y.rf = (double)rhof;
+  y.irf = 1.0 / y.rf;
+  y.rf2 = (double)(rhof * rhof);
+  y.irf2 = 1.0 / y.rf2;
+  y.gq = (double)(2.0f * bf * bf);
+  y.vtp = vtp; y.rtp = rtp;
+}
+
+SWDK_HD void make_love_layer(LoveLayer& y, double d, double zb, double zr, double vtp, double rtp) {
+  y.d = d; y.zb = zb; y.zr = zr;
+  y.ib2 = (zb > 0.0) ? 1.0 / (zb * zb) : 0.0;
+  y.mu = zr * zb * zb;
+  y.imu = (y.mu > 0.0) ? 1.0 / y.mu : 0.0;
+  y.vtp = vtp; y.rtp = rtp;
+}
 
 // _ParamConvert (SurfaceWave.cpp:59-101) and the empirical chain rule
 // (SurfaceWave.cpp:491-500) applied to each layer's raw kernels as the energy
@@ -37,7 +86,7 @@ struct NodeSink {
   double* kp;         // node accumulator [nz] (null: no kernels wanted)
   const float2* crs;  // (dalpha/dbeta, drho/dalpha) per node
   int L, nw;
-  SWDK_HD void add(const EigModel& M, int l, double xa, double xb, double xr) const {
+  SWDK_HD void add(int l, double fa, double fr, double xa, double xb, double xr) const {
     if (!kp) return;
     int n0, n1 = -1;
     double w0, w1 = 0.0;
@@ -53,7 +102,6 @@ struct NodeSink {
       n1 = n0 + 1;
       w1 = t;
     }
-    const double fa = M.vtp[l], fr = M.rtp[l];
     const double xbf = xb * fa, xaf = xa * fa, xrf = xr * fr;
     {
       const float2 c = crs[n0];
@@ -68,250 +116,208 @@ struct NodeSink {
   }
 };
 
-// ---------------------------------------------------------------------------
-// varsv (sregn96.f90:827-911) for the pure real / pure imaginary vertical
-// wavenumbers that cdsqrt of a real argument produces
-// ---------------------------------------------------------------------------
-struct Vars {
-  double cosp, cosq, rsinp, rsinq, sinpr, sinqr, pex, svex;
+// slot constants: wavenumber, frequency and their reciprocals
+struct SlotK {
+  double k, k2, ik, ik2, om, om2, iom2;
 };
 
-SWDK_HD void varsv_real(double x2p, double x2s, double zd, int iwat, Vars& v) {
+SWDK_HD SlotK slot_consts(double omega, double wvno) {
+  SlotK s;
+  s.k = wvno;
+  s.k2 = wvno * wvno;
+  s.ik = 1.0 / wvno;
+  s.ik2 = s.ik * s.ik;
+  s.om = omega;
+  s.om2 = omega * omega;
+  s.iom2 = 1.0 / s.om2;
+  return s;
+}
+
+// exact power-of-two exponent e with 2^(e-1) <= t < 2^e (t > 0 finite) and
+// the scale 2^-e
+SWDK_HD int pow2_norm(double t, double& scale) {
+  int e;
+  frexp(t, &e);
+  scale = ldexp(1.0, -e);
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// varsv (sregn96.f90:827-911) for the pure real / pure imaginary vertical
+// wavenumbers that cdsqrt of a real argument produces, plus what the energy
+// integrals need of the same layer: |r|, 1/|r|, and exp(-r d) (real r, cut
+// to 0 beyond r d = 75 as ffunc..h2func do) or cos/sin(|r| d) (imaginary r)
+// ---------------------------------------------------------------------------
+struct LVars {
+  double cosp, rsinp, sinpr, pex, ep, rp, irp, sp;  // P: ep = exp(-rp d) (1 if imaginary), sp = sin(|rp| d)
+  double cosq, rsinq, sinqr, svex, eq, rs, irs, sq;
+  bool preal, sreal;
+};
+
+SWDK_HD void vars_one(double x2, double d, double& cosv, double& rsinv, double& sinvr, double& ex, double& e,
+                      double& r, double& ir, double& sv, bool& real) {
   const double tiny = (double)1.0e-5f;
-  // P
-  if (x2p >= 0.0) {  // rp real
-    const double rp = sqrt(x2p), pr = rp * zd;
-    const double pfac = (pr < 30.) ? exp(-2. * pr) : 0.0;
-    v.cosp = 0.5 + pfac * 0.5;
-    const double sre = 0.5 - pfac * 0.5;
-    v.rsinp = rp * sre;
-    v.sinpr = (fabs(pr) < tiny && rp < tiny) ? zd : sre / rp;
-    v.pex = pr;
-  } else {  // rp = i r
-    const double r = sqrt(-x2p), pi = r * zd;
-    double sp, cp;
-    sincos(pi, &sp, &cp);
-    v.cosp = cp;
-    v.rsinp = -r * sp;
-    v.sinpr = (r < tiny) ? zd : sp / r;
-    v.pex = 0.0;
-  }
-  if (iwat == 1) {
-    v.cosq = 1.0; v.rsinq = 0.0; v.sinqr = 0.0; v.svex = 0.0;
-    return;
-  }
-  if (x2s >= 0.0) {
-    const double rs = sqrt(x2s), qr = rs * zd;
-    const double sfac = (qr < 30.) ? exp(-2. * qr) : 0.0;
-    v.cosq = 0.5 + sfac * 0.5;
-    const double sre = 0.5 - sfac * 0.5;
-    v.rsinq = rs * sre;
-    v.sinqr = (fabs(qr) < tiny && rs < tiny) ? zd : sre / rs;
-    v.svex = qr;
-  } else {
-    const double r = sqrt(-x2s), qi = r * zd;
-    double sq, cq;
-    sincos(qi, &sq, &cq);
-    v.cosq = cq;
-    v.rsinq = -r * sq;
-    v.sinqr = (r < tiny) ? zd : sq / r;
-    v.svex = 0.0;
+  if (x2 >= 0.0) {  // r real
+    ir = (x2 > 0.0) ? rsqrt(x2) : 0.0;
+    r = x2 * ir;
+    const double pr = r * d;
+    e = (pr < 75.0) ? exp(-pr) : 0.0;
+    const double fac = (pr < 30.0) ? e * e : 0.0;  // exp(-2 pr)
+    cosv = 0.5 + fac * 0.5;
+    const double sre = 0.5 - fac * 0.5;
+    rsinv = r * sre;
+    sinvr = (fabs(pr) < tiny && r < tiny) ? d : sre * ir;
+    ex = pr;
+    sv = 0.0;
+    real = true;
+  } else {  // r = i |r|
+    ir = rsqrt(-x2);
+    r = -x2 * ir;
+    double s, c;
+    sincos(r * d, &s, &c);
+    cosv = c;
+    rsinv = -r * s;
+    sinvr = (r < tiny) ? d : s * ir;
+    ex = 0.0;
+    e = 1.0;
+    sv = s;
+    real = false;
   }
 }
 
-// dnka of sregn96 (REAL*4 rho, b); ca[i][j] = CA(i+1,j+1)
-SWDK_HD void dnka_r(double ca[5][5], const Vars& v, float rho, float b, int iwat, double wvno, double wvno2,
-                    double om2) {
-  const double ex = v.pex, exa = v.pex + v.svex;
-  if (iwat == 1) {
-    for (int i = 0; i < 5; ++i)
-      for (int j = 0; j < 5; ++j) ca[i][j] = 0.0;
-    const double dfac = (ex > 35.0) ? 0.0 : exp(-ex);
-    ca[2][2] = dfac;
-    ca[0][0] = v.cosp;
-    ca[4][4] = v.cosp;
-    ca[0][1] = -v.rsinp / ((double)rho * om2);
-    ca[1][0] = -((double)rho * v.sinpr * om2);
-    ca[1][1] = v.cosp;
-    ca[3][3] = v.cosp;
-    ca[3][4] = ca[0][1];
-    ca[4][3] = ca[1][0];
+SWDK_HD void vars_lean(double x2p, double x2s, double d, int iwat, LVars& v) {
+  vars_one(x2p, d, v.cosp, v.rsinp, v.sinpr, v.pex, v.ep, v.rp, v.irp, v.sp, v.preal);
+  if (iwat == 1) {  // the S terms of a fluid layer (the energy integrals use only ra there)
+    v.cosq = 1.0; v.rsinq = 0.0; v.sinqr = 0.0; v.svex = 0.0; v.eq = 1.0;
+    v.rs = 0.0; v.irs = 0.0; v.sq = 0.0; v.sreal = true;
     return;
   }
-  const double a0 = (exa < 60.0) ? exp(-exa) : 0.0;
+  vars_one(x2s, d, v.cosq, v.rsinq, v.sinqr, v.svex, v.eq, v.rs, v.irs, v.sq, v.sreal);
+}
+
+// ee = cp * CA with CA the dnka matrix of sregn96 (REAL*4 rho, b; CA(i,j)
+// = c<i-1><j-1> below), formed entry by entry into the product so that the
+// 25 entries are never all held at once
+SWDK_HD void dnka_apply(const LVars& v, const RayLayer& y, int iwat, const SlotK& s, const double* cp, double* ee) {
+  const double irom2 = y.irf * s.iom2, rom2 = y.rf * s.om2;
+  if (iwat == 1) {  // fluid: CA = diag(cosp, ., dfac, ., cosp) with the (1,2)/(2,1) and (4,5)/(5,4) pairs
+    const double dfac = (v.pex > 35.0) ? 0.0 : v.ep;  // exp(-ex)
+    const double c01 = -v.rsinp * irom2, c10 = -(y.rf * v.sinpr * s.om2);
+    ee[0] = cp[0] * v.cosp + cp[1] * c10;
+    ee[1] = cp[0] * c01 + cp[1] * v.cosp;
+    ee[2] = cp[2] * dfac;
+    ee[3] = cp[3] * v.cosp + cp[4] * c10;
+    ee[4] = cp[3] * c01 + cp[4] * v.cosp;
+    return;
+  }
+  const double exa = v.pex + v.svex;
+  const double a0 = (exa < 60.0) ? v.ep * v.eq : 0.0;  // exp(-exa)
   const double cosp = v.cosp, cossv = v.cosq, rsinp = v.rsinp, rsinsv = v.rsinq, sinpr = v.sinpr,
                sinsvr = v.sinqr;
+  const double k = s.k, k2 = s.k2, ik = s.ik, ik2 = s.ik2;
   const double cpcq = cosp * cossv, cpy = cosp * sinsvr, cpz = cosp * rsinsv, cqw = cossv * sinpr,
                cqx = cossv * rsinp;
   const double xy = rsinp * sinsvr, xz = rsinp * rsinsv, wy = sinpr * sinsvr, wz = sinpr * rsinsv;
-  const float rho2 = rho * rho;
-  const double gam = (double)(2.0f * b * b) * wvno2 / om2;
+  const double gam = y.gq * k2 * s.iom2;
   const double gam2 = gam * gam, gamm1 = gam - 1., gamm2 = gamm1 * gamm1;
-  const double cqww2 = cqw * wvno2, cqxw2 = cqx / wvno2, gg1 = gam * gamm1;
+  const double cqww2 = cqw * k2, cqxw2 = cqx * ik2, gg1 = gam * gamm1;
   const double a0c = 2.0 * (a0 - cpcq);
-  const double xz2 = xz / wvno2, gxz2 = gam * xz2, g2xz2 = gam2 * xz2;
+  const double xz2 = xz * ik2, gxz2 = gam * xz2, g2xz2 = gam2 * xz2;
   const double a0cgg1 = a0c * (gam + gamm1);
-  const double wy2 = wy * wvno2, g2wy2 = gamm2 * wy2, g1wy2 = gamm1 * wy2;
-  const double rhod = (double)rho, rho2d = (double)rho2;
-  const double rom2 = rhod * om2;
-  double temp = a0c * gg1 + g2xz2 + g2wy2;
-  ca[2][2] = a0 + temp + temp;
-  ca[0][0] = cpcq - temp;
-  ca[0][1] = (-cqx + wvno2 * cpy) / rom2;
-  temp = 0.5 * a0cgg1 + gxz2 + g1wy2;
-  ca[0][2] = wvno * temp / rom2;
-  ca[0][3] = (-cqww2 + cpz) / rom2;
-  temp = wvno2 * (a0c + wy2) + xz;
-  ca[0][4] = -temp / (rho2d * om2 * om2);
-  ca[1][0] = (-gamm2 * cqw + gam2 * cpz / wvno2) * rhod * om2;
-  ca[1][1] = cpcq;
-  ca[1][2] = (gamm1 * cqww2 - gam * cpz) / wvno;
-  ca[1][3] = -wz;
-  ca[1][4] = ca[0][3];
-  temp = 0.5 * a0cgg1 * gg1 + gam2 * gxz2 + gamm2 * g1wy2;
-  ca[2][0] = -2.0 * temp * rhod * om2 / wvno;
-  ca[2][1] = (-wvno * (gam * cqxw2 - gamm1 * cpy)) * 2.0;
-  ca[2][3] = -2.0 * ca[1][2];
-  ca[2][4] = -2.0 * ca[0][2];
-  ca[3][0] = (-gam2 * cqxw2 + gamm2 * cpy) * rhod * om2;
-  ca[3][1] = -xy;
-  ca[3][2] = -ca[2][1] / 2.0;
-  ca[3][3] = ca[1][1];
-  ca[3][4] = ca[0][1];
-  temp = gamm2 * (a0c * gam2 + g2wy2) + gam2 * g2xz2;
-  ca[4][0] = -rho2d * om2 * om2 * temp / wvno2;
-  ca[4][1] = ca[3][0];
-  ca[4][2] = -ca[2][0] / 2.0;
-  ca[4][3] = ca[1][0];
-  ca[4][4] = ca[0][0];
+  const double wy2 = wy * k2, g2wy2 = gamm2 * wy2, g1wy2 = gamm1 * wy2;
+  const double t1 = a0c * gg1 + g2xz2 + g2wy2;
+  const double c00 = cpcq - t1;
+  const double c22 = a0 + t1 + t1;
+  const double c01 = (-cqx + k2 * cpy) * irom2;
+  const double c02 = k * (0.5 * a0cgg1 + gxz2 + g1wy2) * irom2;
+  const double c03 = (-cqww2 + cpz) * irom2;
+  const double c04 = -(k2 * (a0c + wy2) + xz) * (y.irf2 * s.iom2 * s.iom2);
+  const double c10 = (-gamm2 * cqw + gam2 * cpz * ik2) * rom2;
+  const double c11 = cpcq;
+  const double c12 = (gamm1 * cqww2 - gam * cpz) * ik;
+  const double c13 = -wz;
+  const double c20 = -2.0 * (0.5 * a0cgg1 * gg1 + gam2 * gxz2 + gamm2 * g1wy2) * rom2 * ik;
+  const double c21 = (-k * (gam * cqxw2 - gamm1 * cpy)) * 2.0;
+  const double c30 = (-gam2 * cqxw2 + gamm2 * cpy) * rom2;
+  const double c31 = -xy;
+  const double c40 = -(y.rf2 * s.om2 * s.om2) * (gamm2 * (a0c * gam2 + g2wy2) + gam2 * g2xz2) * ik2;
+  // rows 2..5 repeat entries: c14 = c03, c23 = -2 c12, c24 = -2 c02,
+  // c32 = -c21/2, c33 = c11, c34 = c01, c41 = c30, c42 = -c20/2, c43 = c10, c44 = c00
+  const double p0 = cp[0], p1 = cp[1], p2 = cp[2], p3 = cp[3], p4 = cp[4];
+  ee[0] = p0 * c00 + p1 * c10 + p2 * c20 + p3 * c30 + p4 * c40;
+  ee[1] = p0 * c01 + p1 * c11 + p2 * c21 + p3 * c31 + p4 * c30;
+  ee[2] = p0 * c02 + p1 * c12 + p2 * c22 + p3 * (-c21 * 0.5) + p4 * (-c20 * 0.5);
+  ee[3] = p0 * c03 + p1 * c13 + p2 * (-2.0 * c12) + p3 * c11 + p4 * c10;
+  ee[4] = p0 * c04 + p1 * c03 + p2 * (-2.0 * c02) + p3 * c01 + p4 * c00;
 }
 
-// hska (sregn96.f90:913-987)
-SWDK_HD void hska_r(double AA[4][4], const Vars& v, float rho, float b, int iwat, double wvno, double wvno2,
-                    double om2) {
-  const double rhod = (double)rho;
+// a0 = AA * vv with AA the hska matrix (sregn96.f90:913-987), formed entry
+// by entry into the product
+SWDK_HD void hska_apply(const LVars& v, const RayLayer& y, int iwat, const SlotK& s, const double* vv, double* a0) {
+  const double irom2 = y.irf * s.iom2, rom2 = y.rf * s.om2;
   if (iwat == 1) {
-    for (int i = 0; i < 4; ++i)
-      for (int j = 0; j < 4; ++j) AA[i][j] = 0.0;
-    const double dfac = (v.pex > 35.0) ? 0.0 : exp(-v.pex);
-    AA[0][0] = dfac;
-    AA[3][3] = dfac;
-    AA[1][1] = v.cosp;
-    AA[2][2] = v.cosp;
-    AA[1][2] = -v.rsinp / (rhod * om2);
-    AA[2][1] = -(rhod * om2 * v.sinpr);
+    const double dfac = (v.pex > 35.0) ? 0.0 : v.ep;
+    const double a12 = -v.rsinp * irom2, a21 = -(rom2 * v.sinpr);
+    a0[0] = dfac * vv[0];
+    a0[1] = v.cosp * vv[1] + a12 * vv[2];
+    a0[2] = a21 * vv[1] + v.cosp * vv[2];
+    a0[3] = dfac * vv[3];
     return;
   }
-  const double dfac = ((v.pex - v.svex) > 70.0) ? 0.0 : exp(v.svex - v.pex);
+  // exp(svex - pex), 0 when pex - svex > 70; exp(-pex) / exp(-svex) while
+  // both factors are held (below 75)
+  double dfac;
+  if ((v.pex - v.svex) > 70.0) dfac = 0.0;
+  else if (v.pex < 75.0 && v.svex < 75.0) dfac = v.ep * recip(v.eq);
+  else dfac = exp(v.svex - v.pex);
   const double cossv = dfac * v.cosq, rsinsv = dfac * v.rsinq, sinsvr = dfac * v.sinqr;
   const double cosp = v.cosp, rsinp = v.rsinp, sinpr = v.sinpr;
-  const double gam = (double)(2.0f * b * b) * wvno2 / om2;
+  const double k = s.k, k2 = s.k2, ik = s.ik, ik2 = s.ik2;
+  const double gam = y.gq * k2 * s.iom2;
   const double gamm1 = gam - 1.0;
-  const double rom2 = rhod * om2;
-  AA[0][0] = cossv + gam * (cosp - cossv);
-  AA[0][1] = -wvno * gamm1 * sinpr + gam * rsinsv / wvno;
-  AA[0][2] = -(wvno * (cosp - cossv) / rom2);
-  AA[0][3] = (wvno2 * sinpr - rsinsv) / rom2;
-  AA[1][0] = gam * rsinp / wvno - wvno * gamm1 * sinsvr;
-  AA[1][1] = cosp - gam * (cosp - cossv);
-  AA[1][2] = (-rsinp + wvno2 * sinsvr) / rom2;
-  AA[1][3] = -AA[0][2];
-  AA[2][0] = rom2 * gam * gamm1 * (cosp - cossv) / wvno;
-  AA[2][1] = rom2 * (-gamm1 * gamm1 * sinpr + gam * gam * rsinsv / wvno2);
-  AA[2][2] = AA[1][1];
-  AA[2][3] = -AA[0][1];
-  AA[3][0] = rom2 * (gam * gam * rsinp / wvno2 - gamm1 * gamm1 * sinsvr);
-  AA[3][1] = -AA[2][0];
-  AA[3][2] = -AA[1][0];
-  AA[3][3] = AA[0][0];
+  const double dc = cosp - cossv;
+  const double A00 = cossv + gam * dc;
+  const double A01 = -k * gamm1 * sinpr + gam * rsinsv * ik;
+  const double A02 = -(k * dc * irom2);
+  const double A03 = (k2 * sinpr - rsinsv) * irom2;
+  const double A10 = gam * rsinp * ik - k * gamm1 * sinsvr;
+  const double A11 = cosp - gam * dc;
+  const double A12 = (-rsinp + k2 * sinsvr) * irom2;
+  const double A20 = rom2 * gam * gamm1 * dc * ik;
+  const double A21 = rom2 * (-gamm1 * gamm1 * sinpr + gam * gam * rsinsv * ik2);
+  const double A30 = rom2 * (gam * gam * rsinp * ik2 - gamm1 * gamm1 * sinsvr);
+  // AA(2,4) = -AA(1,3), AA(3,3) = AA(2,2), AA(3,4) = -AA(1,2),
+  // AA(4,2) = -AA(3,1), AA(4,3) = -AA(2,1), AA(4,4) = AA(1,1)
+  const double v0 = vv[0], v1 = vv[1], v2 = vv[2], v3 = vv[3];
+  a0[0] = A00 * v0 + A01 * v1 + A02 * v2 + A03 * v3;
+  a0[1] = A10 * v0 + A11 * v1 + A12 * v2 + (-A02) * v3;
+  a0[2] = A20 * v0 + A21 * v1 + A11 * v2 + (-A01) * v3;
+  a0[3] = A30 * v0 + (-A20) * v1 + (-A10) * v2 + A00 * v3;
 }
 
-// evalg with jbdry = 0 (sregn96.f90:649-825); solid or fluid layer m
-struct EMat {
-  cx ra, rb;
-  cx e[4][4], ei[4][4];
-};
-
-SWDK_HD void evalg_r(const EigModel& M, int m, int iwat, bool allfluid, double wvno, double om, double om2,
-                     double wvno2, EMat& E, cx* gbr) {
-  const double xka = om / M.za[m];
-  const double xkb = (M.zb[m] > 0.0) ? om / M.zb[m] : 0.0;
-  E.ra = csqrt_real(wvno2 - xka * xka);
-  E.rb = csqrt_real(wvno2 - xkb * xkb);
-  double gam = M.zb[m] * wvno / om;
+// half-space start vector of the up pass: evalg's gbr (sregn96.f90:736-760,
+// 774-790) for the bottom layer, once per pass
+SWDK_HD void halfspace_gbr(const RayLayer& y, int iwat, const SlotK& s, double g[5]) {
+  const cx ra = csqrt_real(s.k2 - s.om2 * y.ia2), rb = csqrt_real(s.k2 - s.om2 * y.ib2);
+  const double zr = y.zr, om2 = s.om2, wvno = s.k, wvno2 = s.k2;
+  double gam = y.zb * wvno / s.om;
   gam = 2.0 * (gam * gam);
   const double gamm1 = gam - 1.0;
-  const cx ra = E.ra, rb = E.rb;
-  const double zr = M.zrho[m];
+  cx gbr[5];
   if (iwat == 0) {
-    const double g1 = zr * om2 * gamm1, g2 = zr * om2 * gam;
-    E.e[0][0] = mkc(wvno); E.e[0][1] = rb; E.e[0][2] = mkc(wvno); E.e[0][3] = -rb;
-    E.e[1][0] = ra; E.e[1][1] = mkc(wvno); E.e[1][2] = -ra; E.e[1][3] = mkc(wvno);
-    E.e[2][0] = mkc(g1); E.e[2][1] = g2 * rb / wvno; E.e[2][2] = mkc(g1); E.e[2][3] = -(g2 * rb / wvno);
-    E.e[3][0] = g2 * ra / wvno; E.e[3][1] = mkc(g1); E.e[3][2] = -(g2 * ra / wvno); E.e[3][3] = mkc(g1);
-    const double h1 = 0.5 * gam / wvno, h2 = -(0.5 / (zr * om2));
-    const cx iga = (0.5 * gamm1) / ra, igb = (0.5 * gamm1) / rb;
-    const cx wa = (0.5 * wvno) / ((zr * om2) * ra), wb = (0.5 * wvno) / ((zr * om2) * rb);
-    E.ei[0][0] = mkc(h1); E.ei[0][1] = -iga; E.ei[0][2] = mkc(h2); E.ei[0][3] = wa;
-    E.ei[1][0] = -igb; E.ei[1][1] = mkc(h1); E.ei[1][2] = wb; E.ei[1][3] = mkc(h2);
-    E.ei[2][0] = mkc(h1); E.ei[2][1] = iga; E.ei[2][2] = mkc(h2); E.ei[2][3] = -wa;
-    E.ei[3][0] = igb; E.ei[3][1] = mkc(h1); E.ei[3][2] = -wb; E.ei[3][3] = mkc(h2);
-    if (gbr) {
-      gbr[0] = (zr * zr * om2 * om2) * (-((gam * gam) * ra * rb) + wvno2 * gamm1 * gamm1);
-      gbr[1] = -((zr * (wvno2 * ra)) * om2);
-      gbr[2] = -(((zr * (-((gam * ra) * rb) + wvno2 * gamm1)) * om2) * wvno);
-      gbr[3] = (zr * (wvno2 * rb)) * om2;
-      gbr[4] = wvno2 * (wvno2 - ra * rb);
-      const cx den = -((zr * zr * om2 * om2 * wvno2) * ra * rb);
-      for (int i = 0; i < 5; ++i) gbr[i] = (0.25 * gbr[i]) / den;
-    }
-  } else {
-    if (gbr) {
-      if (allfluid) {
-        gbr[0] = 0.5 / ra;
-        gbr[1] = mkc(0.5) / mkc(-(zr * om2));
-        gbr[2] = mkc(0); gbr[3] = mkc(0); gbr[4] = mkc(0);
-      } else {
-        gbr[0] = mkc(0); gbr[1] = mkc(0); gbr[2] = mkc(0);
-        gbr[3] = (0.5 * zr * om2) / ra;
-        gbr[4] = mkc(-0.5);
-      }
-    }
-    for (int i = 0; i < 4; ++i)
-      for (int j = 0; j < 4; ++j) { E.e[i][j] = mkc(0); E.ei[i][j] = mkc(0); }
-    E.e[0][0] = ra; E.e[0][1] = -ra;
-    E.e[1][0] = mkc(-(zr * om2)); E.e[1][1] = mkc(-(zr * om2));
-    E.ei[0][0] = 0.5 / ra;
-    E.ei[0][1] = mkc(-(0.5 / (zr * om2)));
-    E.ei[1][0] = -(0.5 / ra);
-    E.ei[1][1] = mkc(-(0.5 / (zr * om2)));
+    gbr[0] = (zr * zr * om2 * om2) * (-((gam * gam) * ra * rb) + wvno2 * gamm1 * gamm1);
+    gbr[1] = -((zr * (wvno2 * ra)) * om2);
+    gbr[2] = -(((zr * (-((gam * ra) * rb) + wvno2 * gamm1)) * om2) * wvno);
+    gbr[3] = (zr * (wvno2 * rb)) * om2;
+    gbr[4] = wvno2 * (wvno2 - ra * rb);
+    const cx den = -((zr * zr * om2 * om2 * wvno2) * ra * rb);
+    for (int i = 0; i < 5; ++i) gbr[i] = (0.25 * gbr[i]) / den;
+  } else {  // a fluid half-space under the column (jbdry = 0)
+    gbr[0] = mkc(0); gbr[1] = mkc(0); gbr[2] = mkc(0);
+    gbr[3] = (0.5 * zr * om2) / ra;
+    gbr[4] = mkc(-0.5);
   }
-}
-
-SWDK_HD cx ffunc_c(cx nub, double dm) {
-  if (cabsc(nub) < 1.0e-08) return mkc(dm);
-  const cx argcd = nub * dm;
-  const cx exqq = (argcd.re < 40.0) ? cexpc(-2.0 * argcd) : mkc(0.0);
-  return (1.0 - exqq) / (2.0 * nub);
-}
-SWDK_HD cx gfunc_c(cx nub, double dm) {
-  const cx argcd = nub * dm;
-  if (argcd.re < 75) return cexpc(-argcd) * dm;
-  return mkc(0.0);
-}
-SWDK_HD cx h1func_c(cx nua, cx nub, double dm) {
-  if (cabsc(nub + nua) < 1.0e-08) return mkc(dm);
-  const cx argcd = (nua + nub) * dm;
-  const cx exqq = (argcd.re < 40.0) ? cexpc(-argcd) : mkc(0.0);
-  return (1.0 - exqq) / (nub + nua);
-}
-SWDK_HD cx h2func_c(cx nua, cx nub, double dm) {
-  if (cabsc(nub - nua) < 1.0e-08) return mkc(dm);
-  cx argcd = nua * dm;
-  const cx exqp = (argcd.re < 40.0) ? cexpc(-argcd) : mkc(0.0);
-  argcd = nub * dm;
-  const cx exqq = (argcd.re < 40.0) ? cexpc(-argcd) : mkc(0.0);
-  return (exqq - exqp) / (nua - nub);
+  for (int i = 0; i < 5; ++i) g[i] = gbr[i].re;
 }
 
 // Eigenfunction values at a layer top: (ur, uz, tz, tr)
@@ -319,12 +325,30 @@ struct Eig4 {
   double ur, uz, tz, tr;
 };
 
-
 struct EnergyAcc {
   double sumi0, sumi1, sumi2, sumi3;
 };
 
-// energy() body for one layer m (sregn96.f90:1097-1178); writes the raw
+SWDK_HD double re_mul(cx a, cx b) { return a.re * b.re - a.im * b.im; }
+// 1/z of a general complex z: conj(z) / |z|^2
+SWDK_HD cx cinv_any(cx z) {
+  const double s = recip(z.re * z.re + z.im * z.im);
+  return mkc(z.re * s, -z.im * s);
+}
+// a vertical wavenumber (pure real or pure imaginary) from its magnitude,
+// and its reciprocal from the magnitude's reciprocal
+SWDK_HD cx rval(bool real, double r) { return real ? mkc(r, 0.0) : mkc(0.0, r); }
+SWDK_HD cx rinv(bool real, double ir) { return real ? mkc(ir, 0.0) : mkc(0.0, -ir); }
+// exp(-r d): real r -> e, imaginary r -> cos - i sin
+SWDK_HD cx rexp(bool real, double e, double c, double s) { return real ? mkc(e, 0.0) : mkc(c, -s); }
+// ffunc (sregn96.f90:1319-1335), (1 - exp(-2 r d)) / (2 r) for |r| >= 1e-8:
+// real r with e = exp(-r d) (0 when r d >= 40); imaginary r from cos, sin
+SWDK_HD cx ffun(bool real, double ir, double e, double c, double s) {
+  if (real) return mkc((1.0 - e * e) * 0.5 * ir, 0.0);
+  return mkc(s * c * ir, -s * s * ir);
+}
+
+// energy() body for one layer (sregn96.f90:1097-1178); writes the raw
 // (un-normalised) dcda, dcdb, dcdr of the layer.
 //
 // intijr (sregn96.f90:1198-1317) is evaluated without forming E and E^-1:
@@ -339,127 +363,108 @@ struct EnergyAcc {
 //     SX_s = H1 (kmpu kmsu - km1pd km1sd) + s H2 (km1pd kmsu - kmpu km1sd)
 //   half-space:     cint = P km1pd^2/(2ra) - X km1pd km1sd/(ra+rb) + Q km1sd^2/(2rb)
 // and the potentials are rows of E^-1 applied to (ur, uz, tz, tr).
-// exp(-2 ra d), exp(-(ra+rb) d) are products of exp(-ra d), exp(-rb d).
-SWDK_HD double re_mul(cx a, cx b) { return a.re * b.re - a.im * b.im; }
-SWDK_HD cx cinv(cx a) {  // 1/a for pure real or pure imaginary a
-  if (a.im == 0.0) return mkc(1.0 / a.re, 0.0);
-  if (a.re == 0.0) return mkc(0.0, -1.0 / a.im);
-  return mkc(1.0) / a;
-}
-
-SWDK_HD void energy_layer_r(const EigModel& M, int m, int iwat, bool allfluid, const Eig4& u0, const Eig4& u1,
-                            double om, double om2, double wvno, double wvno2, double c, EnergyAcc& acc,
-                            double& dcda, double& dcdb, double& dcdr) {
-  (void)allfluid;
-  const int typelyr = (m == M.L - 1) ? 1 : 0;
-  const double za = M.za[m], zb = M.zb[m], zr = M.zrho[m], zdm = M.zd[m];
-  const double xka = om / za;
-  const double xkb = (zb > 0.0) ? om / zb : 0.0;
-  const double ra2 = wvno2 - xka * xka, rb2 = wvno2 - xkb * xkb;
-  const cx ra = csqrt_real(ra2), rb = csqrt_real(rb2);
-  double gam = zb * wvno / om;
-  gam = 2.0 * (gam * gam);
+SWDK_HD void energy_lean(const RayLayer& y, const LVars& v, int iwat, bool half, const Eig4& u0, const Eig4& u1,
+                         const SlotK& s, double c, EnergyAcc& acc, double& dcda, double& dcdb, double& dcdr) {
+  const double za = y.za, zb = y.zb, zr = y.zr, zdm = y.d;
+  const double k = s.k, k2 = s.k2, ik = s.ik, ik2 = s.ik2;
+  const double ra2 = k2 - s.om2 * y.ia2, rb2 = k2 - s.om2 * y.ib2;
+  const cx ra = rval(v.preal, v.rp), ira = rinv(v.preal, v.irp);
+  const double gam = 2.0 * (zb * zb * k2 * s.iom2);  // 2 (zb wvno / om)^2
   const double gamm1 = gam - 1.0;
-  const double rom2 = zr * om2;
+  const double rom2 = zr * s.om2, irom2 = y.izr * s.iom2;
   double INT11, INT13 = 0.0, INT22, INT24 = 0.0, INT33 = 0.0, INT44 = 0.0;
-  // exp(-ra d), exp(-rb d) with the reference's cut-offs applied by the users
-  auto cexp_neg = [](cx r, double d) { return cexpc(mkc(-r.re * d, -r.im * d)); };
   if (iwat == 0) {
-    const double g1 = rom2 * gamm1, g2 = rom2 * gam / wvno;
-    const double h1 = 0.5 * gam / wvno, h2 = -(0.5 / rom2), ga = 0.5 * gamm1, wa = 0.5 * wvno / rom2;
-    const cx ira = cinv(ra), irb = cinv(rb);
+    const cx rb = rval(v.sreal, v.rs), irb = rinv(v.sreal, v.irs);
+    const double g1 = rom2 * gamm1, g2 = rom2 * gam * ik;
+    const double h1 = 0.5 * gam * ik, h2 = -(0.5 * irom2), ga = 0.5 * gamm1, wa = 0.5 * k * irom2;
     const cx km1pd = (h1 * u0.ur + h2 * u0.tz) + (ga * u0.uz - wa * u0.tr) * ira;
     const cx km1sd = (ga * u0.ur - wa * u0.tz) * irb + (h1 * u0.uz + h2 * u0.tr);
-    const double k = wvno, k2 = wvno2;
-    // pair coefficients: P (real), Q (real), X = xr * r (r = ra or rb)
-    if (typelyr == 0) {
+    if (!half) {
       const cx kmpu = (h1 * u1.ur + h2 * u1.tz) - (ga * u1.uz - wa * u1.tr) * ira;
       const cx kmsu = (h1 * u1.uz + h2 * u1.tr) - (ga * u1.ur - wa * u1.tz) * irb;
       // FA, GA, FB, GB, H1, H2 (sregn96.f90:1319-1397)
-      const cx ard = ra * zdm, brd = rb * zdm;
-      const cx ea = (ard.re < 75.0) ? cexp_neg(ra, zdm) : mkc(0.0);
-      const cx eb = (brd.re < 75.0) ? cexp_neg(rb, zdm) : mkc(0.0);
-      const cx ea40 = (ard.re < 40.0) ? ea : mkc(0.0);
-      const cx eb40 = (brd.re < 40.0) ? eb : mkc(0.0);
-      const cx FA = (cabsc(ra) < 1.0e-08) ? mkc(zdm) : (1.0 - ea40 * ea40) / (2.0 * ra);
-      const cx FB = (cabsc(rb) < 1.0e-08) ? mkc(zdm) : (1.0 - eb40 * eb40) / (2.0 * rb);
+      const double ard = v.preal ? v.rp * zdm : 0.0, brd = v.sreal ? v.rs * zdm : 0.0;
+      const cx ea = rexp(v.preal, v.ep, v.cosp, v.sp), eb = rexp(v.sreal, v.eq, v.cosq, v.sq);
+      const cx ea40 = (ard < 40.0) ? ea : mkc(0.0), eb40 = (brd < 40.0) ? eb : mkc(0.0);
+      const cx FA = (v.rp < 1.0e-08) ? mkc(zdm) : ffun(v.preal, v.irp, ea40.re, v.cosp, v.sp);
+      const cx FB = (v.rs < 1.0e-08) ? mkc(zdm) : ffun(v.sreal, v.irs, eb40.re, v.cosq, v.sq);
       const cx GA = ea * zdm, GB = eb * zdm;
       const cx sab = ra + rb;
       const cx H1 = (cabsc(sab) < 1.0e-08) ? mkc(zdm)
-                    : (1.0 - ((((ard + brd).re) < 40.0) ? ea * eb : mkc(0.0))) / sab;
+                    : (1.0 - ((ard + brd < 40.0) ? ea * eb : mkc(0.0))) * cinv_any(sab);
       const cx dab = ra - rb;
-      const cx H2 = (cabsc(dab) < 1.0e-08) ? mkc(zdm) : (eb40 - ea40) / dab;
+      const cx H2 = (cabsc(dab) < 1.0e-08) ? mkc(zdm) : (eb40 - ea40) * cinv_any(dab);
       const cx pp = kmpu * kmpu + km1pd * km1pd, ss = kmsu * kmsu + km1sd * km1sd;
       const cx pd = kmpu * km1pd, sd = kmsu * km1sd;
       const cx x1 = kmpu * kmsu - km1pd * km1sd, x2 = km1pd * kmsu - kmpu * km1sd;
-      const cx FApp = FA * pp, GApd2 = 2.0 * (GA * pd), FBss = FB * ss, GBsd2 = 2.0 * (GB * sd);
+      const double FApp = re_mul(FA, pp), GApd2 = 2.0 * re_mul(GA, pd), FBss = re_mul(FB, ss),
+                   GBsd2 = 2.0 * re_mul(GB, sd);
       const cx H1x = H1 * x1, H2x = H2 * x2;
-      const cx SAp = FApp + GApd2, SAm = FApp - GApd2;
-      const cx SBp = FBss - GBsd2, SBm = FBss + GBsd2;
-      const cx SXp = H1x + H2x, SXm = H1x - H2x;
-      INT11 = k2 * SAp.re + rb2 * SBp.re + 2.0 * k * re_mul(rb, SXp);
-      INT13 = k * g1 * SAp.re + g2 * rb2 * SBp.re + (k * g2 + g1) * re_mul(rb, SXp);
-      INT33 = g1 * g1 * SAp.re + g2 * g2 * rb2 * SBp.re + 2.0 * g1 * g2 * re_mul(rb, SXp);
-      INT22 = ra2 * SAm.re + k2 * SBm.re + 2.0 * k * re_mul(ra, SXm);
-      INT24 = g2 * ra2 * SAm.re + k * g1 * SBm.re + (g1 + k * g2) * re_mul(ra, SXm);
-      INT44 = g2 * g2 * ra2 * SAm.re + g1 * g1 * SBm.re + 2.0 * g1 * g2 * re_mul(ra, SXm);
+      const double SAp = FApp + GApd2, SAm = FApp - GApd2;
+      const double SBp = FBss - GBsd2, SBm = FBss + GBsd2;
+      const double Xp = re_mul(rb, H1x + H2x), Xm = re_mul(ra, H1x - H2x);
+      INT11 = k2 * SAp + rb2 * SBp + 2.0 * k * Xp;
+      INT13 = k * g1 * SAp + g2 * rb2 * SBp + (k * g2 + g1) * Xp;
+      INT33 = g1 * g1 * SAp + g2 * g2 * rb2 * SBp + 2.0 * g1 * g2 * Xp;
+      INT22 = ra2 * SAm + k2 * SBm + 2.0 * k * Xm;
+      INT24 = g2 * ra2 * SAm + k * g1 * SBm + (g1 + k * g2) * Xm;
+      INT44 = g2 * g2 * ra2 * SAm + g1 * g1 * SBm + 2.0 * g1 * g2 * Xm;
     } else {
-      const cx TA = (km1pd * km1pd) / (2.0 * ra), TB = (km1sd * km1sd) / (2.0 * rb);
-      const cx TX = -((km1pd * km1sd) / (ra + rb));
-      INT11 = k2 * TA.re + rb2 * TB.re + 2.0 * k * re_mul(rb, TX);
-      INT13 = k * g1 * TA.re + g2 * rb2 * TB.re + (k * g2 + g1) * re_mul(rb, TX);
-      INT33 = g1 * g1 * TA.re + g2 * g2 * rb2 * TB.re + 2.0 * g1 * g2 * re_mul(rb, TX);
-      INT22 = ra2 * TA.re + k2 * TB.re + 2.0 * k * re_mul(ra, TX);
-      INT24 = g2 * ra2 * TA.re + k * g1 * TB.re + (g1 + k * g2) * re_mul(ra, TX);
-      INT44 = g2 * g2 * ra2 * TA.re + g1 * g1 * TB.re + 2.0 * g1 * g2 * re_mul(ra, TX);
+      const double TA = re_mul(km1pd * km1pd, 0.5 * ira), TB = re_mul(km1sd * km1sd, 0.5 * irb);
+      const cx TX = -((km1pd * km1sd) * cinv_any(ra + rb));
+      const double Xb = re_mul(rb, TX), Xa = re_mul(ra, TX);
+      INT11 = k2 * TA + rb2 * TB + 2.0 * k * Xb;
+      INT13 = k * g1 * TA + g2 * rb2 * TB + (k * g2 + g1) * Xb;
+      INT33 = g1 * g1 * TA + g2 * g2 * rb2 * TB + 2.0 * g1 * g2 * Xb;
+      INT22 = ra2 * TA + k2 * TB + 2.0 * k * Xa;
+      INT24 = g2 * ra2 * TA + k * g1 * TB + (g1 + k * g2) * Xa;
+      INT44 = g2 * g2 * ra2 * TA + g1 * g1 * TB + 2.0 * g1 * g2 * Xa;
     }
   } else {
     // fluid layer: 2x2 E = [[ra, -ra], [-rho om2, -rho om2]] (sregn96.f90:791-801)
-    const cx ira = cinv(ra);
-    const double ir = -(0.5 / rom2);
+    const double ir = -(0.5 * irom2);
     const cx km1pd = (-0.5 * u0.uz) * ira + ir * u0.tz;
     const double w = -rom2;
-    if (typelyr == 0) {
+    if (!half) {
       const cx kmpu = (0.5 * u1.uz) * ira + ir * u1.tz;
-      const cx ard = ra * zdm;
-      const cx ea = (ard.re < 75.0) ? cexp_neg(ra, zdm) : mkc(0.0);
-      const cx ea40 = (ard.re < 40.0) ? ea : mkc(0.0);
-      const cx FA = (cabsc(ra) < 1.0e-08) ? mkc(zdm) : (1.0 - ea40 * ea40) / (2.0 * ra);
+      const double ard = v.preal ? v.rp * zdm : 0.0;
+      const cx ea = rexp(v.preal, v.ep, v.cosp, v.sp);
+      const cx ea40 = (ard < 40.0) ? ea : mkc(0.0);
+      const cx FA = (v.rp < 1.0e-08) ? mkc(zdm) : ffun(v.preal, v.irp, ea40.re, v.cosp, v.sp);
       const cx GA = ea * zdm;
       const cx sq = (kmpu * kmpu + km1pd * km1pd) * FA, cr = 2.0 * (kmpu * km1pd * GA);
       INT11 = ra2 * (sq - cr).re;
       INT22 = w * w * (sq + cr).re;
     } else {
-      const cx t = (km1pd * km1pd) / (2.0 * ra);
       INT11 = 0.0;
-      INT22 = w * w * t.re;
+      INT22 = w * w * re_mul(km1pd * km1pd, 0.5 * ira);
     }
   }
   // getmat (sregn96.f90:1531-1583) and the energy sums
   const double rho = zr, ah = za, av = za, eta = 1.0;
-  const double TA = zr * za * za, TC = zr * za * za;
+  const double TA = zr * za * za, TC = TA, iTC = y.izr * y.ia2;
   if (iwat == 1) {
     const double TN = 0.0, TF = TA - 2. * TN;
-    const double a12 = -(wvno * wvno - om * om / (ah * ah)) / (rho * om * om);
-    const double wr = wvno / (rho * om2);
+    const double a12 = -(k2 - s.om2 * y.ia2) * irom2;
+    const double wr = k * irom2;
     const double URUR = INT22 * (wr * wr), UZUZ = INT11;
-    const double URDUZ = -((wvno / (rho * om2)) * a12 * INT22);
+    const double URDUZ = -(wr * a12 * INT22);
     const double DUZDUZ = a12 * a12 * INT22;
     acc.sumi0 = acc.sumi0 + rho * (URUR + UZUZ);
     acc.sumi1 = acc.sumi1 + TA * URUR;
     acc.sumi2 = acc.sumi2 - TF * URDUZ;
     acc.sumi3 = acc.sumi3 + TC * DUZDUZ;
-    const double facah = rho * ah * (URUR - 2. * eta * URDUZ / wvno);
-    const double facav = rho * av * DUZDUZ / wvno2;
+    const double facah = rho * ah * (URUR - 2. * eta * URDUZ * ik);
+    const double facav = rho * av * DUZDUZ * ik2;
     dcda = facah + facav;
     dcdb = 0.0;
     const double facr = -(0.5 * c * c * (URUR + UZUZ));
-    dcdr = 0.5 * (av * facav + ah * facah) / rho + facr;
+    dcdr = 0.5 * (av * facav + ah * facah) * y.izr + facr;
   } else {
     const double bv = zb;
     const double TL = zr * zb * zb;
     const double TF = TA - 2. * TL;
-    const double a12 = -wvno, a14 = 1.0 / TL, a21 = wvno * TF / TC, a23 = 1.0 / TC;
+    const double a12 = -k, a14 = y.izr * y.ib2, a21 = k * TF * iTC, a23 = iTC;
     const double URUR = INT11, UZUZ = INT22;
     const double DURDUR = a12 * a12 * INT22 + 2. * a12 * a14 * INT24 + a14 * a14 * INT44;
     const double DUZDUZ = a21 * a21 * INT11 + 2. * a21 * a23 * INT13 + a23 * a23 * INT33;
@@ -469,19 +474,19 @@ SWDK_HD void energy_layer_r(const EigModel& M, int m, int iwat, bool allfluid, c
     acc.sumi1 = acc.sumi1 + TL * UZUZ + TA * URUR;
     acc.sumi2 = acc.sumi2 + TL * UZDUR - TF * URDUZ;
     acc.sumi3 = acc.sumi3 + TL * DURDUR + TC * DUZDUZ;
-    const double facah = rho * ah * (URUR - 2. * eta * URDUZ / wvno);
-    const double facav = rho * av * DUZDUZ / wvno2;
-    const double facbv = rho * bv * (UZUZ + 2. * UZDUR / wvno + DURDUR / wvno2 + 4. * eta * URDUZ / wvno);
+    const double facah = rho * ah * (URUR - 2. * eta * URDUZ * ik);
+    const double facav = rho * av * DUZDUZ * ik2;
+    const double facbv = rho * bv * (UZUZ + 2. * UZDUR * ik + DURDUR * ik2 + 4. * eta * URDUZ * ik);
     dcda = facah + facav;
     dcdb = facbv;
     const double facr = -(0.5 * c * c * (URUR + UZUZ));
-    dcdr = 0.5 * (av * facav + ah * facah + bv * facbv) / rho + facr;
+    dcdr = 0.5 * (av * facav + ah * facah + bv * facbv) * y.izr + facr;
   }
 }
 
-// svfunc eigenfunction at layer top i from the compound (cd) and Haskell (vv)
-// vectors (sregn96.f90:279-312)
-SWDK_HD Eig4 eigen_at(const double* cd, const double* vv, double ext, double f1213) {
+// svfunc eigenfunction at a layer top from the compound (cd) and Haskell
+// (vv) vectors (sregn96.f90:279-312); if1213 = 1/f1213
+SWDK_HD Eig4 eigen_at(const double* cd, const double* vv, double ext, double if1213) {
   const double cd1 = cd[0], cd2 = cd[1], cd3 = cd[2], cd4 = -cd[2], cd5 = cd[3], cd6 = cd[4];
   const double tz1 = -vv[3], tz2 = -vv[2], tz3 = vv[1], tz4 = vv[0];
   const double uu1 = tz2 * cd6 - tz3 * cd5 + tz4 * cd4;
@@ -490,107 +495,91 @@ SWDK_HD Eig4 eigen_at(const double* cd, const double* vv, double ext, double f12
   const double uu4 = -tz1 * cd4 + tz2 * cd2 - tz3 * cd1;
   Eig4 u;
   if (ext > -80.0 && ext < 80.0) {
-    const double fact = exp(ext);
-    u.ur = uu1 * fact / f1213;
-    u.uz = uu2 * fact / f1213;
-    u.tz = uu3 * fact / f1213;
-    u.tr = uu4 * fact / f1213;
+    const double fact = exp(ext) * if1213;
+    u.ur = uu1 * fact;
+    u.uz = uu2 * fact;
+    u.tz = uu3 * fact;
+    u.tr = uu4 * fact;
   } else {
     u.ur = 0.0; u.uz = 0.0; u.tz = 0.0; u.tr = 0.0;
   }
   return u;
 }
 
-// Scratch of one Rayleigh pass: per layer 6 doubles (cd[5], exe), reused for
-// the raw layer kernels (dcda, dcdb, dcdr) once the layer has been consumed.
-// Returns ugr (flat) and norm = ugr*sumi0; scr[6m+0..2] = raw dcda/dcdb/dcdr.
-SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, double wvno, double* scr, double& ugr,
-                            double& norm, const NodeSink& sink) {
-  const int L = M.L;
-  const double wvno2 = wvno * wvno, om2 = omega * omega;
+// One Rayleigh pass (sregn96's svfunc + energy) at (omega, wvno) over the
+// column's layer records lay[0..L-1] (top-down, lay[L-1] the half-space).
+// scr: 6 doubles per layer (up-pass compound vector and its exponent).
+// Returns ugr (flat) and norm = ugr*sumi0; the raw layer kernels go to the
+// sink as the top-down sweep produces them.
+template <class Sink>
+SWDK_HDI void rayleigh_pass(const RayLayer* lay, int L, double omega, double wvno, double* scr, double& ugr,
+                            double& norm, const Sink& sink) {
+  const SlotK s = slot_consts(omega, wvno);
   // ---- up (sregn96.f90:401-489) ----
   {
-    cx gbr[5];
-    EMat E;
-    const int iw = (M.zb[L - 1] > 0.0) ? 0 : 1;
-    evalg_r(M, L - 1, iw, allfluid, wvno, omega, om2, wvno2, E, gbr);
+    const RayLayer& y = lay[L - 1];
     double* c0 = scr + 6 * (L - 1);
-    for (int j = 0; j < 5; ++j) c0[j] = gbr[j].re;
+    halfspace_gbr(y, (y.zb > 0.0) ? 0 : 1, s, c0);
     c0[5] = 0.0;
   }
   double exr = 0.0;
   int exi = 0;
-  double ca[5][5];
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = L - 2; m >= 0; --m) {
-    const double zam = M.za[m], zbm = M.zb[m], zdm = M.zd[m];
-    const int iw = (zbm > 0.0) ? 0 : 1;
-    const double xka = omega / zam;
-    const double xkb = (zbm > 0.0) ? omega / zbm : 0.0;
-    Vars v;
-    varsv_real(wvno2 - xka * xka, wvno2 - xkb * xkb, zdm, iw, v);
-    dnka_r(ca, v, (float)M.zrho[m], (float)zbm, iw, wvno, wvno2, om2);
-    const double* cp = scr + 6 * (m + 1);
+    const RayLayer& y = lay[m];
+    const int iw = (y.zb > 0.0) ? 0 : 1;
+    LVars v;
+    vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
     double ee[5];
-    for (int i = 0; i < 5; ++i) {
-      double cr = 0.0;
-      for (int j = 0; j < 5; ++j) cr = cr + cp[j] * ca[j][i];
-      ee[i] = cr;
-    }
+    dnka_apply(v, y, iw, s, scr + 6 * (m + 1), ee);
     double t1 = 0.0;
     for (int i = 0; i < 5; ++i) t1 = fmax(t1, fabs(ee[i]));
     int e = 0;
-    if (t1 >= 1.e-40) e = pow2_exponent(t1);
+    double sc = 1.0;
+    if (t1 >= 1.e-40) e = pow2_norm(t1, sc);
     double* cm = scr + 6 * m;
-    for (int i = 0; i < 5; ++i) cm[i] = ldexp(ee[i], -e);
+    for (int i = 0; i < 5; ++i) cm[i] = ee[i] * sc;
     exr = exr + v.pex + v.svex;
     exi += e;
     cm[5] = exr + (double)exi * LN2;
   }
   // ---- down + svfunc + energy, top-down ----
-  const double f1213 = -scr[1];
+  const double if1213 = -1.0 / scr[1];
   const double exe0 = scr[5];
   Eig4 u0;
   u0.ur = scr[2] / scr[1];
   u0.uz = 1.0; u0.tz = 0.0; u0.tr = 0.0;
-  if (M.zb[0] <= 0.0 && !allfluid) { u0.ur = 0.0; u0.tr = 0.0; }  // fluid top (jwat)
+  if (lay[0].zb <= 0.0) { u0.ur = 0.0; u0.tr = 0.0; }  // fluid top (jwat)
   double vv[4] = {1.0, 0.0, 0.0, 0.0};
   double dxr = 0.0;
   int dxi = 0;
   EnergyAcc acc = {0.0, 0.0, 0.0, 0.0};
-  const double c = omega / wvno;
-  double AA[4][4];
+  const double c = omega * s.ik;
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = 0; m < L; ++m) {
-    const double zbm = M.zb[m];
-    const int iw = (zbm > 0.0) ? 0 : 1;
+    const RayLayer& y = lay[m];
+    const int iw = (y.zb > 0.0) ? 0 : 1;
+    const bool half = (m == L - 1);
+    LVars v;
+    vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
     Eig4 u1 = u0;
-    if (m < L - 1) {
-      const double zam = M.za[m], zdm = M.zd[m];
-      const double xka = omega / zam;
-      const double xkb = (zbm > 0.0) ? omega / zbm : 0.0;
-      Vars v;
-      varsv_real(wvno2 - xka * xka, wvno2 - xkb * xkb, zdm, iw, v);
-      hska_r(AA, v, (float)M.zrho[m], (float)zbm, iw, wvno, wvno2, om2);
+    if (!half) {
       double a0[4];
-      for (int i = 0; i < 4; ++i) {
-        double cc = 0.0;
-        for (int j = 0; j < 4; ++j) cc = cc + AA[i][j] * vv[j];
-        a0[i] = cc;
-      }
+      hska_apply(v, y, iw, s, vv, a0);
       double t1 = fmax(fmax(fabs(a0[0]), fabs(a0[1])), fmax(fabs(a0[2]), fabs(a0[3])));
       int e = 0;
-      if (t1 >= 1.e-40) e = pow2_exponent(t1);
-      for (int i = 0; i < 4; ++i) vv[i] = ldexp(a0[i], -e);
+      double sc = 1.0;
+      if (t1 >= 1.e-40) e = pow2_norm(t1, sc);
+      for (int i = 0; i < 4; ++i) vv[i] = a0[i] * sc;
       dxr = dxr + v.pex;
       dxi += e;
       const double exa1 = dxr + (double)dxi * LN2;
       const double* cd1 = scr + 6 * (m + 1);
-      u1 = eigen_at(cd1, vv, exa1 + cd1[5] - exe0, f1213);
+      u1 = eigen_at(cd1, vv, exa1 + cd1[5] - exe0, if1213);
     }
     double da, db, dr;
-    energy_layer_r(M, m, iw, allfluid, u0, u1, omega, om2, wvno, wvno2, c, acc, da, db, dr);
-    sink.add(M, m, da, db, dr);
+    energy_lean(y, v, iw, half, u0, u1, s, c, acc, da, db, dr);
+    sink.add(m, y.vtp, y.rtp, da, db, dr);
     u0 = u1;
   }
   ugr = (wvno * acc.sumi1 + acc.sumi2) / (omega * acc.sumi0);
@@ -598,23 +587,21 @@ SWDK_HDI void rayleigh_pass(const EigModel& M, bool allfluid, double omega, doub
 }
 
 // ---------------------------------------------------------------------------
-// Love pass (slegn96.f90): up, shfunc normalisation, energy.  scr holds 3
-// doubles per layer (uu, tt, exl) then the raw (dcdb, dcdr).  Returns ugr and
-// the normaliser sumi1.
+// One Love pass (slegn96.f90): up, shfunc normalisation, energy.  scr holds
+// 3 doubles per layer (uu, tt, exl).  Returns ugr and the normaliser sumi1.
 // ---------------------------------------------------------------------------
-SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* scr, double& ugr, double& norm,
-                        const NodeSink& sink) {
-  const int L = M.L;
-  const double wvno2 = wvno * wvno;
+template <class Sink>
+SWDK_HDI void love_pass(const LoveLayer* lay, int L, double omega, double wvno, double* scr, double& ugr,
+                        double& norm, const Sink& sink) {
+  const double wvno2 = wvno * wvno, om2 = omega * omega, ik = 1.0 / wvno, ik2 = ik * ik;
   // ---- up (slegn96.f90:372-445) ----
   {
+    const LoveLayer& y = lay[L - 1];
     double* s0 = scr + 3 * (L - 1);
-    if (M.zb[L - 1] > (double)0.01f) {
-      const double zb = M.zb[L - 1];
-      const double xkb = omega / zb;
-      const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    if (y.zb > (double)0.01f) {
+      const double rb = sqrt(fabs(wvno2 - om2 * y.ib2));
       s0[0] = 1.0;
-      s0[1] = -(M.zrho[L - 1] * (zb * zb)) * rb;
+      s0[1] = -y.mu * rb;
     } else {
       s0[0] = 1.0;
       s0[1] = 0.0;
@@ -624,36 +611,37 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = L - 2; k >= 0; --k) {
     double* sk = scr + 3 * k;
-    const double zb = M.zb[k];
-    if (!(zb > 0.0)) { sk[0] = 0.0; sk[1] = 0.0; sk[2] = 0.0; continue; }
-    const double dpth = M.zd[k];
-    const double xkb = omega / zb;
-    const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
-    const double q = rb * dpth;
-    const double mu = M.zrho[k] * zb * zb;
+    const LoveLayer& y = lay[k];
+    if (!(y.zb > 0.0)) { sk[0] = 0.0; sk[1] = 0.0; sk[2] = 0.0; continue; }
+    const double dpth = y.d;
+    const double x2 = wvno2 - om2 * y.ib2;  // (wvno + xkb)(wvno - xkb)
     double cosq, yl, zl, eexl = 0.0;
-    if (wvno < xkb) {
+    if (x2 < 0.0) {  // wvno < xkb
+      const double ir = rsqrt(-x2), rb = -x2 * ir;
       double sq, cq;
-      sincos(q, &sq, &cq);
-      yl = sq / rb; zl = -rb * sq; cosq = cq;
-    } else if (wvno == xkb) {
+      sincos(rb * dpth, &sq, &cq);
+      yl = sq * ir; zl = -rb * sq; cosq = cq;
+    } else if (x2 == 0.0) {
       cosq = 1.0; yl = dpth; zl = 0.0;
     } else {
+      const double ir = rsqrt(x2), rb = x2 * ir, q = rb * dpth;
       eexl = q;
-      const double fac = (q < 18.0) ? exp(-2.0 * q) : 0.0;
+      const double e1 = (q < 18.0) ? exp(-q) : 0.0;
+      const double fac = e1 * e1;  // exp(-2q)
       cosq = (1.0 + fac) * 0.5;
       const double sq = (1.0 - fac) * 0.5;
-      yl = sq / rb; zl = rb * sq;
+      yl = sq * ir; zl = rb * sq;
     }
-    const double a11 = cosq, a22 = cosq, a12 = -(yl / mu), a21 = -(zl * mu);
+    const double a11 = cosq, a22 = cosq, a12 = -(yl * y.imu), a21 = -(zl * y.mu);
     const double* s1 = scr + 3 * (k + 1);
     const double amp0 = a11 * s1[0] + a12 * s1[1];
     const double str0 = a21 * s1[0] + a22 * s1[1];
     const double rr = fmax(fabs(amp0), fabs(str0));
     int e = 0;
-    if (rr >= 1.e-30) e = pow2_exponent(rr);
-    sk[0] = ldexp(amp0, -e);
-    sk[1] = ldexp(str0, -e);
+    double sc = 1.0;
+    if (rr >= 1.e-30) e = pow2_norm(rr, sc);
+    sk[0] = amp0 * sc;
+    sk[1] = str0 * sc;
     sk[2] = (double)e * LN2 + eexl;
   }
   // ---- shfunc normalisation (slegn96.f90:212-240) ----
@@ -663,9 +651,9 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = 1; k < L; ++k) {
     double* sk = scr + 3 * k;
-    if (M.zb[k] > 0.0) {
+    if (lay[k].zb > 0.0) {
       ext = ext + scr[3 * (k - 1) + 2];
-      const double fact = (ext < 80.0) ? 1. / exp(ext) : 0.0;
+      const double fact = (ext < 80.0) ? exp(-ext) : 0.0;
       sk[0] = sk[0] * fact;
       sk[1] = sk[1] * fact;
     } else {
@@ -676,7 +664,7 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
   if (scr[0] != 0.0) umax = scr[0];
   const double iumax = (fabs(umax) > 0.0) ? 1.0 / umax : 1.0;
   // ---- energy (slegn96.f90:447-576) with uu/tt scaled by 1/umax on the fly ----
-  const double c = omega / wvno;
+  const double c = omega * ik;
   double sumi0 = 0.0, sumi1 = 0.0;
   double prev_uu = scr[0] * iumax, prev_tt = scr[1] * iumax;
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
@@ -689,90 +677,57 @@ SWDK_HDI void love_pass(const EigModel& M, double omega, double wvno, double* sc
     }
     prev_uu = nuu;
     prev_tt = ntt;
-    const double zb = M.zb[k];
+    const LoveLayer& y = lay[k];
+    const double zb = y.zb;
     if (!(zb > 0.0)) continue;
-    const double zr = M.zrho[k];
-    const double TN = zr * zb * zb;
-    const double drho = zr, dpth = M.zd[k];
-    const double xkb = omega / zb;
-    double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
-    const double dmu = zr * (zb * zb);
-    if (rb < 1.0e-10) rb = 1.0e-10;
+    const double drho = y.zr, dpth = y.d, dmu = y.mu;
+    const double x2 = wvno2 - om2 * y.ib2;
+    double rb = 0.0, irb = 0.0;
+    if (x2 != 0.0) {
+      irb = rsqrt(fabs(x2));
+      rb = fabs(x2) * irb;
+    }
+    if (rb < 1.0e-10) { rb = 1.0e-10; irb = 1.0e10; }
     double upup, dupdup;
     if (k == L - 1) {
-      upup = (0.5 / rb) * uu * uu;
+      upup = (0.5 * irb) * uu * uu;
       dupdup = (0.5 * rb) * uu * uu;
     } else {
-      cx nub = mkc(rb, 0.0);
-      if (wvno < xkb) nub = mkc(0.0, rb);
-      const cx xnub = dmu * nub;
-      const cx ei11 = mkc(0.5 / wvno), ei12 = 0.5 / (wvno * xnub), ei21 = mkc(0.5 / wvno),
-               ei22 = -(0.5 / (wvno * xnub));
-      const cx el11 = mkc(wvno), el12 = mkc(wvno);
-      const cx km1dn = ei21 * uu + ei22 * tt;
-      const cx kmup = ei11 * nuu + ei12 * ntt;
-      const cx f3 = nub * dpth;
-      cx exqq = mkc(0.0);
-      if (f3.re < 40.0) exqq = cexpc(-2.0 * f3);
-      const cx f = (1.0 - exqq) / (2.0 * nub);
-      exqq = mkc(0.0);
-      if (f3.re < 75.0) exqq = cexpc(-f3);
-      const cx g = dpth * exqq;
-      const cx f1 = f * (el11 * el11 * kmup * kmup + el12 * el12 * km1dn * km1dn);
-      const cx f2 = g * (el11 * el12 + el11 * el12) * kmup * km1dn;
+      const bool real = !(x2 < 0.0);  // nub = rb, or i rb when wvno < xkb
+      // ei11 = ei21 = 0.5/wvno, ei12 = -ei22 = 0.5/(wvno dmu nub)
+      const double e0 = 0.5 * ik;
+      const cx ei12 = rinv(real, 0.5 * ik * y.imu * irb);
+      const cx km1dn = mkc(e0 * uu) - ei12 * tt;
+      const cx kmup = mkc(e0 * nuu) + ei12 * ntt;
+      const double q = rb * dpth;
+      cx f, g;
+      if (real) {
+        const double e1 = (q < 75.0) ? exp(-q) : 0.0;
+        const double e2 = (q < 40.0) ? e1 * e1 : 0.0;  // exp(-2 nub d)
+        f = mkc((1.0 - e2) * 0.5 * irb, 0.0);
+        g = mkc(dpth * e1, 0.0);
+      } else {
+        double sn, cs;
+        sincos(q, &sn, &cs);
+        f = mkc(sn * cs * irb, -sn * sn * irb);
+        g = mkc(dpth * cs, -dpth * sn);
+      }
+      const cx f1 = f * (wvno2 * (kmup * kmup + km1dn * km1dn));
+      const cx f2 = g * (2.0 * wvno2) * kmup * km1dn;
       upup = (f1 + f2).re;
-      dupdup = (nub * nub * (f1 - f2)).re;
+      const double nub2 = real ? rb * rb : -rb * rb;
+      dupdup = nub2 * (f1 - f2).re;
     }
     sumi0 = sumi0 + drho * upup;
-    sumi1 = sumi1 + TN * upup;
+    sumi1 = sumi1 + dmu * upup;
     const double VSHH = zb, VSHV = zb;
     const double DCDBH = c * drho * VSHH * upup;
-    const double DCDBV = c * drho * VSHV * dupdup / wvno2;
-    sink.add(M, k, 0.0, DCDBH + DCDBV, 0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup / wvno2));
+    const double DCDBV = c * drho * VSHV * dupdup * ik2;
+    sink.add(k, y.vtp, y.rtp, 0.0, DCDBH + DCDBV,
+             0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup * ik2));
   }
   ugr = sumi1 / (c * sumi0);
   norm = sumi1;
-}
-
-// ---------------------------------------------------------------------------
-// _ParamConvert (SurfaceWave.cpp:59-101) of x(l) = raw(l)/norm * fac(l)
-// into node values out[0..nz-1]; nw leading fluid nodes.
-// raw(l) = scr[stride*l + off]
-// ---------------------------------------------------------------------------
-SWDK_HD double layer_val(const double* scr, int stride, int off, int l, double norm, const double* fac) {
-  return (scr[stride * l + off] / norm) * fac[l];
-}
-
-SWDK_HDI void param_convert_dev(const double* scr, int stride, int off, double norm, const double* fac, int L, int nz,
-                                int nw, double* out) {
-  const int n = 4;
-  if (nw == 0) {
-    for (int i = 0; i < nz; ++i) {
-      double tup = 0.0, tdwn = 0.0;
-      const int idup = (i - 1) * n, iddw = i * n;
-      for (int j = 0; j < n; ++j) {
-        const double tmp = (2. * j + 1.0) / (2. * n);
-        if (idup + j >= 0) tup += layer_val(scr, stride, off, idup + j, norm, fac) * tmp;
-        if (iddw + j < L) tdwn += layer_val(scr, stride, off, iddw + j, norm, fac) * (1.0 - tmp);
-        if (iddw == L - 1) tdwn += layer_val(scr, stride, off, L - 1, norm, fac);
-      }
-      out[i] = 0.0 + (tup + tdwn);
-    }
-  } else {
-    out[0] = layer_val(scr, stride, off, 0, norm, fac);
-    for (int i = 1; i < nw; ++i) out[i] = 0.0;
-    for (int i = nw; i < nz; ++i) {
-      double tup = 0.0, tdwn = 0.0;
-      const int idup = (i - nw - 1) * n + 1, iddw = (i - nw) * n + 1;
-      for (int j = 0; j < n; ++j) {
-        const double tmp = (2. * j + 1.0) / (2. * n);
-        if (idup + j >= 1) tup += layer_val(scr, stride, off, idup + j, norm, fac) * tmp;
-        if (iddw + j < L) tdwn += layer_val(scr, stride, off, iddw + j, norm, fac) * (1.0 - tmp);
-        if (iddw == L - 1) tdwn += layer_val(scr, stride, off, L - 1, norm, fac);
-      }
-      out[i] = 0.0 + (tup + tdwn);
-    }
-  }
 }
 
 }  // namespace swdk

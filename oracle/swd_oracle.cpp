@@ -1882,6 +1882,14 @@ struct Opts {
   int sphere;
 };
 
+// Conditioning probe (test hook, not a reference behaviour): kernel1d and
+// disp1d hand the eigenfunction routines c*(1+g_cpert) instead of each root
+// c (and c1, c2 of the group kernels), so a test can measure how far the
+// oracle's own kernels and group velocities move under a rounding-level
+// change of their input.  0 (the default) leaves both exactly as the
+// reference.
+double g_cpert = 0.0;
+
 // kernel1D (SurfaceWave.cpp:266-412); kvs/kvp/krho are (nz, kmax) column-major
 void kernel1d(const float* vs, const float* vp, const float* rho, const float* dep, int nz, const Tables& T,
               double* vc, double* vout, double* kvs, double* kvp, double* krho, int* status, const Opts& op,
@@ -1913,6 +1921,7 @@ void kernel1d(const float* vs, const float* vp, const float* rho, const float* d
             for (int iz = 0; iz < nz; ++iz) { kvs[k * nz + iz] = 0; kvp[k * nz + iz] = 0; krho[k * nz + iz] = 0; }
             continue;
           }
+          if (g_cpert != 0.0) vc[k] = vc[k] * (1.0 + g_cpert);
           if (w == 0) {
             sregn96_(TH, VP, VS, RH, rmax, &tt[i], vc + k, &cg, ur.data(), uz.data(), tr.data(), tz.data(),
                      dcdar.data(), dcdbr.data(), dcdhr.data(), dcdrr.data(), iflsph);
@@ -1951,6 +1960,11 @@ void kernel1d(const float* vs, const float* vp, const float* rho, const float* d
             vc[k] = 0.0; vout[k] = 0.0;
             for (int iz = 0; iz < nz; ++iz) { kvs[k * nz + iz] = 0; kvp[k * nz + iz] = 0; krho[k * nz + iz] = 0; }
             continue;
+          }
+          if (g_cpert != 0.0) {
+            cp[i] = cp[i] * (1.0 + g_cpert);
+            c1[i] = c1[i] * (1.0 + g_cpert);
+            c2[i] = c2[i] * (1.0 + g_cpert);
           }
           if (w == 1) {
             sregnpu_(TH, VP, VS, RH, rmax, &tt[i], &cp[i], vc + k, ur.data(), uz.data(), tr.data(), tz.data(),
@@ -2009,6 +2023,7 @@ void disp1d(const float* vs, const float* vp, const float* rho, const float* dep
         for (int i = 0; i < nt; ++i) {
           double* cgp = vout + idx + i;
           if (cp[i] == 0.0) { *cgp = 0.0; continue; }
+          if (g_cpert != 0.0) cp[i] = cp[i] * (1.0 + g_cpert);
           if (w == 1)
             sregn96_(TH, VP, VS, RH, rmax, tt + i, &cp[i], cgp, b0.data(), b1.data(), b2.data(), b3.data(),
                      b4.data(), b5.data(), b6.data(), b7.data(), iflsph);
@@ -2033,6 +2048,9 @@ int total_kmax(const Tables& T) {
 }  // namespace
 
 extern "C" {
+
+// the conditioning probe of kernel1d (0 = off)
+void swdo_set_eigen_cpert(double rel) { g_cpert = rel; }
 
 // get_1d_kernel (SurfaceWave.cpp:458-502) over ncol columns with OpenMP.
 //   vs: (ncol, nz) column-major float; vp_in/rho_in optional explicit node

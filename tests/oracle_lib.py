@@ -183,6 +183,44 @@ def get_1d_kernel(case, refine=1, rtol=1e-10, sngl=1, sphere=1, nthreads=0, cols
     return dict(vc=vc, vout=vo, kernel=ker, status=st, nevals=nev.value)
 
 
+def kernel_spread(case, cols, rel=1e-15, steps=(-3, -1, 1, 3)):
+    """Conditioning of the oracle's own kernel path at the given columns:
+    get_1d_kernel with every phase velocity handed to sregn96/slegn96 (and
+    c1, c2 of the group kernels) moved by s*rel relative, s in `steps`.
+    Returns (kernel spread, U spread): per (slot, column) the largest change
+    of the node kernel relative to the slot's largest |kernel|, and the
+    largest change of vout (km/s), over the steps."""
+    base = get_1d_kernel(case, cols=cols)
+    scale = np.abs(base["kernel"]).max(axis=1) + 1e-30
+    ks = np.zeros_like(scale)
+    us = np.zeros_like(scale)
+    try:
+        for st in steps:
+            lib().swdo_set_eigen_cpert(C.c_double(st * rel))
+            r = get_1d_kernel(case, cols=cols)
+            ks = np.maximum(ks, np.abs(r["kernel"] - base["kernel"]).max(axis=1) / scale)
+            us = np.maximum(us, np.abs(r["vout"] - base["vout"]))
+    finally:
+        lib().swdo_set_eigen_cpert(C.c_double(0.0))
+    return ks, us
+
+
+def map_spread(case, cols, rel=1e-15, steps=(-3, -1, 1, 3)):
+    """The same conditioning probe for get_2d_map: the largest change of vout
+    (km/s) per (slot, column) when the phase velocity handed to
+    sregn96/slegn96 moves by s*rel relative."""
+    base = get_2d_map(case, cols=cols)
+    us = np.zeros_like(base["vout"])
+    try:
+        for st in steps:
+            lib().swdo_set_eigen_cpert(C.c_double(st * rel))
+            r = get_2d_map(case, cols=cols)
+            us = np.maximum(us, np.abs(r["vout"] - base["vout"]))
+    finally:
+        lib().swdo_set_eigen_cpert(C.c_double(0.0))
+    return us
+
+
 def get_2d_map(case, refine=1, rtol=1e-10, sngl=1, sphere=1, nthreads=0, cols=None):
     from jdsurfg_b200.synth import subset_columns
     if cols is not None:

@@ -1,15 +1,24 @@
-"""Accuracy report on the 256x256x64, 60-period grid with phase AND group
-velocity of Rayleigh and Love (mode 0): max and RMS |dc|, |dU| and kernel
-relative error of the GPU path against the all-FP64 oracle.
+"""Accuracy report of the GPU path against the all-FP64 oracle on 2048
+seeded random columns of two grids:
 
-The reference's group velocity in the kernel path (sregnpu/slegnpu energy
-integrals) is ill-conditioned at a few (column, period) points: moving the
-phase velocity input by 1e-15 relative moves U by up to 1e-4 km/s there.
-Two correct FP64 implementations then disagree by that much.  A slot whose
-|dU| exceeds 1e-6 km/s therefore passes only if the oracle's own U moves by
-at least |dU| under such a perturbation (sregnpu_/slegnpu_ called directly);
-its kernel, and the phase kernel of the same period, are held to the same
-rule with a looser factor.
+* the 256x256x64 grid at 60 periods 1-80 s with phase AND group velocity of
+  Rayleigh and Love (mode 0), and
+* the 128x128x48 production grid at 40 periods 1-60 s, Rayleigh and Love
+  modes 0-1, phase and group, with water layers and low-velocity zones.
+
+Per grid it prints max and RMS |dc|, |dU| and the kernel error (relative to
+the slot's largest |kernel|).  Tolerances: |dc|, |dU| <= 1e-6 km/s, kernel
+<= 1e-5.
+
+Exemptions are in matching units.  The reference's kernel path is
+ill-conditioned at a few (column, period) points: moving the phase velocity
+handed to sregn96/sregnpu/slegn96/slegnpu by 1e-15 relative then moves U by
+up to 1e-4 km/s and the kernel by up to 1e-3 of its largest value, so two
+correct FP64 implementations disagree by that much.  A slot outside the
+tolerance passes only if the oracle's own U (km/s) and kernel (relative)
+move by comparable amounts under such changes (oracle_lib.kernel_spread):
+|dU| <= max(1e-6, 2 * U spread) and kernel error <= max(1e-5, 10 * kernel
+spread).  The number of exempted slots is printed.
 """
 import numpy as np
 import pytest
@@ -20,38 +29,82 @@ from jdsurfg_b200 import Engine, synth
 pytestmark = pytest.mark.gpu
 
 TOL_C, TOL_U, TOL_K = 1e-6, 1e-6, 1e-5
+NCOL = 2048
 
 
-def test_accuracy_report_phase_and_group():
-    full = synth.make_config("mixed", seed=2024)
-    ncol = 96
-    case = synth.subset_columns(full, np.arange(ncol))
+def _report(name, seed):
+    full = synth.make_config(name, seed=seed)
+    ncol_full = full["nx"] * full["ny"]
+    cols = np.sort(np.random.default_rng(seed + 1).choice(ncol_full, NCOL, replace=False))
+    case = synth.subset_columns(full, cols)
     ref = O.get_1d_kernel(case, refine=1, rtol=1e-10)
     eng = Engine(device=0)
     eng.setup(case)
     g = eng.get_1d_kernel(case["vs"], case["vp"], case["rho"], nx=case["nx"], ny=case["ny"])
     eng.close()
-    assert np.array_equal(g["status"], ref["status"])
-    ok = ref["status"] == 0
+    np.testing.assert_array_equal(g["status"], ref["status"])
+    ok = (ref["status"] == 0) | (ref["status"] == 2)
     dc = np.abs(g["vc"] - ref["vc"])
     du = np.abs(g["vout"] - ref["vout"])
-    scale = np.abs(ref["kernel"]).max(axis=1, keepdims=True) + 1e-30
-    kr = (np.abs(g["kernel"] - ref["kernel"]) / scale).max(axis=1)
-    print(f"|dc| max {dc[ok].max():.3g} rms {np.sqrt(np.mean(dc[ok] ** 2)):.3g}; "
-          f"|dU| max {du[ok].max():.3g} rms {np.sqrt(np.mean(du[ok] ** 2)):.3g}; "
-          f"kernel rel max {kr[ok].max():.3g} rms {np.sqrt(np.mean(kr[ok] ** 2)):.3g}")
+    scale = np.abs(ref["kernel"]).max(axis=1) + 1e-30
+    kr = np.abs(g["kernel"] - ref["kernel"]).max(axis=1) / scale
+    assert dc[ok].max() <= TOL_C, f"{name}: max |dc| {dc[ok].max():.3g}"
+    bad = ok & ((du > TOL_U) | (kr > TOL_K))
+    bcols = np.nonzero(bad.any(axis=0))[0]
+    nexempt = 0
+    if len(bcols):
+        ks, us = O.kernel_spread(case, bcols)
+        for j, col in enumerate(bcols):
+            for s in np.nonzero(bad[:, col])[0]:
+                print(f"{name} slot {s} column {cols[col]}: |dU| {du[s, col]:.3g} (oracle U spread {us[s, j]:.3g}), "
+                      f"kernel {kr[s, col]:.3g} (oracle kernel spread {ks[s, j]:.3g})")
+                assert du[s, col] <= max(TOL_U, 2.0 * us[s, j])
+                assert kr[s, col] <= max(TOL_K, 10.0 * ks[s, j])
+                nexempt += 1
+    rms = lambda x: float(np.sqrt(np.mean(x[ok] ** 2)))
+    line = (f"{name}: {NCOL} columns x {ref['vc'].shape[0]} slots ({int(ok.sum())} with a root): "
+            f"|dc| max {dc[ok].max():.3g} rms {rms(dc):.3g} km/s; |dU| max {du[ok].max():.3g} rms {rms(du):.3g} km/s; "
+            f"kernel rel max {kr[ok].max():.3g} rms {rms(kr):.3g}; {nexempt} slots exempted by the oracle's own "
+            f"conditioning")
+    print(line)
+    return nexempt, int(ok.sum())
+
+
+def test_accuracy_256x256x64_phase_and_group():
+    nexempt, n = _report("mixed", 2024)
+    assert nexempt <= n // 1000
+
+
+def test_accuracy_production_modes_water():
+    nexempt, n = _report("production", 4048)
+    assert nexempt <= n // 1000
+
+
+def test_group_map_production_1024_columns():
+    """get_2d_map (SurfaceWave.cpp:420-450): phase and group maps of Rayleigh
+    and Love modes 0-1 (group velocity from sregn96/slegn96 at the phase
+    root, disp1D) on 1024 random columns of the production grid."""
+    full = synth.make_config("production", seed=777)
+    cols = np.sort(np.random.default_rng(778).choice(full["nx"] * full["ny"], 1024, replace=False))
+    case = synth.subset_columns(full, cols)
+    ref = O.get_2d_map(case, refine=1, rtol=1e-10)
+    eng = Engine(device=0)
+    eng.setup(case)
+    g = eng.get_2d_map(case["vs"], case["vp"], case["rho"], nx=case["nx"], ny=case["ny"])
+    eng.close()
+    np.testing.assert_array_equal(g["status"], ref["status"])
+    ok = (ref["status"] == 0) | (ref["status"] == 2)
+    dc = np.abs(g["vc"] - ref["vc"])
+    du = np.abs(g["vout"] - ref["vout"])
     assert dc[ok].max() <= TOL_C
-    periods = np.geomspace(1.0, 80.0, 60)
-    bad = np.argwhere(ok & ((du > TOL_U) | (kr > TOL_K)))
-    assert len(bad) <= max(3, ok.sum() // 1000), f"{len(bad)} slots outside tolerance"
-    for s, col in bad:
-        wave = ("Rc", "Rg", "Lc", "Lg")[s // 60]
-        assert dc[s, col] <= TOL_C
-        # the eigenfunctions (and so phase kernels too) share the group slot's
-        # conditioning at the same period and phase velocity
-        probe = "Rg" if wave in ("Rc", "Rg") else "Lg"
-        _, spread = O.group_u_spread(case, int(col), probe, periods, int(s % 60))
-        print(f"slot {s} column {col}: |dU| {du[s, col]:.3g}, kernel {kr[s, col]:.3g}, oracle U spread "
-              f"under 1e-15 changes of c: {spread:.3g}")
-        assert du[s, col] <= max(TOL_U, 2 * spread)
-        assert kr[s, col] <= max(TOL_K, 10 * spread)
+    bad = ok & (du > TOL_U)
+    bcols = np.nonzero(bad.any(axis=0))[0]
+    if len(bcols):
+        us = O.map_spread(case, bcols)
+        for j, col in enumerate(bcols):
+            for s in np.nonzero(bad[:, col])[0]:
+                print(f"map slot {s} column {cols[col]}: |dU| {du[s, col]:.3g} (oracle U spread {us[s, j]:.3g})")
+                assert du[s, col] <= max(TOL_U, 2.0 * us[s, j])
+    print(f"get_2d_map production: {ok.sum()} slots, |dc| max {dc[ok].max():.3g}, |dU| max {du[ok].max():.3g} "
+          f"rms {np.sqrt(np.mean(du[ok] ** 2)):.3g} km/s, {int(bad.sum())} exempted")
+    assert bad.sum() <= ok.sum() // 1000
