@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--split-cols", type=int, default=0,
                     help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
     ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="strong scaling: ONE model split by columns over the ranks (allocate_tasks), each step "
+                         "computing the rank's block and all-gathering the vc/vout/status maps with NCCL")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
@@ -457,6 +460,74 @@ def run_uneven(args, torch, dev, rank, world, pg):
     return 0
 
 
+def run_sharded(args, torch, dev, rank, world, pg):
+    """Strong scaling of get_1d_kernel over the ranks: every rank holds the
+    same model (the workload's seed 2024 grid) in HBM, computes its column
+    block (jdsurfg_b200/shard.py, the reference's allocate_tasks split) and
+    the maps are all-gathered on the devices; depth kernels stay with the
+    rank that computed them.  value = all slots of the one model / step time
+    (max over ranks)."""
+    from jdsurfg_b200 import Engine, learn
+    from jdsurfg_b200.shard import ShardedSurfTime, column_block
+    case = workload(args, 0)
+    eng = Engine(device=dev.index, refine=args.refine)
+    if args.proposal == "learned":
+        learn.load_proposals(eng)
+    eng.setup(case)
+    ncol, kmax = case["nx"] * case["ny"], eng.kmax
+    units = ncol * kmax
+    sh = ShardedSurfTime(rank, world, engine=eng)
+    t = lambda a: None if a is None else torch.from_numpy(a).to(dev)
+    vs, vp, rho = t(case["vs"]), t(case["vp"]), t(case["rho"])
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sptr = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        flush.fill_(1)
+        return sh.get_1d_kernel_device(vs, vp, rho, stream=sptr)
+
+    for _ in range(args.warmup):
+        r = step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        r = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if pg:
+        tt = torch.tensor([ms], device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        ms = float(tt.item())
+    c0, c1 = column_block(ncol, world, rank)
+    gather_bytes = 3 * kmax * (-(-ncol // world)) * 8 * world
+    launches = eng.stats()["kernel_launches"] * args.steps
+    if rank == 0:
+        line = {"metric": METRIC, "value": units / (ms / args.steps * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator, jdsurfg_b200/synth.py)",
+                "config": dict(case_desc(args, case, kmax), sharded=True,
+                               timed_as="per step: the rank's column block through get_1d_kernel_device, then the "
+                                        "NCCL all-gather of the vc/vout/status maps (device tensors)",
+                               columns_rank0=c1 - c0, all_gather_bytes_per_step=gather_bytes),
+                "clocks": clk, "e2e": None, "gpu_launches": launches, "roofline": None, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -475,6 +546,8 @@ def main():
         return run_uneven(args, torch, dev, rank, world, pg)
     if args.workload == "fmst":
         return run_fmst(args, torch, dev, rank, world, pg)
+    if args.sharded:
+        return run_sharded(args, torch, dev, rank, world, pg)
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
     eng = Engine(device=local, refine=args.refine, split_cols=args.split_cols, block_roots=args.roots_blocks)
@@ -533,6 +606,7 @@ def main():
         probe_eng.close()
         acc = {k: probe[k] * nsteps for k in STAT_KEYS}
         acc["kernel_launches"] = launches * nsteps
+        acc["evals_by_phase"] = probe["evals_by_phase"]
         use_graph = not args.no_graph
         if use_graph:
             eng.graph_capture("kernel", nx, ny, nz, vs, vp, rho, vc, vout, ker, st)
@@ -589,6 +663,7 @@ def main():
                  "learned_speedup": (pms / args.steps) / ms_per_step,
                  "learned_roots_speedup": pacc["ms_roots"] / max(1e-9, roots_ms + acc["ms_proposal"]),
                  "learned_eval_reduction": pacc["secular_evals"] / max(1, evals),
+                 "evals_per_slot_by_phase": {k: v / units for k, v in pacc["evals_by_phase"].items()},
                  "max_abs_dc_learned_vs_plain_km_s": dmax}
         nets, _ = learn.load_proposals(eng)  # the e2e leg runs the learned path again
         eng_nets_on[0] = True
@@ -683,6 +758,7 @@ def main():
                 "plain": plain,
                 "detail": {"secular_evals_per_step": evals / args.steps,
                            "evals_per_slot": evals / args.steps / units,
+                           "evals_per_slot_by_phase": {k: v / units for k, v in acc["evals_by_phase"].items()},
                            "proposals_used": acc["proposals_accepted"] / args.steps,
                            "proposals_fell_back": acc["proposals_rejected"] / args.steps,
                            "ms_prep": acc["ms_prep"] / args.steps, "ms_proposal": acc["ms_proposal"] / args.steps,

@@ -93,6 +93,13 @@ typedef struct swdk_stats {
   int64_t proposals_rejected;  /* learned brackets that fell back to the plain scan  */
   float ms_proposal;           /* device time of feature extraction + inference  */
   int32_t kernel_launches;     /* kernels this library launched for the call       */
+  int64_t evals_by_phase[6];   /* secular evaluations by phase: [0] the scan of a
+                                  mode's first period (getsol, surfdisp96.f:400-495),
+                                  [1] scans of later periods, group passes and
+                                  dropped proposals, [2] the learned cell's two ends,
+                                  [3] walks from a learned cell, [4] the refinement
+                                  (nevill / Brent), [5] single-period retries
+                                  (surfdisp.cpp:94-109)                          */
 } swdk_stats;
 
 typedef struct swdk_ctx swdk_ctx;

@@ -38,6 +38,13 @@ namespace {
 constexpr int FEAT_NODES = 64, FEAT_DIM = 320;  // proposal network input (see swdk_mlp.cu)
 constexpr double FEAT_C0 = 3.5;                  // phase velocity offset of the network target
 
+// statistics counters of a call (device array, copied to the host):
+// [0] secular evaluations, [1]/[2] Rayleigh/Love layer-evaluations,
+// [3]/[4] learned cells used / dropped, [5..10] evaluations by phase
+// (EV_* below)
+constexpr int NCOUNT = 11;
+constexpr int EV_BASE = 5;
+
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
   float betmx;  // largest flattened shear velocity
@@ -482,6 +489,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
   // the chain's state machine lives in shared memory, so the registers go to
   // the secular function: 96 registers, 5 blocks of 128 per SM
   __shared__ ChainState sst[128];
+  __shared__ unsigned long long phase_ev[NPHASE_EV];
+  if (threadIdx.x < NPHASE_EV) phase_ev[threadIdx.x] = 0ull;
+  __syncthreads();
   ChainState& s = sst[threadIdx.x];
   ChainParams P;
   ChainIO io;
@@ -559,11 +569,15 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
     }
     if (__ballot_sync(0xffffffffu, need) == 0u) break;
     if (need) {
+      atomicAdd(&phase_ev[eval_phase(s)], 1ull);
       s.last = secular_fast(V, P.iwave, P.refine, s.omega / s.creq, s.omega);
       s.nevals++;
       s.phase = s.next;
     }
   }
+  __syncthreads();
+  if (threadIdx.x < NPHASE_EV && nevals && phase_ev[threadIdx.x])
+    atomicAdd(nevals + EV_BASE + threadIdx.x, phase_ev[threadIdx.x]);
   unsigned long long e = ev_r + ev_l;
   for (int o = 16; o > 0; o >>= 1) {
     e += __shfl_down_sync(0xffffffffu, e, o);
@@ -713,6 +727,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     atomicAdd(nevals, ev_r);
     atomicAdd(nevals + 1, lay_r);
     atomicAdd(nevals + 2, lay_l);
+    atomicAdd(nevals + EV_BASE + EV_RETRY, ev_r);
   }
 }
 
@@ -1321,7 +1336,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(ctx->chainrule.ensure((size_t)nz * ncol * sizeof(float2)));
   CK(ctx->croot.ensure((size_t)P.nroot * ncol * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)P.nroot * ncol * sizeof(int32_t)));
-  CK(ctx->nevals.ensure(5 * sizeof(unsigned long long)));
+  CK(ctx->nevals.ensure(NCOUNT * sizeof(unsigned long long)));
   if (wantfeat) CK(ctx->nodefeat.ensure((size_t)ncol * FEAT_NODES * sizeof(float4)));
   CK(ctx->depth_d.ensure((size_t)nz * sizeof(float)));
   if (ctx->depth_dev != ctx->depth_d.p) {  // first call after swdk_set_depth (never inside a capture)
@@ -1329,7 +1344,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
     CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
     ctx->depth_dev = ctx->depth_d.p;
   }
-  CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, NCOUNT * sizeof(unsigned long long), st));
   const bool timing = !ctx->capturing;  // stage events and statistics only on eager calls
   if (timing) CK(cudaEventRecord(ctx->ev[0], st));
   ctx->launches = 1;
@@ -1395,7 +1410,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   }
   if (timing) {
     CK(cudaEventRecord(ctx->ev[3], st));
-    CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, NCOUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(ctx->ev[4], st));
     ctx->stats_pending = true;
   }
@@ -1422,6 +1437,7 @@ void collect_stats(swdk_ctx* ctx) {
       t.layer_evals_love += a.layer_evals_love;
       t.proposals_accepted += a.proposals_accepted;
       t.proposals_rejected += a.proposals_rejected;
+      for (int i = 0; i < NPHASE_EV; ++i) t.evals_by_phase[i] += a.evals_by_phase[i];
       t.kernel_launches += a.kernel_launches;
       t.nchains = a.nchains;
       t.nslots = a.nslots;
@@ -1440,6 +1456,7 @@ void collect_stats(swdk_ctx* ctx) {
   ctx->stats.layer_evals_love = (int64_t)ctx->h_nevals[2];
   ctx->stats.proposals_accepted = (int64_t)ctx->h_nevals[3];
   ctx->stats.proposals_rejected = (int64_t)ctx->h_nevals[4];
+  for (int i = 0; i < NPHASE_EV; ++i) ctx->stats.evals_by_phase[i] = (int64_t)ctx->h_nevals[EV_BASE + i];
   cudaEventElapsedTime(&ctx->stats.ms_prep, ctx->ev[0], ctx->ev[1]);
   cudaEventElapsedTime(&ctx->stats.ms_proposal, ctx->ev[1], ctx->ev[5]);
   cudaEventElapsedTime(&ctx->stats.ms_roots, ctx->ev[5], ctx->ev[2]);
@@ -1643,13 +1660,13 @@ int swdk_create(swdk_ctx** out, const swdk_config* cfg) {
   cudaError_t e = cudaSetDevice(ctx->cfg.device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_nevals, 5 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_nevals, NCOUNT * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     fprintf(stderr, "swdk_create: %s\n", cudaGetErrorString(e));
     swdk_destroy(ctx);
     return SWDK_E_CUDA;
   }
-  for (int i = 0; i < 5; ++i) ctx->h_nevals[i] = 0;
+  for (int i = 0; i < NCOUNT; ++i) ctx->h_nevals[i] = 0;
   *out = ctx;
   return SWDK_OK;
 }
@@ -1775,8 +1792,8 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(ctx->croot.ensure((size_t)mode * kmax * nm * sizeof(double)));
   CK(ctx->cstat.ensure((size_t)mode * kmax * nm * sizeof(int32_t)));
   CK(ctx->ierr.ensure(nm * sizeof(int32_t)));
-  CK(ctx->nevals.ensure(5 * sizeof(unsigned long long)));
-  CK(cudaMemsetAsync(ctx->nevals.p, 0, 5 * sizeof(unsigned long long), st));
+  CK(ctx->nevals.ensure(NCOUNT * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(ctx->nevals.p, 0, NCOUNT * sizeof(unsigned long long), st));
   CK(cudaEventRecord(ctx->ev[0], st));
   k_prep_layers<<<(nmodel + 127) / 128, 128, 0, st>>>(nmodel, nlayer, d_in, d_in + nin, d_in + 2 * nin,
                                                        d_in + 3 * nin, iflsph, ctx->layR.as<float4>(),
@@ -1800,7 +1817,7 @@ int swdk_surfdisp96_batch(swdk_ctx* ctx, int nmodel, int nlayer, const float* th
   CK(cudaMemcpyAsync(tmp.data(), ctx->croot.as<double>() + (size_t)(mode - 1) * kmax * nm,
                      (size_t)kmax * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (ierr) CK(cudaMemcpyAsync(ierr, ctx->ierr.p, nm * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, NCOUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(ctx->ev[4], st));
   ctx->stats_pending = true;
   CK(cudaStreamSynchronize(st));

@@ -666,6 +666,13 @@ SWDK_HD double scan_grid(double c1, int j) {
   return c;
 }
 
+// Evaluation phases counted by the root kernels' statistics: the getsol
+// scan of a mode's first period, the scan of later periods (and of group
+// passes and dropped proposals), the learned cell's two ends, the walk from
+// a learned cell, the refinement, and the single-period retries.
+constexpr int EV_SCAN_FIRST = 0, EV_SCAN = 1, EV_CELL = 2, EV_WALK = 3, EV_REFINE = 4, EV_RETRY = 5;
+constexpr int NPHASE_EV = 6;
+
 // request a secular-function value at c; continue with phase nxt
 #define SWDK_REQ(cv, nxt) do { s.creq = (cv); s.next = (nxt); return true; } while (0)
 
@@ -1043,6 +1050,20 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
   }
 }
 #undef SWDK_REQ
+
+// phase of the evaluation a chain has just requested (s.next set)
+SWDK_HD int eval_phase(const ChainState& s) {
+  if (s.sub) return EV_RETRY;
+  switch (s.next) {
+    case PH_GS_FIRST:
+    case PH_SCAN_GOT: return (s.k == 1 && s.gpass == 0) ? EV_SCAN_FIRST : EV_SCAN;
+    case PH_PROP_HI:
+    case PH_PROP_CHECK: return EV_CELL;
+    case PH_PROP_DOWN_GOT:
+    case PH_PROP_C1_GOT: return EV_WALK;
+    default: return EV_REFINE;
+  }
+}
 
 // Runs a whole chain.  io.cb must have KMAX_CHAIN + 24 doubles (Neville x/y).
 // On the device every lane of the warp must call this (active = false for

@@ -42,7 +42,9 @@ class Stats(C.Structure):
                 ("nchains", C.c_int32), ("nslots", C.c_int32),
                 ("ms_prep", C.c_float), ("ms_roots", C.c_float), ("ms_eigen", C.c_float),
                 ("proposals_accepted", C.c_int64), ("proposals_rejected", C.c_int64), ("ms_proposal", C.c_float),
-                ("kernel_launches", C.c_int32)]
+                ("kernel_launches", C.c_int32), ("evals_by_phase", C.c_int64 * 6)]
+
+EVAL_PHASES = ("scan_first_period", "scan", "learned_cell", "walk", "refine", "retry")
 
 
 _LIB = None
@@ -300,4 +302,5 @@ class Engine:
                     layer_evals_love=s.layer_evals_love, nchains=s.nchains, nslots=s.nslots, ms_prep=s.ms_prep,
                     ms_roots=s.ms_roots, ms_eigen=s.ms_eigen, proposals_accepted=s.proposals_accepted,
                     proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal,
-                    kernel_launches=s.kernel_launches)
+                    kernel_launches=s.kernel_launches,
+                    evals_by_phase=dict(zip(EVAL_PHASES, [int(x) for x in s.evals_by_phase])))

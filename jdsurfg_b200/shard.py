@@ -22,7 +22,9 @@ column gather provides.
 The per-block computations are injected (`compute`, `march`), so the host
 logic -- block bounds, padding, gather and reassembly -- is tested on CPU
 with gloo ranks; on GPUs the defaults compute with the rank's Engine and
-FMST.
+FMST.  The *_device methods keep everything on the GPU: the block is
+computed from the device-resident model and the maps are gathered by one
+NCCL all-gather into device tensors.
 """
 import numpy as np
 
@@ -109,6 +111,79 @@ class ShardedSurfTime:
         r = self._local("kernel", vs, vp, rho, c0, c1)
         vc, vout, st = self._gather_maps(r["vc"], r["vout"], r["status"], ncol)
         return dict(vc=vc, vout=vout, status=st, kernel=r["kernel"], columns=(c0, c1))
+
+    # -- device-resident path: maps gathered by the collective on the GPU ----
+    def _local_device(self, path, vs, vp, rho, c0, c1, stream=None):
+        """This rank's column block [c0, c1) of a device-resident model (nz,
+        ncol): vc, vout, status (kmax, c1-c0) and, for path "kernel", the
+        kernel block (kmax, nz, c1-c0), as tensors on vs's device."""
+        import torch
+        blk = lambda a: None if a is None else a[:, c0:c1].contiguous()
+        vs_b, vp_b, rho_b = blk(vs), blk(vp), blk(rho)
+        if self.compute is not None:
+            np_ = lambda a: None if a is None else a.cpu().numpy()
+            r = self.compute(path, np_(vs_b), np_(vp_b), np_(rho_b))
+            out = {k: torch.as_tensor(r[k], device=vs.device) for k in ("vc", "vout", "status")}
+            if path == "kernel":
+                out["kernel"] = torch.as_tensor(r["kernel"], device=vs.device)
+            return out
+        nz, n = vs_b.shape
+        kmax = self.engine.kmax
+        dev = vs.device
+        vc = torch.empty((kmax, n), dtype=torch.float64, device=dev)
+        vout = torch.empty_like(vc)
+        st = torch.empty((kmax, n), dtype=torch.int32, device=dev)
+        if path == "kernel":
+            ker = torch.empty((kmax, nz, n), dtype=torch.float64, device=dev)
+            self.engine.get_1d_kernel_device(n, 1, nz, vs_b, vp_b, rho_b, vc, vout, ker, st, stream=stream)
+            return dict(vc=vc, vout=vout, status=st, kernel=ker)
+        self.engine.get_2d_map_device(n, 1, nz, vs_b, vp_b, rho_b, vc, vout, st, stream=stream)
+        return dict(vc=vc, vout=vout, status=st)
+
+    def _gather_maps_device(self, vc, vout, st, ncol):
+        """All-gather the (kmax, block) maps of every rank into (kmax, ncol)
+        tensors on this rank's device: one collective over a (3, kmax, bmax)
+        FP64 pack per rank (status as exact small integers), no host copy."""
+        import torch
+        import torch.distributed as dist
+        kmax, n = vc.shape
+        if self.world == 1 and not dist.is_initialized():  # one process, nothing to exchange
+            return vc, vout, st
+        bmax = -(-ncol // self.world)  # the largest block (allocate_tasks)
+        pack = torch.zeros((3, kmax, bmax), dtype=torch.float64, device=vc.device)
+        pack[0, :, :n] = vc
+        pack[1, :, :n] = vout
+        pack[2, :, :n] = st.to(torch.float64)
+        if dist.get_backend(self.group) == "nccl":
+            out = torch.empty((self.world, 3, kmax, bmax), dtype=torch.float64, device=vc.device)
+            dist.all_gather_into_tensor(out, pack, group=self.group)
+            parts = list(out.unbind(0))
+        else:
+            parts = [torch.empty_like(pack) for _ in range(self.world)]
+            dist.all_gather(parts, pack, group=self.group)
+        full = torch.empty((3, kmax, ncol), dtype=torch.float64, device=vc.device)
+        for r, o in enumerate(parts):
+            c0, c1 = column_block(ncol, self.world, r)
+            full[:, :, c0:c1] = o[:, :, :c1 - c0]
+        return full[0], full[1], full[2].to(torch.int32)
+
+    def get_1d_kernel_device(self, vs, vp=None, rho=None, stream=None):
+        """get_1d_kernel of a device-resident model (nz, ncol) tensors, each
+        rank computing its column block: the full vc/vout/status maps on
+        every rank's device, the kernel block of this rank's columns."""
+        ncol = vs.shape[1]
+        c0, c1 = column_block(ncol, self.world, self.rank)
+        r = self._local_device("kernel", vs, vp, rho, c0, c1, stream)
+        vc, vout, st = self._gather_maps_device(r["vc"], r["vout"], r["status"], ncol)
+        return dict(vc=vc, vout=vout, status=st, kernel=r["kernel"], columns=(c0, c1))
+
+    def get_2d_map_device(self, vs, vp=None, rho=None, stream=None):
+        """get_2d_map of a device-resident model: full maps on every rank."""
+        ncol = vs.shape[1]
+        c0, c1 = column_block(ncol, self.world, self.rank)
+        r = self._local_device("map", vs, vp, rho, c0, c1, stream)
+        vc, vout, st = self._gather_maps_device(r["vc"], r["vout"], r["status"], ncol)
+        return dict(vc=vc, vout=vout, status=st)
 
     # -- fast marching over a block of the station pairs ---------------------
     def _march(self, sub, vc, vout, want_fdm):

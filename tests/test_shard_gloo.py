@@ -48,8 +48,15 @@ def _rank_main(rank, world, port, out_dir):
     sh = ShardedSurfTime(rank, world, compute=compute)
     m = sh.get_2d_map(case["vs"], case["vp"], case["rho"])
     k = sh.get_1d_kernel(case["vs"], case["vp"], case["rho"])
+    # the tensor path (device tensors on GPUs; CPU tensors over gloo here)
+    import torch
+    t = lambda a: None if a is None else torch.from_numpy(a)
+    kd = sh.get_1d_kernel_device(t(case["vs"]), t(case["vp"]), t(case["rho"]))
+    md = sh.get_2d_map_device(t(case["vs"]), t(case["vp"]), t(case["rho"]))
     np.savez(os.path.join(out_dir, f"rank{rank}.npz"), vc=m["vc"], vout=m["vout"], status=m["status"],
-             kvc=k["vc"], kernel=k["kernel"], c0=k["columns"][0], c1=k["columns"][1])
+             kvc=k["vc"], kernel=k["kernel"], c0=k["columns"][0], c1=k["columns"][1],
+             dvc=kd["vc"].numpy(), dvout=kd["vout"].numpy(), dstatus=kd["status"].numpy(),
+             dkernel=kd["kernel"].numpy(), mvc=md["vc"].numpy(), mvout=md["vout"].numpy())
     dist.barrier()
     dist.destroy_process_group()
 
@@ -77,6 +84,10 @@ def test_sharded_maps_equal_single_process(tmp_path):
         c0, c1 = int(d["c0"]), int(d["c1"])
         assert (c0, c1) == column_block(15, world, r)
         assert np.array_equal(d["kernel"], full_ker["kernel"][:, :, c0:c1])
+        assert np.array_equal(d["dvc"], full_ker["vc"]) and np.array_equal(d["dvout"], full_ker["vout"])
+        assert np.array_equal(d["dstatus"], full_ker["status"])
+        assert np.array_equal(d["dkernel"], full_ker["kernel"][:, :, c0:c1])
+        assert np.array_equal(d["mvc"], full_map["vc"]) and np.array_equal(d["mvout"], full_map["vout"])
 
 
 def _rank_pairs(rank, world, port, out_dir):
