@@ -42,6 +42,17 @@ UNIT = "column-period-modes/s"
 # divisions, square roots and exp/sin/cos are not counted.
 F_SEC_RAYLEIGH = 161
 F_SEC_LOVE = 19
+# Algorithmic FP64 flops per layer of one eigenfunction pass (FMA = 2), hand
+# count of the formulation in jdsurfg_b200/csrc/swdk_eigen.cuh for a solid
+# layer with real vertical wavenumbers: Rayleigh = up sweep (varsv terms 22,
+# dnka product 139, normalisation 9) + down sweep (varsv terms 22, hska
+# product 78, normalisation and exponents 9, svfunc eigenfunction 25, energy
+# integrals and getmat 354, _ParamConvert/chain-rule sink 17); Love = up 24 +
+# shfunc 3 + energy and sink 105.  Divisions, square roots and exp/sin/cos
+# are not counted.  A phase slot is one pass, a group slot three
+# (sregnpu/slegnpu at T, T(1+0.005), T(1-0.005)).
+F_EIG_RAYLEIGH = 675
+F_EIG_LOVE = 132
 # proposal network multiply-adds per row: 320x256 + 3 x 256x256 + 256x64
 MLP_MACS_PER_ROW = 320 * 256 + 3 * 256 * 256 + 256 * 64
 
@@ -722,6 +733,28 @@ def main():
                 "work": "plain-method secular evaluations x layers x flops per layer (the learned "
                         "path's saved evaluations show up as a shorter duration)",
                 "share_of_step": roots_ms / ms if ms else None}
+    # the eigen stage (k_eigen): passes x layers x F_EIG over its measured
+    # stage time, and the write-out bandwidth of its outputs
+    from jdsurfg_b200 import synth as _synth
+    passes = {"rayleigh": 0, "love": 0}
+    for w, tab in enumerate(case["tables"]):
+        if tab is None:
+            continue
+        nslot = _synth.kmax_of([tab if i == w else None for i in range(4)])
+        passes["rayleigh" if w < 2 else "love"] += nslot * (3 if w in (1, 3) else 1)
+    L = 4 * nz - 3
+    eig_flops = ncol * L * (passes["rayleigh"] * F_EIG_RAYLEIGH + passes["love"] * F_EIG_LOVE) * args.steps
+    eig_s = acc["ms_eigen"] * 1e-3
+    out_bytes = (ncol * kmax * (nz + 2) * 8 + ncol * kmax * 4) * args.steps  # kernel, vc, vout (f64), status
+    if eig_s > 0:
+        ach_e = eig_flops / eig_s / 1e12
+        roofline["eigen"] = {"kernel": "k_eigen", "bound": "fp64", "achieved": ach_e, "peak": peak, "unit": "TFLOP/s",
+                             "frac": ach_e / peak if peak else None, "traffic": None,
+                             "flops_per_layer_pass": {"rayleigh": F_EIG_RAYLEIGH, "love": F_EIG_LOVE},
+                             "passes_per_column": passes, "layers": L,
+                             "writeout_gbs": out_bytes / eig_s / 1e9,
+                             "writeout_bytes_per_step": out_bytes // args.steps,
+                             "share_of_step": acc["ms_eigen"] / ms}
     if args.proposal == "learned" and acc["ms_proposal"] > 0:
         peaks = {}
         try:

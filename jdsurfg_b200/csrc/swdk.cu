@@ -48,6 +48,7 @@ constexpr int EV_BASE = 5;
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
   float betmx;  // largest flattened shear velocity
+  float htot;   // total flattened thickness of the finite layers
   int L;        // sublayers incl. half-space
   int llw;      // 2 if the top layer is fluid
   int nw;       // leading fluid grid nodes
@@ -184,6 +185,9 @@ __device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, cons
   cc1 = fmul(0.90f, cc1);
   ci.cc = (double)cc1;
   ci.betmx = betmx;
+  float ht = 0.0f;
+  for (int i = 0; i < L - 1; ++i) ht += d[i];
+  ci.htot = ht;
 }
 
 __device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
@@ -395,6 +399,9 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   V.col = ccol;
   V.L = ci.L;
   V.llw = ci.llw;
+  V.trunc = 0;
+  V.htot = ci.htot;
+  V.bmax = ci.betmx;
   ChainParams P;
   P.t = periods + cd.t_off;
   P.kmax = cd.np;
@@ -525,6 +532,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         V.col = col;
         V.L = ci.L;
         V.llw = ci.llw;
+        V.trunc = (refine == 1);
+        V.htot = ci.htot;
+        V.bmax = ci.betmx;
         P.t = periods + cd.t_off;
         P.kmax = cd.np;
         P.nmode = cd.nmode;
@@ -681,6 +691,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     V.col = col;
     V.L = ci.L;
     V.llw = ci.llw;
+    V.trunc = (refine == 1);
+    V.htot = ci.htot;
+    V.bmax = ci.betmx;
     P.t = periods + cd.t_off;
     P.kmax = cd.np;
     P.nmode = cd.nmode;

@@ -112,6 +112,8 @@ struct LayerView {
   int ncol, col;
   int L;    // layers including the half-space
   int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
+  int trunc;          // secular_fast may cut the depth (secular_depth)
+  float htot, bmax;   // total finite-layer thickness and largest shear velocity
   SWDK_HD size_t idx(int m) const { return (size_t)(L - 1 - m) * ncol + col; }
   SWDK_HD float4 get(int m) const {  // m: reference (top-down, 0-based) index
     return lay[idx(m)];
@@ -397,13 +399,45 @@ SWDK_HD void apply_dunkin(const LayerCoef& k, double wvno2, double& e0, double& 
   e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
 }
 
+// Depth cut of one secular evaluation.  The period equation's value is the
+// propagated compound (Rayleigh) or Haskell (Love) vector at the surface;
+// in an evanescent layer its parts below the dominant one shrink by
+// exp(-2 Re(r_beta) d) relative to it, so below the depth where
+// sum(Re(r_beta) d) from the top exceeds SEC_TRUNC_Q the deeper structure
+// changes the value by less than exp(-2 SEC_TRUNC_Q) relative, far below
+// rounding: the evaluation then starts from the next layer as its
+// half-space.  Returns the index of the layer used as the half-space (L-1:
+// no cut).  A bound k H sqrt(1 - c^2/bmax^2) on the whole column's decay
+// skips the search where no cut is possible (long periods).
+constexpr double SEC_TRUNC_Q = 30.0;
+
+SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
+  if (!V.trunc) return V.L - 1;
+  const double c = omega / wvno, bm = V.bmax;
+  const double u = 1.0 - (c / bm) * (c / bm);
+  if (!(u > 0.0) || wvno * (double)V.htot * sqrt(u) <= SEC_TRUNC_Q) return V.L - 1;
+  const double wvno2 = wvno * wvno;
+  double cum = 0.0;
+  for (int m = V.llw - 1; m < V.L - 2; ++m) {
+    const float4 ly = V.lay[V.idx(m)];
+    if (ly.z > 0.0f) {
+      const double xkb = omega * recip((double)ly.z);
+      const double x2 = wvno2 - xkb * xkb;
+      if (x2 > 0.0) cum += x2 * rsqrt(x2) * (double)ly.x;
+    }
+    if (cum > SEC_TRUNC_Q) return m + 1;
+  }
+  return V.L - 1;
+}
+
 template <int NORM>
 SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   double omega = omga;
   if (omega < 1.0e-4) omega = 1.0e-4;
   const double wvno2 = wvno * wvno;
   const double iom = 1.0 / omega;
-  const float4 h = V.lay[V.idx(V.L - 1)];
+  const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
+  const float4 h = V.lay[V.idx(hs)];
   double xka = omega * recip((double)h.y), xkb = omega * recip((double)h.z);
   const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
   const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
@@ -420,8 +454,8 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   const int mlo = V.llw - 1;
   int since = 0;
   // the next layer's float4 is loaded one layer ahead of its use
-  float4 ly = V.lay[V.idx(V.L - 2 >= mlo ? V.L - 2 : mlo)];
-  for (int m = V.L - 2; m >= mlo; --m) {
+  float4 ly = V.lay[V.idx(hs - 1 >= mlo ? hs - 1 : mlo)];
+  for (int m = hs - 1; m >= mlo; --m) {
     const float4 cur_ly = ly;
     if (m > mlo) ly = V.lay[V.idx(m - 1)];
     const LayerCoef cur = layer_coef(cur_ly, wvno, wvno2, omega, iom);
@@ -466,7 +500,8 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
 // dltar1 with 1/b and 1/(rho b^2) from recip()
 template <int NORM>
 SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
-  float4 h = V.lay[V.idx(V.L - 1)];
+  const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
+  float4 h = V.lay[V.idx(hs)];
   double beta1 = h.z, rho1 = h.w;
   double xkb = omega * recip(beta1);
   double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
@@ -475,8 +510,8 @@ SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
   int since = 0;
   const int mlo = V.llw - 1;
   // the next layer's float4 is loaded one layer ahead of its use
-  float4 nx = V.lay[V.idx(V.L - 2 >= mlo ? V.L - 2 : mlo)];
-  for (int m = V.L - 2; m >= mlo; --m) {
+  float4 nx = V.lay[V.idx(hs - 1 >= mlo ? hs - 1 : mlo)];
+  for (int m = hs - 1; m >= mlo; --m) {
     const float4 ly = nx;
     if (m > mlo) nx = V.lay[V.idx(m - 1)];
     beta1 = ly.z;

@@ -506,15 +506,44 @@ SWDK_HD Eig4 eigen_at(const double* cd, const double* vv, double ext, double if1
   return u;
 }
 
+// Depth truncation of a pass.  Below the layer where the S-wave evanescent
+// decay sum(Re r_beta d) accumulated from the top exceeds trunc_q, the
+// eigenfunctions are below exp(-trunc_q) of their surface amplitude and the
+// layers' energy integrals and kernels below exp(-2 trunc_q) of the largest:
+// the pass then treats the next layer as the half-space (the up pass's start
+// vector there converges to the same surface value to a relative
+// exp(-2 trunc_q), the compound vector's subdominant parts decaying by
+// exp(-2 q) per evanescent layer) and the layers below it get zero kernels.
+// Returns the number of layers the pass uses (L when nothing is cut;
+// trunc_q <= 0 disables the cut).
+template <class Layer>
+SWDK_HD int pass_layers(const Layer* lay, int L, double k2, double om2, double trunc_q) {
+  if (!(trunc_q > 0.0)) return L;
+  double cum = 0.0;
+  for (int m = 0; m < L - 2; ++m) {
+    const Layer& y = lay[m];
+    if (y.zb > 0.0) {
+      const double x2s = k2 - om2 * y.ib2;
+      if (x2s > 0.0) cum += x2s * rsqrt(x2s) * y.d;
+    }
+    if (cum > trunc_q) return m + 2;  // lay[m+1] becomes the half-space
+  }
+  return L;
+}
+
+constexpr double EIG_TRUNC_Q = 40.0;
+
 // One Rayleigh pass (sregn96's svfunc + energy) at (omega, wvno) over the
-// column's layer records lay[0..L-1] (top-down, lay[L-1] the half-space).
-// scr: 6 doubles per layer (up-pass compound vector and its exponent).
-// Returns ugr (flat) and norm = ugr*sumi0; the raw layer kernels go to the
-// sink as the top-down sweep produces them.
+// column's layer records lay[0..L-1] (top-down, lay[L-1] the half-space),
+// depth-truncated by pass_layers.  scr: 6 doubles per layer (up-pass
+// compound vector and its exponent).  Returns ugr (flat) and
+// norm = ugr*sumi0; the raw layer kernels go to the sink as the top-down
+// sweep produces them.
 template <class Sink>
-SWDK_HDI void rayleigh_pass(const RayLayer* lay, int L, double omega, double wvno, double* scr, double& ugr,
-                            double& norm, const Sink& sink) {
+SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double wvno, double* scr, double& ugr,
+                            double& norm, const Sink& sink, double trunc_q = EIG_TRUNC_Q) {
   const SlotK s = slot_consts(omega, wvno);
+  const int L = pass_layers(lay, Lfull, s.k2, s.om2, trunc_q);
   // ---- up (sregn96.f90:401-489) ----
   {
     const RayLayer& y = lay[L - 1];
@@ -591,9 +620,10 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int L, double omega, double wvn
 // 3 doubles per layer (uu, tt, exl).  Returns ugr and the normaliser sumi1.
 // ---------------------------------------------------------------------------
 template <class Sink>
-SWDK_HDI void love_pass(const LoveLayer* lay, int L, double omega, double wvno, double* scr, double& ugr,
-                        double& norm, const Sink& sink) {
+SWDK_HDI void love_pass(const LoveLayer* lay, int Lfull, double omega, double wvno, double* scr, double& ugr,
+                        double& norm, const Sink& sink, double trunc_q = EIG_TRUNC_Q) {
   const double wvno2 = wvno * wvno, om2 = omega * omega, ik = 1.0 / wvno, ik2 = ik * ik;
+  const int L = pass_layers(lay, Lfull, wvno2, om2, trunc_q);
   // ---- up (slegn96.f90:372-445) ----
   {
     const LoveLayer& y = lay[L - 1];

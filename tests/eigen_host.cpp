@@ -27,10 +27,11 @@ struct LayerSink {
 // wave 1 Love, 2 Rayleigh.  The layer model (top-down, last = half-space)
 // becomes the pass's model as the eigen kernel builds it: flat, or with the
 // earth-flattening transform of bldsph (ar = 6371) when sphere != 0.
-// Returns the flat group velocity, the normaliser and per-layer raw kernels.
+// Returns the flat group velocity, the normaliser and per-layer raw kernels;
+// trunc_q is the pass's depth-truncation threshold (0: every layer).
 extern "C" int eig_host_pass(int wave, int L, const float* thk, const float* vp, const float* vs, const float* rho,
-                             int sphere, double t, double c, double* ugr, double* norm, double* da, double* db,
-                             double* dr) {
+                             int sphere, double t, double c, double trunc_q, double* ugr, double* norm, double* da,
+                             double* db, double* dr) {
   if (L < 2 || L > LMAX) return -1;
   std::vector<double> drs(L), zd(L), za(L), zb(L), zr(L), vtp(L), rtp(L);
   double acc = 0.0;
@@ -68,11 +69,11 @@ extern "C" int eig_host_pass(int wave, int L, const float* thk, const float* vp,
   if (wave == 1) {
     std::vector<LoveLayer> lay(L);
     for (int i = 0; i < L; ++i) make_love_layer(lay[i], zd[i], zb[i], zr[i], vtp[i], rtp[i]);
-    love_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink);
+    love_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink, trunc_q);
   } else {
     std::vector<RayLayer> lay(L);
     for (int i = 0; i < L; ++i) make_ray_layer(lay[i], zd[i], za[i], zb[i], zr[i], vtp[i], rtp[i]);
-    rayleigh_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink);
+    rayleigh_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink, trunc_q);
   }
   return 0;
 }

@@ -42,14 +42,14 @@ def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def host_pass(wave, thk, vp, vs, rho, t, c, sphere=0):
+def host_pass(wave, thk, vp, vs, rho, t, c, sphere=0, trunc_q=0.0):
     f = lambda a: np.ascontiguousarray(a, np.float32)
     thk, vp, vs, rho = f(thk), f(vp), f(vs), f(rho)
     L = len(thk)
     ugr, norm = C.c_double(0), C.c_double(0)
     da, db, dr = np.zeros(L), np.zeros(L), np.zeros(L)
     rc = _lib().eig_host_pass(wave, L, _p(thk), _p(vp), _p(vs), _p(rho), sphere, C.c_double(t), C.c_double(c),
-                              C.byref(ugr), C.byref(norm), _p(da), _p(db), _p(dr))
+                              C.c_double(trunc_q), C.byref(ugr), C.byref(norm), _p(da), _p(db), _p(dr))
     assert rc == 0
     return ugr.value, norm.value, da, db, dr
 
@@ -104,3 +104,25 @@ def test_eigen_passes_match_oracle_flat(wave):
                 assert eu <= TOL_U, (mi, mode, t, c, eu)
     assert n >= 40
     print(f"{n} passes: max kernel rel err {worst_k:.2e}, max |dU|/U {worst_u:.2e}")
+
+
+@pytest.mark.parametrize("wave", [2, 1], ids=["rayleigh", "love"])
+def test_depth_truncation_changes_nothing_measurable(wave):
+    """The device passes cut the layers below exp(-40) of the S-wave decay
+    from the top (swdk_eigen.cuh pass_layers): against the full-depth pass,
+    group velocity and kernels agree to rounding (1e-12), and short periods cut
+    layers."""
+    worst = 0.0
+    cut = 0
+    for th, a, b, r in _models()[:3]:
+        cg, _, _ = O.surfdisp96(th, a, b, r, 1, wave, 1, 0, PERIODS, refine=1, rtol=1e-12, sngl=0)
+        for t, c in zip(PERIODS, cg):
+            u0, n0, a0, b0, r0 = host_pass(wave, th, a, b, r, t, c, sphere=1, trunc_q=0.0)
+            u1, n1, a1, b1, r1 = host_pass(wave, th, a, b, r, t, c, sphere=1, trunc_q=40.0)
+            k0 = np.concatenate([a0, b0, r0]) / n0
+            k1 = np.concatenate([a1, b1, r1]) / n1
+            worst = max(worst, np.abs(k1 - k0).max() / np.abs(k0).max(), abs(u1 - u0) / abs(u0))
+            cut += int((np.concatenate([a1, b1, r1]) == 0).sum() > (np.concatenate([a0, b0, r0]) == 0).sum())
+    print(f"truncated vs full: max rel diff {worst:.2e}, {cut} passes cut")
+    assert worst <= 1e-12
+    assert cut >= 3
