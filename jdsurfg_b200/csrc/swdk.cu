@@ -781,18 +781,19 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
 // get_1d_kernel, 1 get_2d_map): one launch per slot group, so each kernel
 // carries only the passes it runs (the all-in-one kernel missed in the
 // instruction cache)
+// one block's work: column col of a model with ncol columns (its arrays
+// passed at the model's offsets)
 template <int WT, int PATH>
-__global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
-                                               const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
-                                               const SlotDesc* __restrict__ slots, int g0, int gn,
-                                               const double* __restrict__ croot, const int32_t* __restrict__ cstat,
-                                               int sphere, double* __restrict__ vc, double* __restrict__ vout,
-                                               double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
+__device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+                                             const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
+                                             const SlotDesc* __restrict__ slots, int g0, int gn,
+                                             const double* __restrict__ croot, const int32_t* __restrict__ cstat,
+                                             int sphere, double* __restrict__ vc, double* __restrict__ vout,
+                                             double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
   constexpr int path = PATH;
   constexpr bool love = WT >= 2;
   using Layer = typename std::conditional<love, LoveLayer, RayLayer>::type;
   extern __shared__ double sm[];
-  const int col = blockIdx.x;
   const ColInfo ci = info[col];
   const int L = ci.L;
   Layer* lay = reinterpret_cast<Layer*>(sm);
@@ -957,6 +958,17 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
     }
     }  // get_1d_kernel
   }
+}
+
+template <int WT, int PATH>
+__global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_EIGEN_MINB) k_eigen(int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+                                               const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
+                                               const SlotDesc* __restrict__ slots, int g0, int gn,
+                                               const double* __restrict__ croot, const int32_t* __restrict__ cstat,
+                                               int sphere, double* __restrict__ vc, double* __restrict__ vout,
+                                               double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
+  eigen_column<WT, PATH>(blockIdx.x, ncol, nz, Lmax, lay0, info, chainrule, slots, g0, gn, croot, cstat, sphere, vc,
+                         vout, kernel, status, ldo);
 }
 
 // ---------------------------------------------------------------------------
