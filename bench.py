@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--split-cols", type=int, default=0,
                     help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
     ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
+    ap.add_argument("--uneven-mode", default="ragged", choices=["ragged", "branches"],
+                    help="uneven workload: one ragged launch per kernel, or a graph branch per model")
     ap.add_argument("--sharded", action="store_true",
                     help="strong scaling: ONE model split by columns over the ranks (allocate_tasks), each step "
                          "computing the rank's block and all-gathering the vc/vout/status maps with NCCL")
@@ -423,11 +425,15 @@ def run_uneven(args, torch, dev, rank, world, pg):
     from jdsurfg_b200 import synth
     from jdsurfg_b200.batch import UnevenBatch
     cases = synth.make_uneven_batch(48, seed=5150 + rank)
-    B = UnevenBatch(cases, learned=(args.proposal == "learned"))
+    B = UnevenBatch(cases, learned=(args.proposal == "learned"), mode=args.uneven_mode)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     B.capture()
+    probe = None
+    if args.uneven_mode == "ragged":
+        B.run()  # one eager pass: stage times and evaluation counts
+        probe = B.stats()
     for _ in range(args.warmup):
         flush.fill_(1)
         B.launch(stream.cuda_stream)
@@ -450,8 +456,22 @@ def run_uneven(args, torch, dev, rank, world, pg):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
     units = B.units
-    launches = sum(e.stats()["kernel_launches"] for e in B.engines)  # per model, from the eager pass
+    if probe is not None:
+        launches = probe["kernel_launches"]
+    else:
+        launches = sum(e.stats()["kernel_launches"] for e in B.engines)  # per model, from the eager pass
     kb = sum(c["nx"] * c["ny"] * c["nz"] * e.kmax * 8 for c, e in zip(cases, B.engines))
+    roofline = None
+    if probe is not None and probe["ms_roots"] > 0:
+        peak = fp64_peak_tflops(torch, dev)
+        fl = probe["layer_evals_rayleigh"] * F_SEC_RAYLEIGH + probe["layer_evals_love"] * F_SEC_LOVE
+        ach = fl / (probe["ms_roots"] * 1e-3) / 1e12
+        roofline = {"kernel": "k_roots_queue+k_retry (one ragged launch each)", "bound": "fp64", "achieved": ach,
+                    "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                    "work": "secular evaluations done (learned path) x layers x flops per layer",
+                    "peak_source": "measured in this run: cuBLAS float64 GEMM 8192^3",
+                    "stage_ms": {k: probe[k] for k in ("ms_prep", "ms_proposal", "ms_roots", "ms_eigen")},
+                    "evals_per_slot_by_phase": {k: v / units for k, v in probe["evals_by_phase"].items()}}
     if rank == 0:
         line = {"metric": METRIC, "value": world * units / (ms / args.steps * 1e-3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -459,9 +479,13 @@ def run_uneven(args, torch, dev, rank, world, pg):
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_uneven_batch)",
                 "config": {"workload": "uneven", "what": WORKLOAD_TEXT["uneven"], "models": len(cases),
                            "slots_per_step": units, "kernel_bytes": kb, "proposal": args.proposal,
-                           "timed_as": "one CUDA graph launch per step (a branch per model)",
+                           "timed_as": ("one CUDA graph launch per step: per-model column preparation and "
+                                        "proposals, one persistent root search over every (model, chain, column), "
+                                        "one retry launch, one eigen launch per wave type over every (model, column)")
+                           if args.uneven_mode == "ragged" else
+                           "one CUDA graph launch per step (a branch per model)",
                            "l2": "flushed between steps (256 MiB write)"},
-                "clocks": clk, "e2e": None, "gpu_launches": launches * args.steps, "roofline": None,
+                "clocks": clk, "e2e": None, "gpu_launches": launches * args.steps, "roofline": roofline,
                 "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     B.close()

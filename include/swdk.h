@@ -297,6 +297,28 @@ int swdk_batch_graph_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls
 int swdk_batch_graph_launch(swdk_graph* graph, void* stream);
 void swdk_batch_graph_destroy(swdk_graph* graph);
 
+/* Ragged batch: the models of one inversion iteration (each context with
+ * its own period tables and depth vector, each call with its own grid and
+ * device buffers, as for swdk_batch_graph_create) computed by ONE
+ * persistent root-search launch over every (model, chain, column), one
+ * retry launch and one eigen launch per wave type over every (model,
+ * column), after each model's column preparation and proposals.  Every call
+ * has the same path and every context the same device, refine, rtol, sngl
+ * and sphere.  The object keeps its own device buffers (layer models, roots)
+ * and a graph of one pass.  New (uneven batches); no reference counterpart:
+ * the reference runs get_1d_kernel model by model (SurfaceWave.cpp:458-502).
+ *   swdk_ragged_run    : one pass enqueued on stream (NULL: the object's own
+ *                        stream, waited for), statistics by swdk_ragged_stats;
+ *   swdk_ragged_launch : the pass as a CUDA graph (captured on the first
+ *                        call after one eager pass); inputs may change in
+ *                        place between launches. */
+typedef struct swdk_ragged swdk_ragged;
+int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swdk_ragged** out);
+int swdk_ragged_run(swdk_ragged* batch, void* stream);
+int swdk_ragged_launch(swdk_ragged* batch, void* stream);
+int swdk_ragged_stats(swdk_ragged* batch, swdk_stats* out);
+void swdk_ragged_destroy(swdk_ragged* batch);
+
 /* Autotuner of the persistent root-search kernel: times the root search on
  * the given device model for 1..k resident blocks per SM (k = occupancy
  * limit) and one oversubscribed grid, keeps the fastest in the context and

@@ -1,10 +1,17 @@
 """Uneven batches: many independent models (different grids, depth vectors,
 period tables, wave types and modes) computed by one CUDA-graph launch.
 
-Each model keeps its own Engine (plans and device buffers); the graph forks
-one branch per model off a main stream (swdk_batch_graph_create), so small
-models run side by side on the GPU instead of one after another.  The
-learned proposal networks are loaded once and shared by all models.
+Each model keeps its own Engine (period tables, depth vector, plans).  Two
+ways to run them:
+
+* "ragged" (default, swdk_ragged_*): every model's column preparation and
+  proposals, then ONE persistent root-search launch over all (model, chain,
+  column) items, one retry launch and one eigen launch per wave type over
+  all (model, column) blocks, captured as one graph;
+* "branches" (swdk_batch_graph_create): the graph forks one branch of each
+  model's own pipeline off a main stream, so models run side by side.
+
+The learned proposal networks are loaded once and shared by all models.
 """
 import ctypes as C
 
@@ -14,12 +21,16 @@ from .engine import Call, Engine, SwdkError, lib
 
 
 class UnevenBatch:
-    def __init__(self, cases, device=0, learned=True, path="kernel"):
+    def __init__(self, cases, device=0, learned=True, path="kernel", mode="ragged"):
         import torch
         from . import learn
+        if mode not in ("ragged", "branches"):
+            raise ValueError(mode)
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.path = path
+        self.mode = mode
+        self.ragged = None
         self.cases = cases
         self.engines, self.bufs = [], []
         self.nets = None
@@ -57,7 +68,37 @@ class UnevenBatch:
         return Call(0 if self.path == "kernel" else 1, c["nx"], c["ny"], c["nz"], p(b["vs"]), p(b["vp"]),
                     p(b["rho"]), p(b["vc"]), p(b["vout"]), p(b["ker"]), p(b["st"]))
 
+    def _ragged(self):
+        if self.ragged is None:
+            n = len(self.engines)
+            calls = (Call * n)(*[self._call(i) for i in range(n)])
+            ctxs = (C.c_void_p * n)(*[e._h.value for e in self.engines])
+            r = C.c_void_p()
+            rc = lib().swdk_ragged_create(n, ctxs, calls, C.byref(r))
+            if rc != 0:
+                raise SwdkError(f"swdk_ragged_create failed ({rc}): "
+                                f"{lib().swdk_last_error(self.engines[0]._h).decode()}")
+            self.ragged = r
+        return self.ragged
+
+    def run(self, stream=None):
+        """One eager pass of the ragged batch (statistics in stats())."""
+        rc = lib().swdk_ragged_run(self._ragged(), stream)
+        if rc != 0:
+            raise SwdkError(f"swdk_ragged_run failed ({rc}): {lib().swdk_last_error(self.engines[0]._h).decode()}")
+
+    def stats(self):
+        from .engine import Stats, stats_dict
+        s = Stats()
+        rc = lib().swdk_ragged_stats(self._ragged(), C.byref(s))
+        if rc != 0:
+            raise SwdkError(f"swdk_ragged_stats failed ({rc})")
+        return stats_dict(s)
+
     def capture(self):
+        if self.mode == "ragged":
+            self._ragged()
+            return
         n = len(self.engines)
         calls = (Call * n)(*[self._call(i) for i in range(n)])
         ctxs = (C.c_void_p * n)(*[e._h.value for e in self.engines])
@@ -68,6 +109,12 @@ class UnevenBatch:
         self.graph = g
 
     def launch(self, stream=None):
+        if self.mode == "ragged":
+            rc = lib().swdk_ragged_launch(self._ragged(), stream)
+            if rc != 0:
+                raise SwdkError(f"swdk_ragged_launch failed ({rc}): "
+                                f"{lib().swdk_last_error(self.engines[0]._h).decode()}")
+            return
         if self.graph is None:
             self.capture()
         rc = lib().swdk_batch_graph_launch(self.graph, stream)
@@ -96,6 +143,9 @@ class UnevenBatch:
         if self.graph is not None:
             lib().swdk_batch_graph_destroy(self.graph)
             self.graph = None
+        if self.ragged is not None:
+            lib().swdk_ragged_destroy(self.ragged)
+            self.ragged = None
         for e in self.engines:
             e.close()
         self.engines = []

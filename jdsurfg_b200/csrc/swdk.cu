@@ -467,6 +467,52 @@ __global__ void __launch_bounds__(128) k_roots_one(ChainDesc cd, int ncol, const
              ierr_out, nullptr);
 }
 
+// ---------------------------------------------------------------------------
+// Ragged batches: many models (own grids, depth vectors, period tables) in
+// one launch of each kernel.  The work items of the root search are (model,
+// chain, column); a block of items is one (model, chain) with the model's
+// ncol columns, blocks ordered Rayleigh chains first.  Each model's arrays
+// live at offsets in shared buffers.
+// ---------------------------------------------------------------------------
+struct RModel {
+  int ncol, nz, Lmax, pad_;
+  long long col0;   // first column of the model in per-column arrays (ColInfo, node features)
+  long long lay0;   // float4 offset of its layer tables (layR / layL / lay0, Lmax*ncol each)
+  long long crs0;   // float2 offset of its chain-rule factors (nz*ncol)
+  long long root0;  // offset of its root slots in croot / cstat / prop (nroot*ncol)
+  double *vc, *vout, *kernel;
+  int32_t* status;
+};
+
+struct RBlock {
+  long long item0;  // first work item of the block
+  int model, chain;  // chain: index into the batch's combined chain array
+};
+
+// eigen launch of one wave type over a ragged batch: blocks [blk0, blk0+ncol)
+// are model `model`'s columns, its slots of this wave type at [g0, g0+gn)
+struct REBlock {
+  long long blk0;
+  int model, g0, gn, pad_;
+};
+
+struct RaggedMap {
+  const RBlock* blocks;  // null: one model, items = order[item / ncol] x columns
+  const RModel* models;
+  int nblocks;
+};
+
+template <class T>
+__device__ __forceinline__ int ragged_find(const T* tab, int n, long long key, long long T::*field) {
+  int lo = 0, hi = n - 1;  // last entry with tab[i].*field <= key
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tab[mid].*field <= key) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Persistent root kernel: lanes take (chain, column) items from a queue
 // (chains in `order`, Rayleigh first, columns consecutive) whenever their
 // current chain is finished, so lanes stay busy while long chains run.
@@ -490,7 +536,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      const float2* __restrict__ prop,
                                                      int2* __restrict__ retry_list, unsigned int* __restrict__ retry_count,
                                                      unsigned int retry_cap,
-                                                     unsigned long long* __restrict__ nevals) {
+                                                     unsigned long long* __restrict__ nevals, RaggedMap rg) {
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
   // the chain's state machine lives in shared memory, so the registers go to
@@ -517,18 +563,30 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         const unsigned int item = atomicAdd(queue, 1u);
         if (item >= (unsigned int)nitems) { exhausted = true; break; }
         item_of = (int)item;
-        cd = chains[order[item / ncol]];
-        col = item % ncol;
-        const ColInfo ci = info[col];
-        double* outp = croot + (size_t)cd.out_off * ncol + col;
-        int32_t* stp = cstat + (size_t)cd.out_off * ncol + col;
+        // the item's model (a ragged batch) or the single model's arrays
+        int mcol = ncol;
+        long long o_col = 0, o_lay = 0, o_root = 0;
+        if (rg.blocks) {
+          const RBlock B = rg.blocks[ragged_find(rg.blocks, rg.nblocks, (long long)item, &RBlock::item0)];
+          const RModel& M = rg.models[B.model];
+          cd = chains[B.chain];
+          col = (int)((long long)item - B.item0);
+          mcol = M.ncol;
+          o_col = M.col0; o_lay = M.lay0; o_root = M.root0;
+        } else {
+          cd = chains[order[item / ncol]];
+          col = item % ncol;
+        }
+        const ColInfo ci = info[o_col + col];
+        double* outp = croot + o_root + (size_t)cd.out_off * mcol + col;
+        int32_t* stp = cstat + o_root + (size_t)cd.out_off * mcol + col;
         if (!ci.valid) {
-          for (int i = 0; i < cd.nmode * cd.np; ++i) { outp[(size_t)i * ncol] = 0.0; stp[(size_t)i * ncol] = ST_NAN_INPUT; }
+          for (int i = 0; i < cd.nmode * cd.np; ++i) { outp[(size_t)i * mcol] = 0.0; stp[(size_t)i * mcol] = ST_NAN_INPUT; }
           continue;
         }
-        V.lay = (cd.iwave == 2) ? layR : layL;
+        V.lay = ((cd.iwave == 2) ? layR : layL) + o_lay;
         V.fast = 1;
-        V.ncol = ncol;
+        V.ncol = mcol;
         V.col = col;
         V.L = ci.L;
         V.llw = ci.llw;
@@ -548,9 +606,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         P.retry = retry;
         io.out = outp;
         io.st = stp;
-        io.stride = cd.np * ncol;
-        io.ostride = ncol;
-        io.prop = prop ? prop + (size_t)cd.out_off * ncol + col : nullptr;
+        io.stride = cd.np * mcol;
+        io.ostride = mcol;
+        io.prop = prop ? prop + o_root + (size_t)cd.out_off * mcol + col : nullptr;
         chain_init(s);
         have = true;
       }
@@ -559,7 +617,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
       // chain finished
       if (s.iterlim)
         for (int i = 0; i < cd.nmode * cd.np; ++i)
-          if (io.st[(size_t)i * ncol] == ST_OK) io.st[(size_t)i * ncol] = ST_ITER_LIMIT;
+          if (io.st[(size_t)i * io.ostride] == ST_OK) io.st[(size_t)i * io.ostride] = ST_ITER_LIMIT;
       if (retry == RETRY_DEFERRED && s.ierr != 0) {
         // failed slots become single-period work items for k_retry
         for (int m = 1; m <= cd.nmode; ++m)
@@ -665,7 +723,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                const int2* __restrict__ retry_list,
                                                                const unsigned int* __restrict__ retry_count,
                                                                unsigned int retry_cap, unsigned int* __restrict__ queue,
-                                                               unsigned long long* __restrict__ nevals) {
+                                                               unsigned long long* __restrict__ nevals, RaggedMap rg) {
   __shared__ ChainState sst[128];  // one copy of the warp's chain state per lane
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
@@ -682,12 +740,25 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     ChainIO io;
     LayerView V;
     const int2 rec = retry_list[r];
-    const ChainDesc cd = chains[order[rec.x / ncol]];
-    const int col = rec.x % ncol, m = rec.y >> 16, k = rec.y & 0xffff;
-    const ColInfo ci = info[col];
-    V.lay = (cd.iwave == 2) ? layR : layL;
+    const int m = rec.y >> 16, k = rec.y & 0xffff;
+    int mcol = ncol, col;
+    long long o_col = 0, o_lay = 0, o_root = 0;
+    ChainDesc cd;
+    if (rg.blocks) {
+      const RBlock B = rg.blocks[ragged_find(rg.blocks, rg.nblocks, (long long)rec.x, &RBlock::item0)];
+      const RModel& M = rg.models[B.model];
+      cd = chains[B.chain];
+      col = (int)((long long)rec.x - B.item0);
+      mcol = M.ncol;
+      o_col = M.col0; o_lay = M.lay0; o_root = M.root0;
+    } else {
+      cd = chains[order[rec.x / ncol]];
+      col = rec.x % ncol;
+    }
+    const ColInfo ci = info[o_col + col];
+    V.lay = ((cd.iwave == 2) ? layR : layL) + o_lay;
     V.fast = 1;
-    V.ncol = ncol;
+    V.ncol = mcol;
     V.col = col;
     V.L = ci.L;
     V.llw = ci.llw;
@@ -707,10 +778,10 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     P.retry = RETRY_ONE;
     io.c = cbuf;
     io.cb = cbbuf;
-    io.out = croot + (size_t)cd.out_off * ncol + col;
-    io.st = cstat + (size_t)cd.out_off * ncol + col;
-    io.stride = cd.np * ncol;
-    io.ostride = ncol;
+    io.out = croot + o_root + (size_t)cd.out_off * mcol + col;
+    io.st = cstat + o_root + (size_t)cd.out_off * mcol + col;
+    io.stride = cd.np * mcol;
+    io.ostride = mcol;
     io.prop = nullptr;
     chain_init_retry(s, m, k);
     unsigned long long nev = 0;
@@ -969,6 +1040,22 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
                                                double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
   eigen_column<WT, PATH>(blockIdx.x, ncol, nz, Lmax, lay0, info, chainrule, slots, g0, gn, croot, cstat, sphere, vc,
                          vout, kernel, status, ldo);
+}
+
+// the same over a ragged batch: block b is column b - blk0 of the model of
+// the REBlock entry holding b
+template <int WT, int PATH>
+__global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_EIGEN_MINB)
+    k_eigen_ragged(const REBlock* __restrict__ eb, int neb, const RModel* __restrict__ models,
+                   const float4* __restrict__ lay0, const ColInfo* __restrict__ info,
+                   const float2* __restrict__ chainrule, const SlotDesc* __restrict__ slots,
+                   const double* __restrict__ croot, const int32_t* __restrict__ cstat, int sphere) {
+  const long long b = blockIdx.x;
+  const REBlock E = eb[ragged_find(eb, neb, b, &REBlock::blk0)];
+  const RModel M = models[E.model];
+  eigen_column<WT, PATH>((int)(b - E.blk0), M.ncol, M.nz, M.Lmax, lay0 + M.lay0, info + M.col0, chainrule + M.crs0,
+                         slots, E.g0, E.gn, croot + M.root0, cstat + M.root0, sphere, M.vc, M.vout, M.kernel,
+                         M.status, M.ncol);
 }
 
 // ---------------------------------------------------------------------------
@@ -1303,25 +1390,32 @@ constexpr int PROP_CHUNK = 1 << 20;  // proposal rows per feature/inference laun
 bool proposals_on(const swdk_ctx* ctx) { return ctx->cfg.refine == 1 && (ctx->net[0] || ctx->net[1]); }
 
 // features -> fused network -> (c, half-width) for every root row of plan P
-int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st) {
+// nodefeat / prop: the node features k_prep wrote and the proposal rows to
+// fill (null: the context's own buffers)
+int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st, const float4* nodefeat = nullptr,
+                  float2* prop = nullptr) {
   const int64_t nrows = (int64_t)P.nroot * ncol;
-  CK(ctx->prop.ensure((size_t)nrows * sizeof(float2)));
+  if (!prop) {
+    CK(ctx->prop.ensure((size_t)nrows * sizeof(float2)));
+    prop = ctx->prop.as<float2>();
+  }
+  if (!nodefeat) nodefeat = ctx->nodefeat.as<float4>();
   CK(ctx->pfeat.ensure((size_t)PROP_CHUNK * FEAT_DIM * sizeof(__nv_bfloat16)));
   const int64_t bound[3] = {0, (int64_t)P.nrootR * ncol, nrows};
   for (int w = 0; w < 2; ++w) {
     const int64_t r0 = bound[w], r1 = bound[w + 1];
     if (r1 <= r0) continue;
     if (!ctx->net[w]) {
-      CK(cudaMemsetAsync(ctx->prop.as<float2>() + r0, 0, (size_t)(r1 - r0) * sizeof(float2), st));
+      CK(cudaMemsetAsync(prop + r0, 0, (size_t)(r1 - r0) * sizeof(float2), st));
       continue;
     }
     for (int64_t a = r0; a < r1; a += PROP_CHUNK) {
       const int n = (int)std::min<int64_t>(PROP_CHUNK, r1 - a);
       ctx->launches += 2;
-      k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(),
-                                              ctx->nodefeat.as<float4>(), nullptr, ctx->pfeat.as<__nv_bfloat16>(), 1);
+      k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(), nodefeat, nullptr,
+                                              ctx->pfeat.as<__nv_bfloat16>(), 1);
       CK(cudaGetLastError());
-      int r = swdk_mlp_propose(ctx->net[w], ctx->pfeat.p, n, ctx->kappa[w], ctx->prop.as<float2>() + a, st);
+      int r = swdk_mlp_propose(ctx->net[w], ctx->pfeat.p, n, ctx->kappa[w], prop + a, st);
       if (r) return fail(ctx, r, std::string("proposal inference: ") + swdk_mlp_last_error(ctx->net[w]));
     }
   }
@@ -1405,13 +1499,13 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
       ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(),
       useprop ? ctx->prop.as<float2>() : nullptr, ctx->retry_list.as<int2>(), rctr, rcap,
-      ctx->nevals.as<unsigned long long>());
+      ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0});
   CK(cudaGetLastError());
   k_retry<<<rblocks, 128, 0, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
                                    ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                    ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, ctx->croot.as<double>(),
                                    ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
-                                   ctx->nevals.as<unsigned long long>());
+                                   ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0});
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
@@ -2082,6 +2176,356 @@ int swdk_batch_graph_launch(swdk_graph* g, void* stream) {
   if (!g || !g->exec) return SWDK_E_ARG;
   if (cudaSetDevice(g->device) != cudaSuccess) return SWDK_E_CUDA;
   return cudaGraphLaunch(g->exec, stream ? (cudaStream_t)stream : g->main) == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batches (swdk_ragged_*): every model's column preparation, then ONE
+// persistent root-search launch over all (model, chain, column) items, one
+// retry launch and one eigen launch per wave type over all (model, column)
+// blocks; each model's arrays at offsets in shared buffers, its plans
+// (chains, periods, slots) concatenated.
+// ---------------------------------------------------------------------------
+struct swdk_ragged {
+  int device = 0, n = 0, path = 0;
+  std::vector<swdk_ctx*> ctx;
+  std::vector<swdk_call> calls;
+  std::vector<RModel> models;
+  std::vector<RBlock> blocks;
+  std::vector<REBlock> eb[4];
+  long long eblocks[4] = {0, 0, 0, 0};
+  int et[4] = {0, 0, 0, 0};
+  std::vector<ChainDesc> chains;
+  std::vector<double> periods;
+  std::vector<SlotDesc> slots;
+  long long nitems = 0, ncol_tot = 0, lay_tot = 0, crs_tot = 0, root_tot = 0, slots_tot = 0;
+  int maxL = 0, maxnz = 0, roots_blocks = 0;
+  bool useprop = false;
+  DevBuf d_models, d_blocks, d_eb[4], d_chains, d_periods, d_slots;
+  DevBuf layR, layL, lay0, info, chainrule, croot, cstat, prop, nodefeat, retry_list, retry_ctr, queue, nevals;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  unsigned long long* h_nevals = nullptr;
+  bool stats_pending = false;
+  swdk_stats stats;
+  int launches = 0;
+};
+
+namespace {
+
+// the kernels of one pass over a ragged batch, enqueued on st; timing
+// events and the statistics copy only when not capturing
+int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
+  swdk_ctx* ctx = R->ctx[0];
+  const swdk_config& cfg = ctx->cfg;
+  CK(cudaMemsetAsync(R->nevals.p, 0, NCOUNT * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(R->queue.p, 0, sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(R->retry_ctr.p, 0, 2 * sizeof(unsigned int), st));
+  if (timing) CK(cudaEventRecord(R->ev[0], st));
+  R->launches = 0;
+  for (int i = 0; i < R->n; ++i) {
+    const RModel& M = R->models[i];
+    const swdk_call& c = R->calls[i];
+    R->launches += 1;
+    k_prep<<<(M.ncol + 127) / 128, 128, 0, st>>>(
+        M.ncol, M.ncol, M.nz, c.d_vs, c.d_vp, c.d_rho, R->ctx[i]->depth_d.as<float>(), cfg.sphere, M.Lmax,
+        R->layR.as<float4>() + M.lay0, R->layL.as<float4>() + M.lay0, R->lay0.as<float4>() + M.lay0,
+        R->info.as<ColInfo>() + M.col0, R->chainrule.as<float2>() + M.crs0,
+        R->useprop ? R->nodefeat.as<float4>() + M.col0 * FEAT_NODES : nullptr);
+    CK(cudaGetLastError());
+  }
+  if (timing) CK(cudaEventRecord(R->ev[1], st));
+  if (R->useprop) {
+    for (int i = 0; i < R->n; ++i) {
+      swdk_ctx* c = R->ctx[i];
+      const RModel& M = R->models[i];
+      const Plan& P = c->plan[R->path];
+      float2* dst = R->prop.as<float2>() + M.root0;
+      if (!proposals_on(c)) {
+        CK(cudaMemsetAsync(dst, 0, (size_t)P.nroot * M.ncol * sizeof(float2), st));
+        continue;
+      }
+      c->launches = 0;
+      const int r = run_proposals(c, P, M.ncol, st, R->nodefeat.as<float4>() + M.col0 * FEAT_NODES, dst);
+      if (r) return fail(ctx, r, "ragged proposals: " + c->err);
+      R->launches += c->launches;
+    }
+  }
+  if (timing) CK(cudaEventRecord(R->ev[5], st));
+  const RaggedMap rg{R->d_blocks.as<RBlock>(), R->d_models.as<RModel>(), (int)R->blocks.size()};
+  const unsigned int rcap = (unsigned int)std::min<long long>(R->root_tot, 0x7fffffffLL);
+  unsigned int* rctr = R->retry_ctr.as<unsigned int>();
+  const long long grid = std::min<long long>(R->roots_blocks, (R->nitems + 127) / 128);
+  R->launches += 2;
+  k_roots_queue<<<(unsigned)std::max(1LL, grid), 128, 0, st>>>(
+      0, (int)R->nitems, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(), R->layR.as<float4>(),
+      R->layL.as<float4>(), R->info.as<ColInfo>(), cfg.refine, cfg.rtol, cfg.sngl, RETRY_DEFERRED,
+      R->croot.as<double>(), R->cstat.as<int32_t>(), R->queue.as<unsigned int>(),
+      R->useprop ? R->prop.as<float2>() : nullptr, R->retry_list.as<int2>(), rctr, rcap,
+      R->nevals.as<unsigned long long>(), rg);
+  CK(cudaGetLastError());
+  k_retry<<<R->roots_blocks, 128, 0, st>>>(0, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(),
+                                           R->layR.as<float4>(), R->layL.as<float4>(), R->info.as<ColInfo>(),
+                                           cfg.refine, cfg.rtol, cfg.sngl, R->croot.as<double>(),
+                                           R->cstat.as<int32_t>(), R->retry_list.as<int2>(), rctr, rcap, rctr + 1,
+                                           R->nevals.as<unsigned long long>(), rg);
+  CK(cudaGetLastError());
+  if (timing) CK(cudaEventRecord(R->ev[2], st));
+  if (R->path != 2) {
+    using EigR = void (*)(const REBlock*, int, const RModel*, const float4*, const ColInfo*, const float2*,
+                          const SlotDesc*, const double*, const int32_t*, int);
+    static const EigR eig[4][2] = {{k_eigen_ragged<0, 0>, k_eigen_ragged<0, 1>},
+                                   {k_eigen_ragged<1, 0>, k_eigen_ragged<1, 1>},
+                                   {k_eigen_ragged<2, 0>, k_eigen_ragged<2, 1>},
+                                   {k_eigen_ragged<3, 0>, k_eigen_ragged<3, 1>}};
+    for (int wt = 0; wt < 4; ++wt) {
+      if (R->eb[wt].empty()) continue;
+      const size_t smem = (size_t)R->maxL * (wt >= 2 ? sizeof(LoveLayer) : sizeof(RayLayer)) +
+                          (size_t)R->maxnz * sizeof(float2);
+      R->launches += 1;
+      eig[wt][R->path]<<<(unsigned)R->eblocks[wt], R->et[wt], smem, st>>>(
+          R->d_eb[wt].as<REBlock>(), (int)R->eb[wt].size(), R->d_models.as<RModel>(), R->lay0.as<float4>(),
+          R->info.as<ColInfo>(), R->chainrule.as<float2>(), R->d_slots.as<SlotDesc>(), R->croot.as<double>(),
+          R->cstat.as<int32_t>(), cfg.sphere);
+      CK(cudaGetLastError());
+    }
+  }
+  if (timing) {
+    CK(cudaEventRecord(R->ev[3], st));
+    CK(cudaMemcpyAsync(R->h_nevals, R->nevals.p, NCOUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(R->ev[4], st));
+    R->stats_pending = true;
+  }
+  return SWDK_OK;
+}
+
+void ragged_collect(swdk_ragged* R) {
+  if (!R->stats_pending) return;
+  cudaEventSynchronize(R->ev[4]);
+  R->stats_pending = false;
+  swdk_stats& t = R->stats;
+  memset(&t, 0, sizeof(t));
+  t.secular_evals = (int64_t)R->h_nevals[0];
+  t.layer_evals_rayleigh = (int64_t)R->h_nevals[1];
+  t.layer_evals_love = (int64_t)R->h_nevals[2];
+  t.proposals_accepted = (int64_t)R->h_nevals[3];
+  t.proposals_rejected = (int64_t)R->h_nevals[4];
+  for (int i = 0; i < NPHASE_EV; ++i) t.evals_by_phase[i] = (int64_t)R->h_nevals[EV_BASE + i];
+  t.nchains = (int)R->chains.size();
+  t.nslots = (int)R->slots_tot;
+  t.kernel_launches = R->launches;
+  cudaEventElapsedTime(&t.ms_prep, R->ev[0], R->ev[1]);
+  cudaEventElapsedTime(&t.ms_proposal, R->ev[1], R->ev[5]);
+  cudaEventElapsedTime(&t.ms_roots, R->ev[5], R->ev[2]);
+  cudaEventElapsedTime(&t.ms_eigen, R->ev[2], R->ev[3]);
+}
+
+}  // namespace
+
+void swdk_ragged_destroy(swdk_ragged* R) {
+  if (!R) return;
+  cudaSetDevice(R->device);
+  if (R->stream) cudaStreamSynchronize(R->stream);
+  if (R->exec) cudaGraphExecDestroy(R->exec);
+  if (R->graph) cudaGraphDestroy(R->graph);
+  DevBuf* bufs[] = {&R->d_models, &R->d_blocks, &R->d_eb[0], &R->d_eb[1], &R->d_eb[2], &R->d_eb[3], &R->d_chains,
+                    &R->d_periods, &R->d_slots, &R->layR, &R->layL, &R->lay0, &R->info, &R->chainrule, &R->croot,
+                    &R->cstat, &R->prop, &R->nodefeat, &R->retry_list, &R->retry_ctr, &R->queue, &R->nevals};
+  for (DevBuf* b : bufs) b->release();
+  for (cudaEvent_t& e : R->ev)
+    if (e) cudaEventDestroy(e);
+  if (R->h_nevals) cudaFreeHost(R->h_nevals);
+  if (R->stream) cudaStreamDestroy(R->stream);
+  delete R;
+}
+
+int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swdk_ragged** out) {
+  if (!out || n <= 0 || !ctxs || !calls) return SWDK_E_ARG;
+  *out = nullptr;
+  swdk_ctx* ctx = ctxs[0];
+  if (!ctx) return SWDK_E_ARG;
+  const int path = calls[0].path;
+  if (path < 0 || path > 2) return fail(ctx, SWDK_E_ARG, "bad path");
+  for (int i = 0; i < n; ++i) {
+    const swdk_ctx* c = ctxs[i];
+    const swdk_call& k = calls[i];
+    if (!c || k.path != path || c->cfg.device != ctx->cfg.device || c->cfg.refine != ctx->cfg.refine ||
+        c->cfg.rtol != ctx->cfg.rtol || c->cfg.sngl != ctx->cfg.sngl || c->cfg.sphere != ctx->cfg.sphere)
+      return fail(ctx, SWDK_E_ARG, "ragged batch: every model needs the same path, device and root settings");
+    if (k.nx <= 0 || k.ny <= 0 || !k.d_vs || (path != 2 && (!k.d_vc || !k.d_vout || (path == 0 && !k.d_kernel))))
+      return fail(ctx, SWDK_E_ARG, "ragged batch: bad call arguments");
+    if ((k.d_vp == nullptr) != (k.d_rho == nullptr)) return fail(ctx, SWDK_E_ARG, "vp and rho must both be given");
+    if ((int)c->depth.size() != k.nz) return fail(ctx, SWDK_E_NODEPTH, "nz does not match swdk_set_depth");
+    if (k.nz < 2 || k.nz > SWDK_MAX_NZ || 4 * k.nz - 3 > SWDK_MAX_LAYERS) return fail(ctx, SWDK_E_LIMIT, "nz out of range");
+  }
+  CK(cudaSetDevice(ctx->cfg.device));
+  swdk_ragged* R = new swdk_ragged();
+  memset(&R->stats, 0, sizeof(R->stats));
+  R->device = ctx->cfg.device;
+  R->n = n;
+  R->path = path;
+  R->ctx.assign(ctxs, ctxs + n);
+  R->calls.assign(calls, calls + n);
+  auto bail = [&](int code, const std::string& msg) {
+    swdk_ragged_destroy(R);
+    return fail(ctx, code, msg);
+  };
+  const int ppath = (path == 2) ? 0 : path;
+  std::vector<int> chain0(n), slot0(n);
+  for (int i = 0; i < n; ++i) {
+    swdk_ctx* c = ctxs[i];
+    const int r = ensure_plans(c);
+    if (r) { swdk_ragged_destroy(R); return r; }
+    const Plan& P = c->plan[ppath];
+    const swdk_call& k = calls[i];
+    RModel M;
+    M.ncol = k.nx * k.ny;
+    M.nz = k.nz;
+    M.Lmax = 4 * k.nz - 3;
+    M.pad_ = 0;
+    M.col0 = R->ncol_tot;
+    M.lay0 = R->lay_tot;
+    M.crs0 = R->crs_tot;
+    M.root0 = R->root_tot;
+    M.vc = k.d_vc;
+    M.vout = k.d_vout;
+    M.kernel = k.d_kernel;
+    M.status = k.d_status;
+    R->models.push_back(M);
+    R->ncol_tot += M.ncol;
+    R->lay_tot += (long long)M.Lmax * M.ncol;
+    R->crs_tot += (long long)M.nz * M.ncol;
+    R->root_tot += (long long)P.nroot * M.ncol;
+    R->slots_tot += (long long)P.kmax;
+    R->maxL = std::max(R->maxL, M.Lmax);
+    R->maxnz = std::max(R->maxnz, M.nz);
+    chain0[i] = (int)R->chains.size();
+    for (ChainDesc d : P.chains) {
+      d.t_off += (int)R->periods.size();
+      R->chains.push_back(d);
+    }
+    R->periods.insert(R->periods.end(), P.periods.begin(), P.periods.end());
+    slot0[i] = (int)R->slots.size();
+    R->slots.insert(R->slots.end(), P.slots.begin(), P.slots.end());
+    for (int g = 0; g < P.groups.n; ++g) {
+      const int wt = P.slots[P.groups.start[g]].wtype;
+      REBlock E;
+      E.blk0 = R->eblocks[wt];
+      E.model = i;
+      E.g0 = slot0[i] + P.groups.start[g];
+      E.gn = P.groups.count[g];
+      E.pad_ = 0;
+      R->eb[wt].push_back(E);
+      R->eblocks[wt] += M.ncol;
+      R->et[wt] = std::max(R->et[wt], std::min(128, ((E.gn + 31) / 32) * 32));
+    }
+    if (proposals_on(c)) R->useprop = true;
+    // the model's depth vector on the device (k_prep reads it)
+    CK(c->depth_d.ensure((size_t)k.nz * sizeof(float)));
+    if (c->depth_dev != c->depth_d.p) {
+      CK(cudaMemcpy(c->depth_d.p, c->depth.data(), k.nz * sizeof(float), cudaMemcpyHostToDevice));
+      c->depth_dev = c->depth_d.p;
+    }
+  }
+  // root work blocks: every model's Rayleigh chains, then the Love chains
+  for (int w = 2; w >= 1; --w)
+    for (int i = 0; i < n; ++i) {
+      const Plan& P = ctxs[i]->plan[ppath];
+      for (int ci : P.order) {
+        if (P.chains[ci].iwave != w) continue;
+        RBlock B;
+        B.item0 = R->nitems;
+        B.model = i;
+        B.chain = chain0[i] + ci;
+        R->blocks.push_back(B);
+        R->nitems += R->models[i].ncol;
+      }
+    }
+  if (R->nitems >= 0x7fffffffLL) return bail(SWDK_E_LIMIT, "ragged batch: too many work items");
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
+    cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess && bytes) e = cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e = up(R->d_models, R->models.data(), R->models.size() * sizeof(RModel));
+  if (e == cudaSuccess) e = up(R->d_blocks, R->blocks.data(), R->blocks.size() * sizeof(RBlock));
+  for (int wt = 0; wt < 4 && e == cudaSuccess; ++wt) e = up(R->d_eb[wt], R->eb[wt].data(), R->eb[wt].size() * sizeof(REBlock));
+  if (e == cudaSuccess) e = up(R->d_chains, R->chains.data(), R->chains.size() * sizeof(ChainDesc));
+  if (e == cudaSuccess) e = up(R->d_periods, R->periods.data(), R->periods.size() * sizeof(double));
+  if (e == cudaSuccess) e = up(R->d_slots, R->slots.data(), R->slots.size() * sizeof(SlotDesc));
+  if (e == cudaSuccess) e = R->layR.ensure((size_t)R->lay_tot * sizeof(float4));
+  if (e == cudaSuccess) e = R->layL.ensure((size_t)R->lay_tot * sizeof(float4));
+  if (e == cudaSuccess) e = R->lay0.ensure((size_t)R->lay_tot * sizeof(float4));
+  if (e == cudaSuccess) e = R->info.ensure((size_t)R->ncol_tot * sizeof(ColInfo));
+  if (e == cudaSuccess) e = R->chainrule.ensure((size_t)R->crs_tot * sizeof(float2));
+  if (e == cudaSuccess) e = R->croot.ensure((size_t)R->root_tot * sizeof(double));
+  if (e == cudaSuccess) e = R->cstat.ensure((size_t)R->root_tot * sizeof(int32_t));
+  if (e == cudaSuccess && R->useprop) e = R->prop.ensure((size_t)R->root_tot * sizeof(float2));
+  if (e == cudaSuccess && R->useprop) e = R->nodefeat.ensure((size_t)R->ncol_tot * FEAT_NODES * sizeof(float4));
+  if (e == cudaSuccess) e = R->retry_list.ensure((size_t)std::min<long long>(R->root_tot, 0x7fffffffLL) * sizeof(int2));
+  if (e == cudaSuccess) e = R->retry_ctr.ensure(2 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = R->queue.ensure(sizeof(unsigned int));
+  if (e == cudaSuccess) e = R->nevals.ensure(NCOUNT * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&R->ev[i]);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&R->h_nevals, NCOUNT * sizeof(unsigned long long));
+  if (e != cudaSuccess) return bail(SWDK_E_CUDA, std::string("ragged batch set-up: ") + cudaGetErrorString(e));
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0);
+  R->roots_blocks = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : std::max(1, nsm * std::max(1, per));
+  *out = R;
+  return SWDK_OK;
+}
+
+int swdk_ragged_run(swdk_ragged* R, void* stream) {
+  if (!R) return SWDK_E_ARG;
+  swdk_ctx* ctx = R->ctx[0];
+  CK(cudaSetDevice(R->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : R->stream;
+  const int r = ragged_enqueue(R, st, true);
+  if (r) return r;
+  if (!stream) {
+    CK(cudaStreamSynchronize(st));
+    ragged_collect(R);
+  }
+  return SWDK_OK;
+}
+
+int swdk_ragged_launch(swdk_ragged* R, void* stream) {
+  if (!R) return SWDK_E_ARG;
+  swdk_ctx* ctx = R->ctx[0];
+  CK(cudaSetDevice(R->device));
+  if (!R->exec) {
+    // one eager pass first (sizes the proposal scratch of every context),
+    // then the same work captured as one graph
+    int r = ragged_enqueue(R, R->stream, true);
+    if (r) return r;
+    CK(cudaStreamSynchronize(R->stream));
+    ragged_collect(R);
+    CK(cudaStreamBeginCapture(R->stream, cudaStreamCaptureModeThreadLocal));
+    r = ragged_enqueue(R, R->stream, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(R->stream, &g);
+    if (r) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e2 != cudaSuccess) return fail(ctx, SWDK_E_CUDA, std::string("ragged capture: ") + cudaGetErrorString(e2));
+    R->graph = g;
+    CK(cudaGraphInstantiate(&R->exec, g, 0));
+  }
+  CK(cudaGraphLaunch(R->exec, stream ? (cudaStream_t)stream : R->stream));
+  return SWDK_OK;
+}
+
+int swdk_ragged_stats(swdk_ragged* R, swdk_stats* out) {
+  if (!R || !out) return SWDK_E_ARG;
+  ragged_collect(R);
+  *out = R->stats;
+  return SWDK_OK;
 }
 
 int swdk_graph_launch(swdk_ctx* ctx, void* stream) {

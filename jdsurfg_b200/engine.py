@@ -47,6 +47,16 @@ class Stats(C.Structure):
 EVAL_PHASES = ("scan_first_period", "scan", "learned_cell", "walk", "refine", "retry")
 
 
+def stats_dict(s):
+    """A swdk_stats structure as a dict."""
+    return dict(secular_evals=s.secular_evals, layer_evals_rayleigh=s.layer_evals_rayleigh,
+                layer_evals_love=s.layer_evals_love, nchains=s.nchains, nslots=s.nslots, ms_prep=s.ms_prep,
+                ms_roots=s.ms_roots, ms_eigen=s.ms_eigen, proposals_accepted=s.proposals_accepted,
+                proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal,
+                kernel_launches=s.kernel_launches,
+                evals_by_phase=dict(zip(EVAL_PHASES, [int(x) for x in s.evals_by_phase])))
+
+
 _LIB = None
 
 
@@ -87,6 +97,12 @@ def lib():
         L.swdk_batch_graph_launch.argtypes = [vp, vp]
         L.swdk_batch_graph_destroy.argtypes = [vp]
         L.swdk_batch_graph_destroy.restype = None
+        L.swdk_ragged_create.argtypes = [C.c_int, vp, vp, C.POINTER(vp)]
+        L.swdk_ragged_run.argtypes = [vp, vp]
+        L.swdk_ragged_launch.argtypes = [vp, vp]
+        L.swdk_ragged_stats.argtypes = [vp, C.POINTER(Stats)]
+        L.swdk_ragged_destroy.argtypes = [vp]
+        L.swdk_ragged_destroy.restype = None
         L.swdk_last_error.argtypes = [vp]
         L.swdk_last_error.restype = C.c_char_p
         _LIB = L
@@ -298,9 +314,4 @@ class Engine:
     def stats(self):
         s = Stats()
         self._check(lib().swdk_get_stats(self._h, C.byref(s)), "swdk_get_stats")
-        return dict(secular_evals=s.secular_evals, layer_evals_rayleigh=s.layer_evals_rayleigh,
-                    layer_evals_love=s.layer_evals_love, nchains=s.nchains, nslots=s.nslots, ms_prep=s.ms_prep,
-                    ms_roots=s.ms_roots, ms_eigen=s.ms_eigen, proposals_accepted=s.proposals_accepted,
-                    proposals_rejected=s.proposals_rejected, ms_proposal=s.ms_proposal,
-                    kernel_launches=s.kernel_launches,
-                    evals_by_phase=dict(zip(EVAL_PHASES, [int(x) for x in s.evals_by_phase])))
+        return stats_dict(s)

@@ -1,6 +1,8 @@
 """Uneven batch (many models of different grids, depths, periods, wave types
 and modes in one CUDA-graph launch) against the oracle, against each model's
-own eager call, and its depth kernels as CSR Frechet rows."""
+own eager call, and its depth kernels as CSR Frechet rows; both the ragged
+single-launch path (one persistent root search and one eigen launch per
+wave type over every model) and the graph of per-model branches."""
 import numpy as np
 import pytest
 
@@ -13,10 +15,11 @@ pytestmark = pytest.mark.gpu
 TOL_C, TOL_K = 1e-6, 1e-5
 
 
-def test_uneven_batch_graph_matches_oracle_and_eager():
+@pytest.mark.parametrize("mode", ["ragged", "branches"])
+def test_uneven_batch_graph_matches_oracle_and_eager(mode):
     cases = synth.make_uneven_batch(6, seed=3, small=True)
     assert len({(c["nx"], c["ny"], c["nz"]) for c in cases}) > 1
-    B = UnevenBatch(cases, learned=True)
+    B = UnevenBatch(cases, learned=True, mode=mode)
     B.launch()
     got = [B.outputs(i) for i in range(len(cases))]
     for i, case in enumerate(cases):
@@ -73,4 +76,38 @@ def test_uneven_batch_csr_rows_match_oracle_layout():
         with pytest.raises(Exception):
             eng.frechet_csr_device(nx, ny, nz, kmax, ker, torch.from_numpy(row_slot).to(dev),
                                    torch.from_numpy(fdm).to(dev), rowptr, idx[:max(0, tot - 1)], val)
+    B.close()
+
+
+def test_ragged_48_model_batch_against_oracle_sampled():
+    """The 48-model uneven batch of the bench (grids 32x32..200x200, 24-80
+    nodes, 15-60 periods, Rayleigh/Love phase/group, modes 0-2) in one
+    ragged pass: 6 random columns of every model against the oracle, and the
+    eager pass equal to the graph replay."""
+    cases = synth.make_uneven_batch(48, seed=5150)
+    B = UnevenBatch(cases, learned=True, mode="ragged")
+    B.run()
+    st = B.stats()
+    eager = [B.outputs(i) for i in range(len(cases))]
+    B.launch()
+    rng = np.random.default_rng(0)
+    worst_c = worst_k = 0.0
+    for i, case in enumerate(cases):
+        g = B.outputs(i)
+        for k in g:
+            assert np.array_equal(g[k], eager[i][k]), (i, k)
+        cols = np.sort(rng.choice(case["nx"] * case["ny"], 6, replace=False))
+        ref = O.get_1d_kernel(case, refine=1, cols=cols)
+        gg = {k: v[..., cols] for k, v in g.items()}
+        np.testing.assert_array_equal(gg["status"], ref["status"], err_msg=f"model {i}")
+        ok = ref["status"] != 1
+        worst_c = max(worst_c, np.abs(gg["vc"] - ref["vc"])[ok].max(initial=0.0))
+        assert np.abs(gg["vc"] - ref["vc"])[ok].max(initial=0.0) <= TOL_C, i
+        assert np.abs(gg["vout"] - ref["vout"])[ok].max(initial=0.0) <= TOL_C, i
+        scale = np.abs(ref["kernel"]).max(axis=1, keepdims=True) + 1e-30
+        kr = (np.abs(gg["kernel"] - ref["kernel"]) / scale).max(initial=0.0)
+        worst_k = max(worst_k, kr)
+        assert kr <= TOL_K, (i, kr)
+    print(f"ragged 48-model batch: {B.units} slots, {st['kernel_launches']} launches per pass, "
+          f"max |dc| {worst_c:.2e} km/s, max kernel rel err {worst_k:.2e} on 288 sampled columns")
     B.close()
