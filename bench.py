@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--split-cols", type=int, default=0,
                     help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
     ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
+    ap.add_argument("--path", default="kernel", choices=["kernel", "map"],
+                    help="kernel: get_1d_kernel (dispersion + depth kernels); map: get_2d_map (phase and group maps "
+                         "of travel_time's line-search steps)")
     ap.add_argument("--uneven-mode", default="ragged", choices=["ragged", "branches"],
                     help="uneven workload: one ragged launch per kernel, or a graph branch per model")
     ap.add_argument("--sharded", action="store_true",
@@ -109,7 +112,7 @@ WORKLOAD_TEXT = {
 def case_desc(args, case, kmax):
     return {"workload": args.workload, "what": WORKLOAD_TEXT[args.workload], "nx": case["nx"], "ny": case["ny"],
             "nz": case["nz"], "kmax": kmax, "columns": case["nx"] * case["ny"], "refine": args.refine,
-            "proposal": args.proposal, "root_tolerance_km_s": 1e-6,
+            "proposal": args.proposal, "root_tolerance_km_s": 1e-6, "path": getattr(args, "path", "kernel"),
             "l2": "flushed between steps (256 MiB write)", "sphere": True}
 
 
@@ -202,8 +205,9 @@ def cpu_baseline(case, args, target_s):
     ncol = case["nx"] * case["ny"]
     refine = 0  # the reference's own algorithm: surfdisp96's scan + nevill refinement
     n = min(ncol, max(cores, 8))
+    fn = O.get_2d_map if getattr(args, "path", "kernel") == "map" else O.get_1d_kernel
     t0 = time.perf_counter()
-    r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n))
+    r = fn(case, refine=refine, nthreads=cores, cols=np.arange(n))
     dt = time.perf_counter() - t0
     kmax = r["vc"].shape[0]
     per_col = dt / n
@@ -211,7 +215,7 @@ def cpu_baseline(case, args, target_s):
     n2 = max(cores, (n2 // cores) * cores) if n2 >= cores else n2
     n2 = min(n2, ncol)
     t0 = time.perf_counter()
-    r = O.get_1d_kernel(case, refine=refine, nthreads=cores, cols=np.arange(n2))
+    r = fn(case, refine=refine, nthreads=cores, cols=np.arange(n2))
     dt = time.perf_counter() - t0
     return {"value": n2 * kmax / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{n2} of {ncol} columns x {kmax} slots ({dt:.1f} s, {how}, OpenMP over columns, "
@@ -295,11 +299,12 @@ def run_reference(args):
     import oracle_lib as O
     refine = 0  # reference-faithful: surfdisp96's own scan + nevill refinement
     cols = np.arange(n2)
+    fn = O.get_2d_map if args.path == "map" else O.get_1d_kernel
     for _ in range(args.warmup):
-        O.get_1d_kernel(case, refine=refine, nthreads=cb["cores"], cols=cols[:max(1, n2 // 4)])
+        fn(case, refine=refine, nthreads=cb["cores"], cols=cols[:max(1, n2 // 4)])
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.get_1d_kernel(case, refine=refine, nthreads=cb["cores"], cols=cols)
+        fn(case, refine=refine, nthreads=cb["cores"], cols=cols)
     dt = time.perf_counter() - t0
     value = args.steps * n2 * kmax / dt
     cb["value"] = value
@@ -600,7 +605,8 @@ def main():
     rho = None if case["rho"] is None else torch.from_numpy(case["rho"]).to(dev)
     vc = torch.empty((kmax, ncol), dtype=torch.float64, device=dev)
     vout = torch.empty_like(vc)
-    ker = torch.empty((kmax, nz, ncol), dtype=torch.float64, device=dev)
+    mapped = args.path == "map"
+    ker = None if mapped else torch.empty((kmax, nz, ncol), dtype=torch.float64, device=dev)
     st = torch.empty((kmax, ncol), dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     # one explicit stream for the flush, the engine's work and the timing
@@ -609,9 +615,15 @@ def main():
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
+    def call(e):
+        if mapped:
+            e.get_2d_map_device(nx, ny, nz, vs, vp, rho, vc, vout, st, stream=sptr)
+        else:
+            e.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
+
     def step():
         flush.fill_(1)
-        eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
+        call(eng)
 
     roots_blocks = eng.autotune(nx, ny, nz, vs, vp, rho) if not args.no_graph and not args.roots_blocks else None
     for _ in range(args.warmup):
@@ -636,7 +648,7 @@ def main():
         if eng_nets_on[0]:
             learn.load_proposals(probe_eng)
         probe_eng.setup(case)
-        probe_eng.get_1d_kernel_device(nx, ny, nz, vs, vp, rho, vc, vout, ker, st, stream=sptr)
+        call(probe_eng)
         probe = probe_eng.stats()
         probe_eng.close()
         acc = {k: probe[k] * nsteps for k in STAT_KEYS}
@@ -644,7 +656,7 @@ def main():
         acc["evals_by_phase"] = probe["evals_by_phase"]
         use_graph = not args.no_graph
         if use_graph:
-            eng.graph_capture("kernel", nx, ny, nz, vs, vp, rho, vc, vout, ker, st)
+            eng.graph_capture(args.path, nx, ny, nz, vs, vp, rho, vc, vout, ker, st)
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
@@ -716,14 +728,18 @@ def main():
             h_rho = pin(case["rho"].shape, torch.float32)
             h_rho[...] = case["rho"]
         h_vc, h_vout = pin((kmax, ncol), torch.float64), pin((kmax, ncol), torch.float64)
-        h_ker = pin((kmax, nz, ncol), torch.float64)
+        h_ker = None if mapped else pin((kmax, nz, ncol), torch.float64)
         h_st = pin((kmax, ncol), torch.int32)
         import ctypes as C
         from jdsurfg_b200.engine import lib, _p
 
         def host_step():
-            rc = lib().swdk_get_1d_kernel(eng._h, nx, ny, nz, _p(h_vs), _p(h_vp), _p(h_rho), _p(h_vc), _p(h_vout),
-                                          _p(h_ker), _p(h_st))
+            if mapped:
+                rc = lib().swdk_get_2d_map(eng._h, nx, ny, nz, _p(h_vs), _p(h_vp), _p(h_rho), _p(h_vc), _p(h_vout),
+                                           _p(h_st))
+            else:
+                rc = lib().swdk_get_1d_kernel(eng._h, nx, ny, nz, _p(h_vs), _p(h_vp), _p(h_rho), _p(h_vc),
+                                              _p(h_vout), _p(h_ker), _p(h_st))
             assert rc == 0, rc
 
         host_step()
@@ -741,7 +757,7 @@ def main():
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             dt = float(t.item())
         h2d = h_vs.nbytes + (0 if h_vp is None else h_vp.nbytes + h_rho.nbytes)
-        d2h = h_vc.nbytes + h_vout.nbytes + h_ker.nbytes + h_st.nbytes
+        d2h = h_vc.nbytes + h_vout.nbytes + (0 if h_ker is None else h_ker.nbytes) + h_st.nbytes
         e2e = {"value": world * units * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h)}
 
@@ -765,11 +781,14 @@ def main():
         if tab is None:
             continue
         nslot = _synth.kmax_of([tab if i == w else None for i in range(4)])
-        passes["rayleigh" if w < 2 else "love"] += nslot * (3 if w in (1, 3) else 1)
+        # kernel path: one pass per phase slot, three per group slot; map
+        # path: one pass per group slot (disp1D's sregn96/slegn96 for U)
+        per = (1 if w in (1, 3) else 0) if mapped else (3 if w in (1, 3) else 1)
+        passes["rayleigh" if w < 2 else "love"] += nslot * per
     L = 4 * nz - 3
     eig_flops = ncol * L * (passes["rayleigh"] * F_EIG_RAYLEIGH + passes["love"] * F_EIG_LOVE) * args.steps
     eig_s = acc["ms_eigen"] * 1e-3
-    out_bytes = (ncol * kmax * (nz + 2) * 8 + ncol * kmax * 4) * args.steps  # kernel, vc, vout (f64), status
+    out_bytes = (ncol * kmax * ((0 if mapped else nz) + 2) * 8 + ncol * kmax * 4) * args.steps  # kernel, vc, vout, status
     if eig_s > 0:
         ach_e = eig_flops / eig_s / 1e12
         roofline["eigen"] = {"kernel": "k_eigen", "bound": "fp64", "achieved": ach_e, "peak": peak, "unit": "TFLOP/s",

@@ -326,6 +326,17 @@ void swdk_ragged_destroy(swdk_ragged* batch);
 int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, const float* d_vp, const float* d_rho,
                   int* blocks);
 
+/* The Frechet rows as the reference's row-file byte stream, built on the
+ * device (replaces the record loop of SurfTime::frechet_matrix,
+ * SurfaceWave.cpp:596-603, 641-659): d_out receives int32 m_header, int32 n,
+ * then per row r int32 row id (d_row_ids[r], or row_id0 + r when d_row_ids
+ * is NULL), int32 nnz, int32 idx[nnz], float32 val[nnz] from the CSR rows
+ * (d_rowptr has m+1 entries, nnz_total = d_rowptr[m]).  The stream needs
+ * 2 + 2*m + 2*nnz_total words; a smaller out_words returns SWDK_E_LIMIT. */
+int swdk_frechet_records_device(int64_t m, int32_t m_header, int32_t n, const int32_t* d_row_ids, int32_t row_id0,
+                                const int64_t* d_rowptr, const int32_t* d_indices, const float* d_values,
+                                int64_t nnz_total, int32_t* d_out, int64_t out_words, void* stream);
+
 /* LSMR's matrix products on the device with the CSR rows of
  * swdk_frechet_csr_device (replaces myaprod_csr, src/shared/parallel.cpp:
  * 31-115, used by LSMR in src/shared/lsmrModule_csr.f90): mode 1 y += A x,

@@ -1135,6 +1135,32 @@ __global__ void k_aprod2(int64_t m, const int64_t* __restrict__ rowptr, const in
 }
 
 // exclusive prefix sum of nnz[0..n) into rowptr[0..n] (one block)
+// The reference's row-file records (SurfaceWave.cpp:596-603, 641-659) from
+// CSR rows: a header (int32 m, int32 n) and per row int32 row id, int32 nnz,
+// int32 idx[nnz], float32 val[nnz]; row r starts at word 2 + 2r + 2 rowptr[r].
+// One warp per row, the index and value runs copied with coalesced accesses.
+__global__ void k_frechet_records(int64_t m, int32_t mh, int32_t n, const int32_t* __restrict__ row_ids, int32_t row0,
+                                  const int64_t* __restrict__ rowptr, const int32_t* __restrict__ idx,
+                                  const float* __restrict__ val, int32_t* __restrict__ out) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r == 0 && lane == 0) { out[0] = mh; out[1] = n; }
+  if (r >= m) return;
+  const int64_t a = rowptr[r], b = rowptr[r + 1];
+  int32_t* rec = out + 2 + 2 * r + 2 * a;
+  if (lane == 0) {
+    rec[0] = row_ids ? row_ids[r] : (int32_t)(row0 + r);
+    rec[1] = (int32_t)(b - a);
+  }
+  const int64_t nnz = b - a;
+  int32_t* oi = rec + 2;
+  int32_t* ov = rec + 2 + nnz;
+  for (int64_t k = lane; k < nnz; k += 32) {
+    oi[k] = idx[a + k];
+    ov[k] = __float_as_int(val[a + k]);
+  }
+}
+
 __global__ void k_rowptr(int n, const int32_t* __restrict__ nnz, int64_t* __restrict__ rowptr) {
   __shared__ long long part[1024];
   __shared__ long long carry;
@@ -2579,6 +2605,19 @@ int swdk_recip_device(const double* d_x, double* d_r, int n, void* stream) {
   if (n < 0 || (n > 0 && (!d_x || !d_r))) return SWDK_E_ARG;
   if (n == 0) return SWDK_OK;
   k_recip<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, d_x, d_r);
+  return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
+}
+
+int swdk_frechet_records_device(int64_t m, int32_t m_header, int32_t n, const int32_t* d_row_ids, int32_t row_id0,
+                                const int64_t* d_rowptr, const int32_t* d_indices, const float* d_values,
+                                int64_t nnz_total, int32_t* d_out, int64_t out_words, void* stream) {
+  if (m < 0 || nnz_total < 0 || !d_out || (m > 0 && (!d_rowptr || (nnz_total > 0 && (!d_indices || !d_values)))))
+    return SWDK_E_ARG;
+  if (out_words < 2 + 2 * m + 2 * nnz_total) return SWDK_E_LIMIT;
+  const int64_t blocks = std::max<int64_t>(1, (m + 7) / 8);  // 8 rows (warps) per block of 256
+  if (blocks > 0x7fffffff) return SWDK_E_LIMIT;
+  k_frechet_records<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(m, m_header, n, d_row_ids, row_id0, d_rowptr,
+                                                                          d_indices, d_values, d_out);
   return cudaGetLastError() == cudaSuccess ? SWDK_OK : SWDK_E_CUDA;
 }
 

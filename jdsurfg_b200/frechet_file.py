@@ -21,6 +21,35 @@ def write_frechet(path, m, n, row_ids, rowptr, indices, values):
             f.write(values[a:b].tobytes())
 
 
+def write_frechet_device(path, m, n, rowptr, indices, values, row_id0=0, row_ids=None, stream=None):
+    """The same file from CSR rows on the device (torch tensors): the record
+    stream is built by swdk_frechet_records_device on the GPU, copied to the
+    host in one piece and written with one write.  `stream` is the CUDA stream
+    handle the rows were made on (None: torch's current stream)."""
+    import ctypes as C
+
+    import torch
+    from .engine import _p, lib
+    L = lib()
+    fn = L.swdk_frechet_records_device
+    vp = C.c_void_p
+    fn.argtypes = [C.c_int64, C.c_int32, C.c_int32, vp, C.c_int32, vp, vp, vp, C.c_int64, vp, C.c_int64, vp]
+    nrow = rowptr.shape[0] - 1
+    nnz = int(rowptr[-1].item()) if nrow > 0 else 0
+    words = 2 + 2 * nrow + 2 * nnz
+    out = torch.empty(words, dtype=torch.int32, device=rowptr.device)
+    sp = stream if stream is not None else torch.cuda.current_stream(rowptr.device).cuda_stream
+    torch.cuda.synchronize(rowptr.device)  # `out` was allocated on torch's stream
+    rc = fn(nrow, m, n, _p(row_ids), int(row_id0), _p(rowptr), _p(indices), _p(values), nnz, _p(out), words,
+            C.c_void_p(sp))
+    if rc != 0:
+        raise RuntimeError(f"swdk_frechet_records_device failed ({rc})")
+    torch.cuda.synchronize(rowptr.device)  # the records were built on `sp`
+    host = out.cpu()
+    with open(path, "wb") as f:
+        f.write(host.numpy().tobytes())
+
+
 def read_frechet(path):
     """-> (m, n, [(row id, idx int32[], val float32[]), ...])"""
     raw = open(path, "rb").read()

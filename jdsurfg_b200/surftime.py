@@ -267,9 +267,9 @@ class SurfTime:
             self.stream.synchronize()
         data = r["ttime"].cpu().numpy()
         nnz = int(idx.shape[0])
-        if outfile is not None:
-            frechet_file.write_frechet(outfile, len(data), n, np.arange(len(data), dtype=np.int32),
-                                       rowptr.cpu().numpy(), idx.cpu().numpy(), val.cpu().numpy())
+        if outfile is not None:  # the record stream is built on the device and written in one piece
+            frechet_file.write_frechet_device(outfile, len(data), n, rowptr, idx, val, row_id0=0,
+                                              stream=self.stream.cuda_stream)
         if return_device:
             return data, nnz, dict(rowptr=rowptr, indices=idx, values=val, n=n, fmst=r)
         return data, nnz

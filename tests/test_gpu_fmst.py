@@ -266,3 +266,24 @@ def test_surftime_compute_grad_against_oracle():
     g *= vs3
     assert np.allclose(data, ref_t, rtol=1e-5, atol=0)
     assert np.abs(grad - g).max() <= 1e-4 * np.abs(g).max()
+
+
+def test_frechet_records_device_equal_host_writer(tmp_path):
+    """The row file built on the device (swdk_frechet_records_device) is
+    byte-identical to the host writer's, with empty rows and a row-id offset
+    (per-rank files start at their first row)."""
+    import torch
+    from jdsurfg_b200 import frechet_file
+    rng = np.random.default_rng(4)
+    m, n = 57, 1234
+    nnz = rng.integers(0, 40, m)
+    nnz[[3, 10]] = 0
+    rowptr = np.concatenate([[0], np.cumsum(nnz)]).astype(np.int64)
+    idx = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in nnz]).astype(np.int32)
+    val = rng.standard_normal(int(rowptr[-1])).astype(np.float32)
+    a, b = str(tmp_path / "host.bin"), str(tmp_path / "dev.bin")
+    frechet_file.write_frechet(a, 999, n, np.arange(17, 17 + m), rowptr, idx, val)
+    dev = torch.device("cuda", 0)
+    frechet_file.write_frechet_device(b, 999, n, torch.from_numpy(rowptr).to(dev), torch.from_numpy(idx).to(dev),
+                                      torch.from_numpy(val).to(dev), row_id0=17)
+    assert open(a, "rb").read() == open(b, "rb").read()
