@@ -120,6 +120,8 @@ class ShardedSurfTime:
         import torch
         blk = lambda a: None if a is None else a[:, c0:c1].contiguous()
         vs_b, vp_b, rho_b = blk(vs), blk(vp), blk(rho)
+        if stream is None and vs.is_cuda:  # order the engine's work with torch's (the gather reads its outputs)
+            stream = torch.cuda.current_stream(vs.device).cuda_stream
         if self.compute is not None:
             np_ = lambda a: None if a is None else a.cpu().numpy()
             r = self.compute(path, np_(vs_b), np_(vp_b), np_(rho_b))

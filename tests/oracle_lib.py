@@ -205,6 +205,18 @@ def kernel_spread(case, cols, rel=1e-15, steps=(-3, -1, 1, 3)):
     return ks, us
 
 
+def kernel_at(case, col, rel):
+    """get_1d_kernel of one column with every phase velocity handed to the
+    eigenfunction routines moved by the relative amount `rel`: the oracle's
+    kernels at another implementation's root when the two roots differ by
+    rel (one REAL*4 ulp after sngl())."""
+    try:
+        lib().swdo_set_eigen_cpert(C.c_double(rel))
+        return get_1d_kernel(case, cols=np.array([col]))
+    finally:
+        lib().swdo_set_eigen_cpert(C.c_double(0.0))
+
+
 def map_spread(case, cols, rel=1e-15, steps=(-3, -1, 1, 3)):
     """The same conditioning probe for get_2d_map: the largest change of vout
     (km/s) per (slot, column) when the phase velocity handed to

@@ -10,6 +10,12 @@ Per grid it prints max and RMS |dc|, |dU| and the kernel error (relative to
 the slot's largest |kernel|).  Tolerances: |dc|, |dU| <= 1e-6 km/s, kernel
 <= 1e-5.
 
+Kernels are compared at the same phase velocity.  Where the GPU's root and
+the oracle's round to different REAL*4 values (one ulp, |dc| ~ 2e-7 km/s,
+within the root tolerance) the oracle's kernel is recomputed at the GPU's
+root before comparing: a kernel at a short period moves by up to a few
+percent under a one-ulp change of c, in the reference as here.
+
 Exemptions are in matching units.  The reference's kernel path is
 ill-conditioned at a few (column, period) points: moving the phase velocity
 handed to sregn96/sregnpu/slegn96/slegnpu by 1e-15 relative then moves U by
@@ -49,6 +55,13 @@ def _report(name, seed):
     scale = np.abs(ref["kernel"]).max(axis=1) + 1e-30
     kr = np.abs(g["kernel"] - ref["kernel"]).max(axis=1) / scale
     assert dc[ok].max() <= TOL_C, f"{name}: max |dc| {dc[ok].max():.3g}"
+    # kernels of slots whose roots differ by a REAL*4 ulp: the oracle at the GPU's root
+    nsame_c = 0
+    for s, col in np.argwhere(ok & (kr > TOL_K) & (dc > 0)):
+        rel = g["vc"][s, col] / ref["vc"][s, col] - 1.0
+        r2 = O.kernel_at(case, int(col), rel)
+        kr[s, col] = np.abs(g["kernel"][s, :, col] - r2["kernel"][s, :, 0]).max() / scale[s, col]
+        nsame_c += 1
     bad = ok & ((du > TOL_U) | (kr > TOL_K))
     bcols = np.nonzero(bad.any(axis=0))[0]
     nexempt = 0
@@ -64,8 +77,8 @@ def _report(name, seed):
     rms = lambda x: float(np.sqrt(np.mean(x[ok] ** 2)))
     line = (f"{name}: {NCOL} columns x {ref['vc'].shape[0]} slots ({int(ok.sum())} with a root): "
             f"|dc| max {dc[ok].max():.3g} rms {rms(dc):.3g} km/s; |dU| max {du[ok].max():.3g} rms {rms(du):.3g} km/s; "
-            f"kernel rel max {kr[ok].max():.3g} rms {rms(kr):.3g}; {nexempt} slots exempted by the oracle's own "
-            f"conditioning")
+            f"kernel rel max {kr[ok].max():.3g} rms {rms(kr):.3g}; {nsame_c} kernels compared at the GPU's root "
+            f"(roots one REAL*4 ulp apart); {nexempt} slots exempted by the oracle's own conditioning")
     print(line)
     return nexempt, int(ok.sum())
 
