@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--split-cols", type=int, default=0,
                     help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
     ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
+    ap.add_argument("--no-node-layers", action="store_true",
+                    help="root search reads the full layer tables instead of rebuilding sublayers from the nodes")
     ap.add_argument("--path", default="kernel", choices=["kernel", "map"],
                     help="kernel: get_1d_kernel (dispersion + depth kernels); map: get_2d_map (phase and group maps "
                          "of travel_time's line-search steps)")
@@ -590,7 +592,8 @@ def main():
         return run_sharded(args, torch, dev, rank, world, pg)
     from jdsurfg_b200 import Engine
     case = workload(args, rank)
-    eng = Engine(device=local, refine=args.refine, split_cols=args.split_cols, block_roots=args.roots_blocks)
+    eng = Engine(device=local, refine=args.refine, split_cols=args.split_cols, block_roots=args.roots_blocks,
+                 node_layers=not args.no_node_layers)
     nets = None
     from jdsurfg_b200 import learn
     eng_nets_on = [args.proposal == "learned"]  # whether the timed engine has the proposal attached
@@ -644,7 +647,7 @@ def main():
         # stage breakdown from one call of an unsplit engine with the same
         # settings (the timed call runs as two overlapping column halves,
         # whose stage times do not add up)
-        probe_eng = Engine(device=local, refine=args.refine, split_cols=-1)
+        probe_eng = Engine(device=local, refine=args.refine, split_cols=-1, node_layers=not args.no_node_layers)
         if eng_nets_on[0]:
             learn.load_proposals(probe_eng)
         probe_eng.setup(case)

@@ -79,6 +79,12 @@ typedef struct swdk_config {
                       default (swdk_autotune sets it)                       */
   int split_cols;  /* calls with at least this many columns run as two
                       concurrent column halves; 0 = 8192, < 0 = never       */
+  int node_layers; /* 1 (default): the root search rebuilds each column's
+                      flattened sublayers from its grid nodes and one
+                      per-depth table (the same arithmetic as the layer
+                      tables, 1 KB per column instead of 8 KB, so the working
+                      set stays in L2); 0: it reads the full layer tables.
+                      Columns with fluid nodes always use the tables.       */
 } swdk_config;
 
 typedef struct swdk_stats {

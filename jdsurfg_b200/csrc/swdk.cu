@@ -5,8 +5,8 @@
 //              grid2LayerModel (SurfaceWave.cpp:113-155), surfdisp96's
 //              sphere() flattening (surfdisp96.f:499-571) and start value
 //              (surfdisp96.f:154-226); writes the REAL*4 layer model
-//              layer-major and bottom-aligned so a warp of columns reads each
-//              layer in one coalesced request.
+//              half-space first and column by column, so each secular
+//              evaluation streams its own column forward.
 //   k_roots  : one thread per (column, root chain); a chain is one
 //              surfdisp96 call (wave, period list, modes 1..M) with the
 //              reference's retry (surfdisp.cpp:94-109); identical chains of
@@ -192,12 +192,12 @@ __device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, cons
 
 __device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
 
-// layer-major, bottom-aligned REAL*4 layers (h, alpha, beta, rho) of the
+// REAL*4 layers (h, alpha, beta, rho), half-space first (layer_index), of the
 // flattened model, one table per wave type (the density transform differs)
-__device__ void write_layers(int L, int ncol, int col, const float* th, const float* a, const float* b,
+__device__ void write_layers(int L, int ncol, int col, int lstride, const float* th, const float* a, const float* b,
                              const float* rR, const float* rL, float4* layR, float4* layL) {
   for (int m = 0; m < L; ++m) {
-    const size_t o = (size_t)(L - 1 - m) * ncol + col;
+    const size_t o = layer_index(L - 1 - m, ncol, col, lstride);
     layR[o] = make_float4(th[m], a[m], b[m], rR[m]);
     layL[o] = make_float4(th[m], a[m], b[m], rL[m]);
   }
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int ldi, int nz, const f
                                               float4* __restrict__ layR, float4* __restrict__ layL,
                                               float4* __restrict__ lay0,
                                               ColInfo* __restrict__ info, float2* __restrict__ chainrule,
-                                              float4* __restrict__ nodefeat) {
+                                              float4* __restrict__ nodefeat, float4* __restrict__ nodes) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   float v[NZMAX], vp[NZMAX], rho[NZMAX], dep[NZMAX];
@@ -278,12 +278,16 @@ __global__ void __launch_bounds__(128) k_prep(int ncol, int ldi, int nz, const f
   b[L - 1] = v[nz - 1];
   r[L - 1] = rho[nz - 1];
   for (int m = 0; m < L; ++m) lay0[(size_t)col * Lmax + m] = make_float4(th[m], a[m], b[m], r[m]);
+  // the grid nodes, from which the root search rebuilds the flattened
+  // sublayers of columns without fluid nodes (LayerView::layer)
+  if (nodes)
+    for (int k2 = 0; k2 < nz; ++k2) nodes[(size_t)col * nz + k2] = make_float4(vp[k2], v[k2], rho[k2], 0.0f);
   ColInfo ci;
   ci.L = L;
   ci.nw = nw;
   ci.valid = valid ? 1 : 0;
   sd96_setup(L, sphere, th, a, b, r, rR, rL, ci);
-  write_layers(L, ncol, col, th, a, b, rR, rL, layR, layL);
+  write_layers(L, ncol, col, Lmax, th, a, b, rR, rL, layR, layL);
   info[col] = ci;
 }
 
@@ -305,8 +309,48 @@ __global__ void k_prep_layers(int nmodel, int nlayer, const float* __restrict__ 
   ci.nw = (b[0] <= 0.0f) ? 1 : 0;
   ci.valid = valid ? 1 : 0;
   sd96_setup(nlayer, sphere, th, a, b, r, rR, rL, ci);
-  write_layers(nlayer, nmodel, col, th, a, b, rR, rL, layR, layL);
+  write_layers(nlayer, nmodel, col, nlayer, th, a, b, rR, rL, layR, layL);
   info[col] = ci;
+}
+
+// The flattening of the standard sublayer grid (no fluid nodes) of a depth
+// vector: thicknesses as grid2LayerModel makes them (4 per node interval,
+// SurfaceWave.cpp:113-155), then sphere()'s loop (surfdisp96.f:499-571,
+// ar = 6370) in the same arithmetic as sd96_setup; one thread.
+__global__ void k_depth_table(int nz, const float* __restrict__ depth, int sphere, DepthLayer* __restrict__ dl) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int L = 4 * nz - 3;
+  const double ar = 6370.0;
+  double dr = 0.0, r0 = ar;
+  for (int m = 0; m < L; ++m) {
+    float th;
+    if (m == L - 1) th = sphere ? 1.0f : 0.0f;  // sphere(): the half-space counts 1 km in the depth sum
+    else {
+      const int i = m >> 2;
+      th = fdiv(fsub(depth[i + 1], depth[i]), 4.0f);
+    }
+    DepthLayer q;
+    q.pad_ = 0.0f;
+    if (sphere) {
+      dr = dadd(dr, (double)th);
+      const double r1 = dsub(ar, dr);
+      const double z0 = dmul(ar, log(ddiv(ar, r0)));
+      const double z1 = dmul(ar, log(ddiv(ar, r1)));
+      q.d = (m == L - 1) ? 0.0f : (float)dsub(z1, z0);
+      q.tmp = ddiv(dadd(ar, ar), dadd(r0, r1));
+      const float btp = (float)q.tmp;
+      q.fR = (float)pow((double)btp, (double)(-2.275f));
+      const float b2 = fmul(btp, btp), b4 = fmul(b2, b2), b5 = fmul(b4, btp);
+      q.fL = fdiv(1.0f, b5);
+      r0 = r1;
+    } else {
+      q.d = th;
+      q.tmp = 1.0;
+      q.fR = 1.0f;
+      q.fL = 1.0f;
+    }
+    dl[m] = q;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -397,6 +441,10 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   V.fast = 0;  // dltar1/dltar4 as the reference writes them
   V.ncol = ncol;
   V.col = ccol;
+  V.lstride = ci.L;  // tables of k_prep_layers: nlayer slots per model
+  V.nodes = nullptr;
+  V.dl = nullptr;
+  V.wave = cd.iwave;
   V.L = ci.L;
   V.llw = ci.llw;
   V.trunc = 0;
@@ -480,6 +528,8 @@ struct RModel {
   long long lay0;   // float4 offset of its layer tables (layR / layL / lay0, Lmax*ncol each)
   long long crs0;   // float2 offset of its chain-rule factors (nz*ncol)
   long long root0;  // offset of its root slots in croot / cstat / prop (nroot*ncol)
+  long long node0;  // float4 offset of its grid nodes (nz*ncol)
+  long long dl0;    // offset of its depth table (Lmax DepthLayer)
   double *vc, *vout, *kernel;
   int32_t* status;
 };
@@ -500,6 +550,7 @@ struct RaggedMap {
   const RBlock* blocks;  // null: one model, items = order[item / ncol] x columns
   const RModel* models;
   int nblocks;
+  int lstride;           // one model: layer slots per column of its tables (Lmax)
 };
 
 template <class T>
@@ -536,7 +587,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      const float2* __restrict__ prop,
                                                      int2* __restrict__ retry_list, unsigned int* __restrict__ retry_count,
                                                      unsigned int retry_cap,
-                                                     unsigned long long* __restrict__ nevals, RaggedMap rg) {
+                                                     unsigned long long* __restrict__ nevals, RaggedMap rg,
+                                                     const float4* __restrict__ nodes,
+                                                     const DepthLayer* __restrict__ dl) {
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
   // the chain's state machine lives in shared memory, so the registers go to
@@ -564,15 +617,16 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         if (item >= (unsigned int)nitems) { exhausted = true; break; }
         item_of = (int)item;
         // the item's model (a ragged batch) or the single model's arrays
-        int mcol = ncol;
-        long long o_col = 0, o_lay = 0, o_root = 0;
+        int mcol = ncol, lstride = rg.lstride;
+        long long o_col = 0, o_lay = 0, o_root = 0, o_node = 0, o_dl = 0;
         if (rg.blocks) {
           const RBlock B = rg.blocks[ragged_find(rg.blocks, rg.nblocks, (long long)item, &RBlock::item0)];
           const RModel& M = rg.models[B.model];
           cd = chains[B.chain];
           col = (int)((long long)item - B.item0);
           mcol = M.ncol;
-          o_col = M.col0; o_lay = M.lay0; o_root = M.root0;
+          lstride = M.Lmax;
+          o_col = M.col0; o_lay = M.lay0; o_root = M.root0; o_node = M.node0; o_dl = M.dl0;
         } else {
           cd = chains[order[item / ncol]];
           col = item % ncol;
@@ -588,11 +642,15 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         V.fast = 1;
         V.ncol = mcol;
         V.col = col;
+        V.lstride = lstride;
         V.L = ci.L;
         V.llw = ci.llw;
         V.trunc = (refine == 1);
         V.htot = ci.htot;
         V.bmax = ci.betmx;
+        V.nodes = (nodes && ci.nw == 0) ? nodes + o_node + (size_t)col * ((lstride + 3) / 4) : nullptr;
+        V.dl = dl + o_dl;
+        V.wave = cd.iwave;
         P.t = periods + cd.t_off;
         P.kmax = cd.np;
         P.nmode = cd.nmode;
@@ -723,7 +781,9 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                const int2* __restrict__ retry_list,
                                                                const unsigned int* __restrict__ retry_count,
                                                                unsigned int retry_cap, unsigned int* __restrict__ queue,
-                                                               unsigned long long* __restrict__ nevals, RaggedMap rg) {
+                                                               unsigned long long* __restrict__ nevals, RaggedMap rg,
+                                                               const float4* __restrict__ nodes,
+                                                               const DepthLayer* __restrict__ dl) {
   __shared__ ChainState sst[128];  // one copy of the warp's chain state per lane
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
@@ -741,8 +801,8 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     LayerView V;
     const int2 rec = retry_list[r];
     const int m = rec.y >> 16, k = rec.y & 0xffff;
-    int mcol = ncol, col;
-    long long o_col = 0, o_lay = 0, o_root = 0;
+    int mcol = ncol, col, lstride = rg.lstride;
+    long long o_col = 0, o_lay = 0, o_root = 0, o_node = 0, o_dl = 0;
     ChainDesc cd;
     if (rg.blocks) {
       const RBlock B = rg.blocks[ragged_find(rg.blocks, rg.nblocks, (long long)rec.x, &RBlock::item0)];
@@ -750,7 +810,8 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
       cd = chains[B.chain];
       col = (int)((long long)rec.x - B.item0);
       mcol = M.ncol;
-      o_col = M.col0; o_lay = M.lay0; o_root = M.root0;
+      lstride = M.Lmax;
+      o_col = M.col0; o_lay = M.lay0; o_root = M.root0; o_node = M.node0; o_dl = M.dl0;
     } else {
       cd = chains[order[rec.x / ncol]];
       col = rec.x % ncol;
@@ -760,11 +821,15 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     V.fast = 1;
     V.ncol = mcol;
     V.col = col;
+    V.lstride = lstride;
     V.L = ci.L;
     V.llw = ci.llw;
     V.trunc = (refine == 1);
     V.htot = ci.htot;
     V.bmax = ci.betmx;
+    V.nodes = (nodes && ci.nw == 0) ? nodes + o_node + (size_t)col * ((lstride + 3) / 4) : nullptr;
+    V.dl = dl + o_dl;
+    V.wave = cd.iwave;
     P.t = periods + cd.t_off;
     P.kmax = cd.np;
     P.nmode = cd.nmode;
@@ -908,7 +973,8 @@ __device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax
   }
   __syncthreads();
 
-  double scr[LMAX * 6];
+  using Scratch = typename std::conditional<love, LoveScratch, RayScratch>::type;
+  Scratch scr;  // up-pass checkpoints and the segment being consumed (per slot thread)
   double kacc[NZMAX], kp[NZMAX];
   NodeSink sink;
   sink.kp = (path == 0) ? kp : nullptr;
@@ -1235,6 +1301,7 @@ struct swdk_ctx {
   bool dirty = true;
   Plan plan[2];  // 0: get_1d_kernel, 1: get_2d_map
   DevBuf layR, layL, lay0, info, chainrule, croot, cstat, nevals, depth_d, ierr, queue;
+  DevBuf nodes, dltab;  // grid nodes and the depth grid's flattening (node-source root search)
   int roots_blocks = 0;
   DevBuf in_vs, in_vp, in_rho, out_vc, out_vout, out_kernel, out_status, in_misc;
   // learned bracket proposals
@@ -1489,14 +1556,26 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
     CK(cudaMemcpyAsync(ctx->depth_d.p, ctx->depth.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
     ctx->depth_dev = ctx->depth_d.p;
   }
+  const bool use_nodes = ctx->cfg.node_layers != 0;
+  if (use_nodes) {
+    CK(ctx->nodes.ensure((size_t)nz * ncol * sizeof(float4)));
+    CK(ctx->dltab.ensure((size_t)Lmax * sizeof(DepthLayer)));
+  }
   CK(cudaMemsetAsync(ctx->nevals.p, 0, NCOUNT * sizeof(unsigned long long), st));
   const bool timing = !ctx->capturing;  // stage events and statistics only on eager calls
   if (timing) CK(cudaEventRecord(ctx->ev[0], st));
-  ctx->launches = 1;
+  ctx->launches = 0;
+  if (use_nodes) {
+    ctx->launches += 1;
+    k_depth_table<<<1, 32, 0, st>>>(nz, ctx->depth_d.as<float>(), ctx->cfg.sphere, ctx->dltab.as<DepthLayer>());
+    CK(cudaGetLastError());
+  }
+  ctx->launches += 1;
   k_prep<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ldi, nz, d_vs, d_vp, d_rho, ctx->depth_d.as<float>(), ctx->cfg.sphere,
                                              Lmax, ctx->layR.as<float4>(), ctx->layL.as<float4>(),
                                              ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                             ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr);
+                                             ctx->chainrule.as<float2>(), wantfeat ? ctx->nodefeat.as<float4>() : nullptr,
+                                             use_nodes ? ctx->nodes.as<float4>() : nullptr);
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(ctx->ev[1], st));
   if (useprop) {
@@ -1525,13 +1604,15 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
       ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(),
       useprop ? ctx->prop.as<float2>() : nullptr, ctx->retry_list.as<int2>(), rctr, rcap,
-      ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0});
+      ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0, Lmax},
+      use_nodes ? ctx->nodes.as<float4>() : nullptr, ctx->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
   k_retry<<<rblocks, 128, 0, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
                                    ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                    ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, ctx->croot.as<double>(),
                                    ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
-                                   ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0});
+                                   ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0, Lmax},
+                                   use_nodes ? ctx->nodes.as<float4>() : nullptr, ctx->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
@@ -1791,6 +1872,7 @@ int swdk_config_default(swdk_config* cfg) {
   cfg->sphere = 1;
   cfg->block_roots = 0;
   cfg->split_cols = 0;
+  cfg->node_layers = 1;
   return SWDK_OK;
 }
 
@@ -1821,6 +1903,7 @@ void swdk_destroy(swdk_ctx* ctx) {
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->layR, &ctx->layL, &ctx->lay0, &ctx->info, &ctx->chainrule, &ctx->croot, &ctx->cstat,
+                    &ctx->nodes, &ctx->dltab,
                     &ctx->nevals, &ctx->depth_d, &ctx->ierr, &ctx->in_vs, &ctx->in_vp, &ctx->in_rho,
                     &ctx->out_vc, &ctx->out_vout, &ctx->out_kernel, &ctx->out_status, &ctx->in_misc,
                     &ctx->queue, &ctx->nodefeat, &ctx->pfeat,
@@ -2228,6 +2311,8 @@ struct swdk_ragged {
   bool useprop = false;
   DevBuf d_models, d_blocks, d_eb[4], d_chains, d_periods, d_slots;
   DevBuf layR, layL, lay0, info, chainrule, croot, cstat, prop, nodefeat, retry_list, retry_ctr, queue, nevals;
+  DevBuf nodes, dltab;
+  long long node_tot = 0, dl_tot = 0;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -2250,15 +2335,23 @@ int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
   CK(cudaMemsetAsync(R->retry_ctr.p, 0, 2 * sizeof(unsigned int), st));
   if (timing) CK(cudaEventRecord(R->ev[0], st));
   R->launches = 0;
+  const bool use_nodes = cfg.node_layers != 0;
   for (int i = 0; i < R->n; ++i) {
     const RModel& M = R->models[i];
     const swdk_call& c = R->calls[i];
+    if (use_nodes) {
+      R->launches += 1;
+      k_depth_table<<<1, 32, 0, st>>>(M.nz, R->ctx[i]->depth_d.as<float>(), cfg.sphere,
+                                      R->dltab.as<DepthLayer>() + M.dl0);
+      CK(cudaGetLastError());
+    }
     R->launches += 1;
     k_prep<<<(M.ncol + 127) / 128, 128, 0, st>>>(
         M.ncol, M.ncol, M.nz, c.d_vs, c.d_vp, c.d_rho, R->ctx[i]->depth_d.as<float>(), cfg.sphere, M.Lmax,
         R->layR.as<float4>() + M.lay0, R->layL.as<float4>() + M.lay0, R->lay0.as<float4>() + M.lay0,
         R->info.as<ColInfo>() + M.col0, R->chainrule.as<float2>() + M.crs0,
-        R->useprop ? R->nodefeat.as<float4>() + M.col0 * FEAT_NODES : nullptr);
+        R->useprop ? R->nodefeat.as<float4>() + M.col0 * FEAT_NODES : nullptr,
+        use_nodes ? R->nodes.as<float4>() + M.node0 : nullptr);
     CK(cudaGetLastError());
   }
   if (timing) CK(cudaEventRecord(R->ev[1], st));
@@ -2279,7 +2372,7 @@ int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
     }
   }
   if (timing) CK(cudaEventRecord(R->ev[5], st));
-  const RaggedMap rg{R->d_blocks.as<RBlock>(), R->d_models.as<RModel>(), (int)R->blocks.size()};
+  const RaggedMap rg{R->d_blocks.as<RBlock>(), R->d_models.as<RModel>(), (int)R->blocks.size(), 0};
   const unsigned int rcap = (unsigned int)std::min<long long>(R->root_tot, 0x7fffffffLL);
   unsigned int* rctr = R->retry_ctr.as<unsigned int>();
   const long long grid = std::min<long long>(R->roots_blocks, (R->nitems + 127) / 128);
@@ -2289,13 +2382,15 @@ int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
       R->layL.as<float4>(), R->info.as<ColInfo>(), cfg.refine, cfg.rtol, cfg.sngl, RETRY_DEFERRED,
       R->croot.as<double>(), R->cstat.as<int32_t>(), R->queue.as<unsigned int>(),
       R->useprop ? R->prop.as<float2>() : nullptr, R->retry_list.as<int2>(), rctr, rcap,
-      R->nevals.as<unsigned long long>(), rg);
+      R->nevals.as<unsigned long long>(), rg, use_nodes ? R->nodes.as<float4>() : nullptr,
+      R->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
   k_retry<<<R->roots_blocks, 128, 0, st>>>(0, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(),
                                            R->layR.as<float4>(), R->layL.as<float4>(), R->info.as<ColInfo>(),
                                            cfg.refine, cfg.rtol, cfg.sngl, R->croot.as<double>(),
                                            R->cstat.as<int32_t>(), R->retry_list.as<int2>(), rctr, rcap, rctr + 1,
-                                           R->nevals.as<unsigned long long>(), rg);
+                                           R->nevals.as<unsigned long long>(), rg,
+                                           use_nodes ? R->nodes.as<float4>() : nullptr, R->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(R->ev[2], st));
   if (R->path != 2) {
@@ -2357,7 +2452,8 @@ void swdk_ragged_destroy(swdk_ragged* R) {
   if (R->graph) cudaGraphDestroy(R->graph);
   DevBuf* bufs[] = {&R->d_models, &R->d_blocks, &R->d_eb[0], &R->d_eb[1], &R->d_eb[2], &R->d_eb[3], &R->d_chains,
                     &R->d_periods, &R->d_slots, &R->layR, &R->layL, &R->lay0, &R->info, &R->chainrule, &R->croot,
-                    &R->cstat, &R->prop, &R->nodefeat, &R->retry_list, &R->retry_ctr, &R->queue, &R->nevals};
+                    &R->cstat, &R->prop, &R->nodefeat, &R->retry_list, &R->retry_ctr, &R->queue, &R->nevals,
+                    &R->nodes, &R->dltab};
   for (DevBuf* b : bufs) b->release();
   for (cudaEvent_t& e : R->ev)
     if (e) cudaEventDestroy(e);
@@ -2377,7 +2473,8 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
     const swdk_ctx* c = ctxs[i];
     const swdk_call& k = calls[i];
     if (!c || k.path != path || c->cfg.device != ctx->cfg.device || c->cfg.refine != ctx->cfg.refine ||
-        c->cfg.rtol != ctx->cfg.rtol || c->cfg.sngl != ctx->cfg.sngl || c->cfg.sphere != ctx->cfg.sphere)
+        c->cfg.rtol != ctx->cfg.rtol || c->cfg.sngl != ctx->cfg.sngl || c->cfg.sphere != ctx->cfg.sphere ||
+        c->cfg.node_layers != ctx->cfg.node_layers)
       return fail(ctx, SWDK_E_ARG, "ragged batch: every model needs the same path, device and root settings");
     if (k.nx <= 0 || k.ny <= 0 || !k.d_vs || (path != 2 && (!k.d_vc || !k.d_vout || (path == 0 && !k.d_kernel))))
       return fail(ctx, SWDK_E_ARG, "ragged batch: bad call arguments");
@@ -2414,6 +2511,8 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
     M.lay0 = R->lay_tot;
     M.crs0 = R->crs_tot;
     M.root0 = R->root_tot;
+    M.node0 = R->node_tot;
+    M.dl0 = R->dl_tot;
     M.vc = k.d_vc;
     M.vout = k.d_vout;
     M.kernel = k.d_kernel;
@@ -2423,6 +2522,8 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
     R->lay_tot += (long long)M.Lmax * M.ncol;
     R->crs_tot += (long long)M.nz * M.ncol;
     R->root_tot += (long long)P.nroot * M.ncol;
+    R->node_tot += (long long)M.nz * M.ncol;
+    R->dl_tot += M.Lmax;
     R->slots_tot += (long long)P.kmax;
     R->maxL = std::max(R->maxL, M.Lmax);
     R->maxnz = std::max(R->maxnz, M.nz);
@@ -2485,6 +2586,8 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
   if (e == cudaSuccess) e = R->lay0.ensure((size_t)R->lay_tot * sizeof(float4));
   if (e == cudaSuccess) e = R->info.ensure((size_t)R->ncol_tot * sizeof(ColInfo));
   if (e == cudaSuccess) e = R->chainrule.ensure((size_t)R->crs_tot * sizeof(float2));
+  if (e == cudaSuccess) e = R->nodes.ensure((size_t)R->node_tot * sizeof(float4));
+  if (e == cudaSuccess) e = R->dltab.ensure((size_t)R->dl_tot * sizeof(DepthLayer));
   if (e == cudaSuccess) e = R->croot.ensure((size_t)R->root_tot * sizeof(double));
   if (e == cudaSuccess) e = R->cstat.ensure((size_t)R->root_tot * sizeof(int32_t));
   if (e == cudaSuccess && R->useprop) e = R->prop.ensure((size_t)R->root_tot * sizeof(float2));

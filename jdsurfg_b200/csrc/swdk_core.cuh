@@ -101,20 +101,90 @@ SWDK_HD int pow2_exponent(double t) {
   return e;
 }
 
+// Element (layer counted from the half-space up, column) of a layer table.
+// Column-major: each column's layers are contiguous, half-space first, so a
+// secular evaluation (half-space upward) streams its column forward and a
+// lane's consecutive layers share cache sectors whatever column the other
+// lanes of its warp work on.
+SWDK_HD size_t layer_index(int up, int ncol, int col, int lstride) {
+#ifdef SWDK_LAYER_ROWMAJOR
+  (void)lstride;
+  return (size_t)up * ncol + col;
+#else
+  (void)ncol;
+  return (size_t)col * lstride + up;
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // secular functions on the flattened REAL*4 layer model
-//   lay[mp*ncol + col] = (d, a, b, rho), mp = 0 is the half-space and mp
-//   counts layers upward (bottom-aligned, layer-major)
+//   lay[layer_index(mp, ncol, col, lstride)] = (d, a, b, rho), mp = 0 is the
+//   half-space and mp counts layers upward
 // ---------------------------------------------------------------------------
+// Flattening of one sublayer of the standard grid (grid2LayerModel without
+// fluid nodes, then surfdisp96's sphere()): the flattened thickness, the
+// velocity factor and the Rayleigh / Love density factors.  They depend on
+// the depth grid only, so one table serves every column.
+struct DepthLayer {
+  double tmp;       // a, b -> (float)((double)a * tmp)
+  float d, fR, fL;  // flattened thickness; rho -> rho * fR (Rayleigh) or * fL (Love)
+  float pad_;
+};
+
 struct LayerView {
   const float4* lay;   // (d, a, b, rho) REAL*4 as surfdisp96 holds them
   int fast;            // 1: secular_fast (recip()-based), 0: dltar1/dltar4 as written
   int ncol, col;
+  int lstride;  // layer slots per column of the table (column-major layout)
   int L;    // layers including the half-space
   int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
   int trunc;          // secular_fast may cut the depth (secular_depth)
   float htot, bmax;   // total finite-layer thickness and largest shear velocity
-  SWDK_HD size_t idx(int m) const { return (size_t)(L - 1 - m) * ncol + col; }
+  // node source (null: the layer table): the column's grid nodes
+  // (vp, vs, rho, -) and the depth grid's flattening factors
+  const float4* nodes;
+  const DepthLayer* dl;
+  int wave;  // 2 Rayleigh, 1 Love: which density factor
+  SWDK_HD size_t idx(int m) const { return layer_index(L - 1 - m, ncol, col, lstride); }
+  // layer m (top-down) of the flattened REAL*4 model, from the table or
+  // rebuilt from the nodes with the arithmetic of the model preparation:
+  // sublayer j of node interval i is v_i + (2j+1)(v_{i+1} - v_i)/8 in REAL*4
+  // (grid2LayerModel, SurfaceWave.cpp:113-155), then a, b times tmp and rho
+  // times the wave's density factor (sphere(), surfdisp96.f:499-571)
+  SWDK_HD float4 layer(int m) const {
+    if (!nodes) return lay[idx(m)];
+    const DepthLayer& q = dl[m];
+    float ai, bi, ri;
+    if (m == L - 1) {
+      const float4 n = nodes[(L + 3) / 4 - 1];
+      ai = n.x; bi = n.y; ri = n.z;
+    } else {
+      const int i = m >> 2;
+      const float4 n0 = nodes[i], n1 = nodes[i + 1];
+      const float w = (float)(2 * (m & 3) + 1);
+#ifdef __CUDA_ARCH__
+      ai = (float)__dadd_rn((double)n0.x, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.x, n0.x)), 0.125));
+      bi = (float)__dadd_rn((double)n0.y, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.y, n0.y)), 0.125));
+      ri = (float)__dadd_rn((double)n0.z, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.z, n0.z)), 0.125));
+#else
+      ai = (float)((double)n0.x + (double)(w * (n1.x - n0.x)) * 0.125);
+      bi = (float)((double)n0.y + (double)(w * (n1.y - n0.y)) * 0.125);
+      ri = (float)((double)n0.z + (double)(w * (n1.z - n0.z)) * 0.125);
+#endif
+    }
+    float4 out;
+    out.x = q.d;
+#ifdef __CUDA_ARCH__
+    out.y = (float)__dmul_rn((double)ai, q.tmp);
+    out.z = (float)__dmul_rn((double)bi, q.tmp);
+    out.w = __fmul_rn(ri, wave == 2 ? q.fR : q.fL);
+#else
+    out.y = (float)((double)ai * q.tmp);
+    out.z = (float)((double)bi * q.tmp);
+    out.w = ri * (wave == 2 ? q.fR : q.fL);
+#endif
+    return out;
+  }
   SWDK_HD float4 get(int m) const {  // m: reference (top-down, 0-based) index
     return lay[idx(m)];
   }
@@ -419,7 +489,7 @@ SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
   const double wvno2 = wvno * wvno;
   double cum = 0.0;
   for (int m = V.llw - 1; m < V.L - 2; ++m) {
-    const float4 ly = V.lay[V.idx(m)];
+    const float4 ly = V.layer(m);
     if (ly.z > 0.0f) {
       const double xkb = omega * recip((double)ly.z);
       const double x2 = wvno2 - xkb * xkb;
@@ -437,7 +507,7 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   const double wvno2 = wvno * wvno;
   const double iom = 1.0 / omega;
   const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
-  const float4 h = V.lay[V.idx(hs)];
+  const float4 h = V.layer(hs);
   double xka = omega * recip((double)h.y), xkb = omega * recip((double)h.z);
   const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
   const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
@@ -454,10 +524,10 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   const int mlo = V.llw - 1;
   int since = 0;
   // the next layer's float4 is loaded one layer ahead of its use
-  float4 ly = V.lay[V.idx(hs - 1 >= mlo ? hs - 1 : mlo)];
+  float4 ly = V.layer(hs - 1 >= mlo ? hs - 1 : mlo);
   for (int m = hs - 1; m >= mlo; --m) {
     const float4 cur_ly = ly;
-    if (m > mlo) ly = V.lay[V.idx(m - 1)];
+    if (m > mlo) ly = V.layer(m - 1);
     const LayerCoef cur = layer_coef(cur_ly, wvno, wvno2, omega, iom);
     apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
     if (++since >= NORM || m == mlo) {
@@ -473,7 +543,7 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
     }
   }
   if (V.llw != 1) {
-    const float4 ly = V.lay[V.idx(0)];
+    const float4 ly = V.layer(0);
     const double dpth = ly.x, rho = ly.w;
     xka = omega * recip((double)ly.y);
     const double Xa = (wvno + xka) * fabs(wvno - xka);
@@ -501,7 +571,7 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
 template <int NORM>
 SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
   const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
-  float4 h = V.lay[V.idx(hs)];
+  float4 h = V.layer(hs);
   double beta1 = h.z, rho1 = h.w;
   double xkb = omega * recip(beta1);
   double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
@@ -510,10 +580,10 @@ SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
   int since = 0;
   const int mlo = V.llw - 1;
   // the next layer's float4 is loaded one layer ahead of its use
-  float4 nx = V.lay[V.idx(hs - 1 >= mlo ? hs - 1 : mlo)];
+  float4 nx = V.layer(hs - 1 >= mlo ? hs - 1 : mlo);
   for (int m = hs - 1; m >= mlo; --m) {
     const float4 ly = nx;
-    if (m > mlo) nx = V.lay[V.idx(m - 1)];
+    if (m > mlo) nx = V.layer(m - 1);
     beta1 = ly.z;
     rho1 = ly.w;
     const double dpth = ly.x;

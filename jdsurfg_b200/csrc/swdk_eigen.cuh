@@ -533,50 +533,77 @@ SWDK_HD int pass_layers(const Layer* lay, int L, double k2, double om2, double t
 
 constexpr double EIG_TRUNC_Q = 40.0;
 
+// Up-pass storage of a Rayleigh pass with checkpoints: the compound vector
+// (and its exponent bookkeeping) is kept only at every RAY_SEG-th layer and
+// at the half-space; the down sweep recomputes each segment of RAY_SEG
+// layers from its checkpoint into seg[] just before it needs them.  The
+// recomputation repeats the up pass's arithmetic exactly, so the values are
+// the ones a full per-layer store would hold, with about 2 KB of scratch per
+// slot instead of 6 doubles per layer.
+constexpr int RAY_SEG = 16;
+constexpr int RAY_NCK = (LMAX + RAY_SEG - 1) / RAY_SEG;
+struct RayScratch {
+  double ck[RAY_NCK][8];  // layer j*RAY_SEG: cd[5], exponent sum, exr, exi
+  double hs[8];           // the half-space start of the (cut) pass
+  double seg[RAY_SEG][6];  // the segment being consumed: cd[5], exponent sum
+};
+
+// one step of the up pass (sregn96.f90:401-489): the compound vector cd of
+// layer m from that of layer m+1 (cp, in place), with its exponent sum
+SWDK_HD void ray_up_step(const RayLayer& y, const SlotK& s, double* cd, double& exr, int& exi) {
+  const int iw = (y.zb > 0.0) ? 0 : 1;
+  LVars v;
+  vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
+  double ee[5];
+  dnka_apply(v, y, iw, s, cd, ee);
+  double t1 = 0.0;
+  for (int i = 0; i < 5; ++i) t1 = fmax(t1, fabs(ee[i]));
+  int e = 0;
+  double sc = 1.0;
+  if (t1 >= 1.e-40) e = pow2_norm(t1, sc);
+  for (int i = 0; i < 5; ++i) cd[i] = ee[i] * sc;
+  exr = exr + v.pex + v.svex;
+  exi += e;
+  cd[5] = exr + (double)exi * LN2;
+}
+
+SWDK_HD void ray_keep(double* dst, const double* cd, double exr, int exi) {
+  for (int i = 0; i < 6; ++i) dst[i] = cd[i];
+  dst[6] = exr;
+  dst[7] = (double)exi;
+}
+
 // One Rayleigh pass (sregn96's svfunc + energy) at (omega, wvno) over the
 // column's layer records lay[0..L-1] (top-down, lay[L-1] the half-space),
-// depth-truncated by pass_layers.  scr: 6 doubles per layer (up-pass
-// compound vector and its exponent).  Returns ugr (flat) and
-// norm = ugr*sumi0; the raw layer kernels go to the sink as the top-down
-// sweep produces them.
+// depth-truncated by pass_layers.  Returns ugr (flat) and norm = ugr*sumi0;
+// the raw layer kernels go to the sink as the top-down sweep produces them.
 template <class Sink>
-SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double wvno, double* scr, double& ugr,
+SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double wvno, RayScratch& scr, double& ugr,
                             double& norm, const Sink& sink, double trunc_q = EIG_TRUNC_Q) {
   const SlotK s = slot_consts(omega, wvno);
   const int L = pass_layers(lay, Lfull, s.k2, s.om2, trunc_q);
-  // ---- up (sregn96.f90:401-489) ----
+  // ---- up (sregn96.f90:401-489), checkpoints only ----
+  double cd[6];
   {
     const RayLayer& y = lay[L - 1];
-    double* c0 = scr + 6 * (L - 1);
-    halfspace_gbr(y, (y.zb > 0.0) ? 0 : 1, s, c0);
-    c0[5] = 0.0;
+    halfspace_gbr(y, (y.zb > 0.0) ? 0 : 1, s, cd);
+    cd[5] = 0.0;
   }
   double exr = 0.0;
   int exi = 0;
+  ray_keep(scr.hs, cd, exr, exi);
+  if ((L - 1) % RAY_SEG == 0) ray_keep(scr.ck[(L - 1) / RAY_SEG], cd, exr, exi);
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = L - 2; m >= 0; --m) {
-    const RayLayer& y = lay[m];
-    const int iw = (y.zb > 0.0) ? 0 : 1;
-    LVars v;
-    vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
-    double ee[5];
-    dnka_apply(v, y, iw, s, scr + 6 * (m + 1), ee);
-    double t1 = 0.0;
-    for (int i = 0; i < 5; ++i) t1 = fmax(t1, fabs(ee[i]));
-    int e = 0;
-    double sc = 1.0;
-    if (t1 >= 1.e-40) e = pow2_norm(t1, sc);
-    double* cm = scr + 6 * m;
-    for (int i = 0; i < 5; ++i) cm[i] = ee[i] * sc;
-    exr = exr + v.pex + v.svex;
-    exi += e;
-    cm[5] = exr + (double)exi * LN2;
+    ray_up_step(lay[m], s, cd, exr, exi);
+    if (m % RAY_SEG == 0) ray_keep(scr.ck[m / RAY_SEG], cd, exr, exi);
   }
   // ---- down + svfunc + energy, top-down ----
-  const double if1213 = -1.0 / scr[1];
-  const double exe0 = scr[5];
+  const double* top = scr.ck[0];  // layer 0
+  const double if1213 = -1.0 / top[1];
+  const double exe0 = top[5];
   Eig4 u0;
-  u0.ur = scr[2] / scr[1];
+  u0.ur = top[2] / top[1];
   u0.uz = 1.0; u0.tz = 0.0; u0.tr = 0.0;
   if (lay[0].zb <= 0.0) { u0.ur = 0.0; u0.tr = 0.0; }  // fluid top (jwat)
   double vv[4] = {1.0, 0.0, 0.0, 0.0};
@@ -586,6 +613,22 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
   const double c = omega * s.ik;
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int m = 0; m < L; ++m) {
+    const int j0 = m - m % RAY_SEG;  // first layer of m's segment
+    if (m == j0 && m < L - 1) {
+      // cd of layers j0+1 .. t from the checkpoint at t
+      const int t = (j0 + RAY_SEG < L - 1) ? j0 + RAY_SEG : L - 1;
+      const double* src = (t == L - 1) ? scr.hs : scr.ck[t / RAY_SEG];
+      double w[6];
+      for (int i = 0; i < 6; ++i) w[i] = src[i];
+      double rexr = src[6];
+      int rexi = (int)src[7];
+      for (int i = 0; i < 6; ++i) scr.seg[t - j0 - 1][i] = w[i];
+#pragma unroll 1
+      for (int l = t - 1; l > j0; --l) {
+        ray_up_step(lay[l], s, w, rexr, rexi);
+        for (int i = 0; i < 6; ++i) scr.seg[l - j0 - 1][i] = w[i];
+      }
+    }
     const RayLayer& y = lay[m];
     const int iw = (y.zb > 0.0) ? 0 : 1;
     const bool half = (m == L - 1);
@@ -603,7 +646,7 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
       dxr = dxr + v.pex;
       dxi += e;
       const double exa1 = dxr + (double)dxi * LN2;
-      const double* cd1 = scr + 6 * (m + 1);
+      const double* cd1 = scr.seg[m - j0];  // layer m + 1
       u1 = eigen_at(cd1, vv, exa1 + cd1[5] - exe0, if1213);
     }
     double da, db, dr;
@@ -616,145 +659,184 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
 }
 
 // ---------------------------------------------------------------------------
-// One Love pass (slegn96.f90): up, shfunc normalisation, energy.  scr holds
-// 3 doubles per layer (uu, tt, exl).  Returns ugr and the normaliser sumi1.
+// One Love pass (slegn96.f90): up, shfunc normalisation, energy.  The up
+// pass keeps (uu, tt, exl) only at every RAY_SEG-th layer and the
+// half-space; the energy sweep recomputes each segment from its checkpoint
+// and applies shfunc's normalisation exp(-ext) on the fly.  Returns ugr and
+// the normaliser sumi1.
 // ---------------------------------------------------------------------------
+struct LoveScratch {
+  double ck[RAY_NCK][3];
+  double hs[3];
+  double seg[RAY_SEG + 1][3];  // layers j0 .. j0 + RAY_SEG of the current segment
+};
+
+// one step of slegn96's up pass (slegn96.f90:372-445): (uu, tt) of layer k
+// from layer k+1 (s1), power-of-two normalised, and the step's exponent exl
+SWDK_HD void love_up_step(const LoveLayer& y, double wvno2, double om2, const double* s1, double* sk) {
+  if (!(y.zb > 0.0)) { sk[0] = 0.0; sk[1] = 0.0; sk[2] = 0.0; return; }
+  const double dpth = y.d;
+  const double x2 = wvno2 - om2 * y.ib2;  // (wvno + xkb)(wvno - xkb)
+  double cosq, yl, zl, eexl = 0.0;
+  if (x2 < 0.0) {  // wvno < xkb
+    const double ir = rsqrt(-x2), rb = -x2 * ir;
+    double sq, cq;
+    sincos(rb * dpth, &sq, &cq);
+    yl = sq * ir; zl = -rb * sq; cosq = cq;
+  } else if (x2 == 0.0) {
+    cosq = 1.0; yl = dpth; zl = 0.0;
+  } else {
+    const double ir = rsqrt(x2), rb = x2 * ir, q = rb * dpth;
+    eexl = q;
+    const double e1 = (q < 18.0) ? exp(-q) : 0.0;
+    const double fac = e1 * e1;  // exp(-2q)
+    cosq = (1.0 + fac) * 0.5;
+    const double sq = (1.0 - fac) * 0.5;
+    yl = sq * ir; zl = rb * sq;
+  }
+  const double a11 = cosq, a22 = cosq, a12 = -(yl * y.imu), a21 = -(zl * y.mu);
+  const double amp0 = a11 * s1[0] + a12 * s1[1];
+  const double str0 = a21 * s1[0] + a22 * s1[1];
+  const double rr = fmax(fabs(amp0), fabs(str0));
+  int e = 0;
+  double sc = 1.0;
+  if (rr >= 1.e-30) e = pow2_norm(rr, sc);
+  sk[0] = amp0 * sc;
+  sk[1] = str0 * sc;
+  sk[2] = (double)e * LN2 + eexl;
+}
+
+// the raw up-pass values of layers j0 .. t (t the checkpoint at or below
+// j0 + RAY_SEG) into seg[0 .. t - j0]
+SWDK_HD void love_fill_segment(const LoveLayer* lay, int L, double wvno2, double om2, LoveScratch& scr, int j0) {
+  const int t = (j0 + RAY_SEG < L - 1) ? j0 + RAY_SEG : L - 1;
+  const double* src = (t == L - 1) ? scr.hs : scr.ck[t / RAY_SEG];
+  for (int i = 0; i < 3; ++i) scr.seg[t - j0][i] = src[i];
+#pragma unroll 1
+  for (int l = t - 1; l >= j0; --l) love_up_step(lay[l], wvno2, om2, scr.seg[l - j0 + 1], scr.seg[l - j0]);
+}
+
 template <class Sink>
-SWDK_HDI void love_pass(const LoveLayer* lay, int Lfull, double omega, double wvno, double* scr, double& ugr,
+SWDK_HDI void love_pass(const LoveLayer* lay, int Lfull, double omega, double wvno, LoveScratch& scr, double& ugr,
                         double& norm, const Sink& sink, double trunc_q = EIG_TRUNC_Q) {
   const double wvno2 = wvno * wvno, om2 = omega * omega, ik = 1.0 / wvno, ik2 = ik * ik;
   const int L = pass_layers(lay, Lfull, wvno2, om2, trunc_q);
-  // ---- up (slegn96.f90:372-445) ----
+  // ---- up (slegn96.f90:372-445), checkpoints only ----
+  double sv[3];
   {
     const LoveLayer& y = lay[L - 1];
-    double* s0 = scr + 3 * (L - 1);
     if (y.zb > (double)0.01f) {
       const double rb = sqrt(fabs(wvno2 - om2 * y.ib2));
-      s0[0] = 1.0;
-      s0[1] = -y.mu * rb;
+      sv[0] = 1.0;
+      sv[1] = -y.mu * rb;
     } else {
-      s0[0] = 1.0;
-      s0[1] = 0.0;
+      sv[0] = 1.0;
+      sv[1] = 0.0;
     }
-    s0[2] = 0.0;
+    sv[2] = 0.0;
   }
+  for (int i = 0; i < 3; ++i) scr.hs[i] = sv[i];
+  if ((L - 1) % RAY_SEG == 0)
+    for (int i = 0; i < 3; ++i) scr.ck[(L - 1) / RAY_SEG][i] = sv[i];
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = L - 2; k >= 0; --k) {
-    double* sk = scr + 3 * k;
-    const LoveLayer& y = lay[k];
-    if (!(y.zb > 0.0)) { sk[0] = 0.0; sk[1] = 0.0; sk[2] = 0.0; continue; }
-    const double dpth = y.d;
-    const double x2 = wvno2 - om2 * y.ib2;  // (wvno + xkb)(wvno - xkb)
-    double cosq, yl, zl, eexl = 0.0;
-    if (x2 < 0.0) {  // wvno < xkb
-      const double ir = rsqrt(-x2), rb = -x2 * ir;
-      double sq, cq;
-      sincos(rb * dpth, &sq, &cq);
-      yl = sq * ir; zl = -rb * sq; cosq = cq;
-    } else if (x2 == 0.0) {
-      cosq = 1.0; yl = dpth; zl = 0.0;
-    } else {
-      const double ir = rsqrt(x2), rb = x2 * ir, q = rb * dpth;
-      eexl = q;
-      const double e1 = (q < 18.0) ? exp(-q) : 0.0;
-      const double fac = e1 * e1;  // exp(-2q)
-      cosq = (1.0 + fac) * 0.5;
-      const double sq = (1.0 - fac) * 0.5;
-      yl = sq * ir; zl = rb * sq;
-    }
-    const double a11 = cosq, a22 = cosq, a12 = -(yl * y.imu), a21 = -(zl * y.mu);
-    const double* s1 = scr + 3 * (k + 1);
-    const double amp0 = a11 * s1[0] + a12 * s1[1];
-    const double str0 = a21 * s1[0] + a22 * s1[1];
-    const double rr = fmax(fabs(amp0), fabs(str0));
-    int e = 0;
-    double sc = 1.0;
-    if (rr >= 1.e-30) e = pow2_norm(rr, sc);
-    sk[0] = amp0 * sc;
-    sk[1] = str0 * sc;
-    sk[2] = (double)e * LN2 + eexl;
+    double nv[3];
+    love_up_step(lay[k], wvno2, om2, sv, nv);
+    for (int i = 0; i < 3; ++i) sv[i] = nv[i];
+    if (k % RAY_SEG == 0)
+      for (int i = 0; i < 3; ++i) scr.ck[k / RAY_SEG][i] = sv[i];
   }
-  // ---- shfunc normalisation (slegn96.f90:212-240) ----
-  double ext = 0.0;
-  double umax = scr[0];
-  scr[1] = 0.0;  // tt(1) = 0
-#pragma unroll 1  // a layer recursion: unrolling only grows the code
-  for (int k = 1; k < L; ++k) {
-    double* sk = scr + 3 * k;
-    if (lay[k].zb > 0.0) {
-      ext = ext + scr[3 * (k - 1) + 2];
-      const double fact = (ext < 80.0) ? exp(-ext) : 0.0;
-      sk[0] = sk[0] * fact;
-      sk[1] = sk[1] * fact;
-    } else {
-      sk[0] = 0.0; sk[1] = 0.0;
+  // ---- shfunc normalisation (slegn96.f90:212-240): layer k's (uu, tt)
+  // are the raw values times exp(-ext), ext summing the exl of the solid
+  // layers above; tt(1) = 0.  The amplitude scale umax is uu(1) unless
+  // that is zero (a fluid top), then the largest normalised |uu|. ----
+  const double top0 = scr.ck[0][0];
+  double umax = top0;
+  if (top0 == 0.0) {
+    double ext = 0.0;
+#pragma unroll 1
+    for (int k = 1; k < L; ++k) {
+      const int j0 = (k - 1) - (k - 1) % RAY_SEG;
+      if (k - 1 == j0) love_fill_segment(lay, L, wvno2, om2, scr, j0);
+      double u = 0.0;
+      if (lay[k].zb > 0.0) {
+        ext = ext + scr.seg[k - 1 - j0][2];
+        const double fact = (ext < 80.0) ? exp(-ext) : 0.0;
+        u = scr.seg[k - j0][0] * fact;
+      }
+      if (fabs(u) > fabs(umax)) umax = u;
     }
-    if (fabs(sk[0]) > fabs(umax)) umax = sk[0];
   }
-  if (scr[0] != 0.0) umax = scr[0];
   const double iumax = (fabs(umax) > 0.0) ? 1.0 / umax : 1.0;
   // ---- energy (slegn96.f90:447-576) with uu/tt scaled by 1/umax on the fly ----
   const double c = omega * ik;
   double sumi0 = 0.0, sumi1 = 0.0;
-  double prev_uu = scr[0] * iumax, prev_tt = scr[1] * iumax;
+  double ext = 0.0;
+  double uu = top0 * iumax, tt = 0.0;
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = 0; k < L; ++k) {
-    const double uu = prev_uu, tt = prev_tt;
+    const int j0 = k - k % RAY_SEG;
     double nuu = 0.0, ntt = 0.0;
     if (k < L - 1) {
-      nuu = scr[3 * (k + 1)] * iumax;
-      ntt = scr[3 * (k + 1) + 1] * iumax;
+      if (k == j0) love_fill_segment(lay, L, wvno2, om2, scr, j0);
+      if (lay[k + 1].zb > 0.0) {
+        ext = ext + scr.seg[k - j0][2];
+        const double fact = (ext < 80.0) ? exp(-ext) : 0.0;
+        nuu = scr.seg[k + 1 - j0][0] * fact * iumax;
+        ntt = scr.seg[k + 1 - j0][1] * fact * iumax;
+      }
     }
-    prev_uu = nuu;
-    prev_tt = ntt;
     const LoveLayer& y = lay[k];
     const double zb = y.zb;
-    if (!(zb > 0.0)) continue;
-    const double drho = y.zr, dpth = y.d, dmu = y.mu;
-    const double x2 = wvno2 - om2 * y.ib2;
-    double rb = 0.0, irb = 0.0;
-    if (x2 != 0.0) {
-      irb = rsqrt(fabs(x2));
-      rb = fabs(x2) * irb;
-    }
-    if (rb < 1.0e-10) { rb = 1.0e-10; irb = 1.0e10; }
-    double upup, dupdup;
-    if (k == L - 1) {
-      upup = (0.5 * irb) * uu * uu;
-      dupdup = (0.5 * rb) * uu * uu;
-    } else {
-      const bool real = !(x2 < 0.0);  // nub = rb, or i rb when wvno < xkb
-      // ei11 = ei21 = 0.5/wvno, ei12 = -ei22 = 0.5/(wvno dmu nub)
-      const double e0 = 0.5 * ik;
-      const cx ei12 = rinv(real, 0.5 * ik * y.imu * irb);
-      const cx km1dn = mkc(e0 * uu) - ei12 * tt;
-      const cx kmup = mkc(e0 * nuu) + ei12 * ntt;
-      const double q = rb * dpth;
-      cx f, g;
-      if (real) {
-        const double e1 = (q < 75.0) ? exp(-q) : 0.0;
-        const double e2 = (q < 40.0) ? e1 * e1 : 0.0;  // exp(-2 nub d)
-        f = mkc((1.0 - e2) * 0.5 * irb, 0.0);
-        g = mkc(dpth * e1, 0.0);
-      } else {
-        double sn, cs;
-        sincos(q, &sn, &cs);
-        f = mkc(sn * cs * irb, -sn * sn * irb);
-        g = mkc(dpth * cs, -dpth * sn);
+    if (zb > 0.0) {
+      const double drho = y.zr, dpth = y.d, dmu = y.mu;
+      const double x2 = wvno2 - om2 * y.ib2;
+      double rb = 0.0, irb = 0.0;
+      if (x2 != 0.0) {
+        irb = rsqrt(fabs(x2));
+        rb = fabs(x2) * irb;
       }
-      const cx f1 = f * (wvno2 * (kmup * kmup + km1dn * km1dn));
-      const cx f2 = g * (2.0 * wvno2) * kmup * km1dn;
-      upup = (f1 + f2).re;
-      const double nub2 = real ? rb * rb : -rb * rb;
-      dupdup = nub2 * (f1 - f2).re;
+      if (rb < 1.0e-10) { rb = 1.0e-10; irb = 1.0e10; }
+      double upup, dupdup;
+      if (k == L - 1) {
+        upup = (0.5 * irb) * uu * uu;
+        dupdup = (0.5 * rb) * uu * uu;
+      } else {
+        const bool real = !(x2 < 0.0);  // nub = rb, or i rb when wvno < xkb
+        // ei11 = ei21 = 0.5/wvno, ei12 = -ei22 = 0.5/(wvno dmu nub)
+        const double e0 = 0.5 * ik;
+        const cx ei12 = rinv(real, 0.5 * ik * y.imu * irb);
+        const cx km1dn = mkc(e0 * uu) - ei12 * tt;
+        const cx kmup = mkc(e0 * nuu) + ei12 * ntt;
+        const double q = rb * dpth;
+        cx f, g;
+        if (real) {
+          const double e1 = (q < 75.0) ? exp(-q) : 0.0;
+          const double e2 = (q < 40.0) ? e1 * e1 : 0.0;  // exp(-2 nub d)
+          f = mkc((1.0 - e2) * 0.5 * irb, 0.0);
+          g = mkc(dpth * e1, 0.0);
+        } else {
+          double sn, cs;
+          sincos(q, &sn, &cs);
+          f = mkc(sn * cs * irb, -sn * sn * irb);
+          g = mkc(dpth * cs, -dpth * sn);
+        }
+        const cx f1 = f * (wvno2 * (kmup * kmup + km1dn * km1dn));
+        const cx f2 = g * (2.0 * wvno2) * kmup * km1dn;
+        upup = (f1 + f2).re;
+        const double nub2 = real ? rb * rb : -rb * rb;
+        dupdup = nub2 * (f1 - f2).re;
+      }
+      sumi0 = sumi0 + drho * upup;
+      sumi1 = sumi1 + dmu * upup;
+      const double VSHH = zb, VSHV = zb;
+      const double DCDBH = c * drho * VSHH * upup;
+      const double DCDBV = c * drho * VSHV * dupdup * ik2;
+      sink.add(k, y.vtp, y.rtp, 0.0, DCDBH + DCDBV,
+               0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup * ik2));
     }
-    sumi0 = sumi0 + drho * upup;
-    sumi1 = sumi1 + dmu * upup;
-    const double VSHH = zb, VSHV = zb;
-    const double DCDBH = c * drho * VSHH * upup;
-    const double DCDBV = c * drho * VSHV * dupdup * ik2;
-    sink.add(k, y.vtp, y.rtp, 0.0, DCDBH + DCDBV,
-             0.5 * c * (-c * c * upup + VSHH * VSHH * upup + VSHV * VSHV * dupdup * ik2));
+    uu = nuu;
+    tt = ntt;
   }
   ugr = sumi1 / (c * sumi0);
   norm = sumi1;

@@ -27,7 +27,7 @@ REFINE = {"reference": 0, "tight": 1}
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("refine", C.c_int), ("rtol", C.c_double), ("sngl", C.c_int),
-                ("sphere", C.c_int), ("block_roots", C.c_int), ("split_cols", C.c_int)]
+                ("sphere", C.c_int), ("block_roots", C.c_int), ("split_cols", C.c_int), ("node_layers", C.c_int)]
 
 
 class Call(C.Structure):
@@ -128,7 +128,8 @@ class SwdkError(RuntimeError):
 class Engine:
     """One GPU context (device buffers, plans, stream) of libswdk."""
 
-    def __init__(self, device=0, refine="tight", rtol=1e-10, sngl=True, sphere=True, block_roots=0, split_cols=0):
+    def __init__(self, device=0, refine="tight", rtol=1e-10, sngl=True, sphere=True, block_roots=0, split_cols=0,
+                 node_layers=True):
         L = lib()
         cfg = Config()
         L.swdk_config_default(C.byref(cfg))
@@ -139,6 +140,7 @@ class Engine:
         cfg.sphere = 1 if sphere else 0
         cfg.block_roots = block_roots
         cfg.split_cols = split_cols
+        cfg.node_layers = 1 if node_layers else 0
         h = C.c_void_p()
         rc = L.swdk_create(C.byref(h), C.byref(cfg))
         if rc != 0:

@@ -62,18 +62,20 @@ extern "C" int eig_host_pass(int wave, int L, const float* thk, const float* vp,
       zd[i] = thk[i];
     }
   }
-  std::vector<double> scr((size_t)LMAX * 6);
+
   const double omega = 2.0 * PI_F / t, wvno = omega / c;
   LayerSink sink{da, db, dr};
   for (int i = 0; i < L; ++i) { da[i] = 0.0; db[i] = 0.0; dr[i] = 0.0; }
   if (wave == 1) {
     std::vector<LoveLayer> lay(L);
     for (int i = 0; i < L; ++i) make_love_layer(lay[i], zd[i], zb[i], zr[i], vtp[i], rtp[i]);
-    love_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink, trunc_q);
+    LoveScratch scr;
+    love_pass(lay.data(), L, omega, wvno, scr, *ugr, *norm, sink, trunc_q);
   } else {
     std::vector<RayLayer> lay(L);
     for (int i = 0; i < L; ++i) make_ray_layer(lay[i], zd[i], za[i], zb[i], zr[i], vtp[i], rtp[i]);
-    rayleigh_pass(lay.data(), L, omega, wvno, scr.data(), *ugr, *norm, sink, trunc_q);
+    RayScratch scr;
+    rayleigh_pass(lay.data(), L, omega, wvno, scr, *ugr, *norm, sink, trunc_q);
   }
   return 0;
 }

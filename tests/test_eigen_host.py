@@ -80,8 +80,6 @@ def test_eigen_passes_match_oracle_flat(wave):
     worst_k = worst_u = 0.0
     n = 0
     for mi, (th, a, b, r) in enumerate(_models()):
-        if wave == 1 and b[0] == 0.0:
-            continue  # Love waves do not see the water layer's model the same way (llw)
         for mode in (1, 2):
             cg, ierr, _ = O.surfdisp96(th, a, b, r, 0, wave, mode, 0, PERIODS, refine=1, rtol=1e-12, sngl=0)
             for t, c in zip(PERIODS, cg):
