@@ -569,10 +569,10 @@ __device__ __forceinline__ int ragged_find(const T* tab, int n, long long key, l
 // current chain is finished, so lanes stay busy while long chains run.
 // queue[0] is the next item; the launch covers the GPU once.
 #ifndef SWDK_ROOTS_MINB
-#define SWDK_ROOTS_MINB 5  // 96 registers with the chain state in shared memory: 5 blocks of 128 per SM
+#define SWDK_ROOTS_MINB 4  // 128 registers (64 B spill): roots 381 ms on the default workload; 5 blocks (96 registers) spill 660 B, 471 ms
 #endif
 #ifndef SWDK_EIGEN_MINB
-#define SWDK_EIGEN_MINB 5  // Rayleigh passes: 96 registers (4: 310 ms, 5: 293 ms, 6: 325 ms on the default workload)
+#define SWDK_EIGEN_MINB 3  // Rayleigh passes: 168 registers, no spill; eigen 171 ms on the default workload (4: 180 ms, 5: 227 ms)
 #endif
 #ifndef SWDK_EIGEN_MINB_LOVE
 #define SWDK_EIGEN_MINB_LOVE 5  // Love passes

@@ -109,6 +109,16 @@ def lib():
     return _LIB
 
 
+def torch_stream(device):
+    """Handle of torch's current stream on `device` for the entry points
+    whose NULL stream means the context's own stream: torch's default stream
+    (handle 0) is passed as cudaStreamLegacy (0x1), the legacy default
+    stream it stands for."""
+    import torch
+    h = torch.cuda.current_stream(device).cuda_stream
+    return h if h else 1
+
+
 def _p(a):
     if a is None:
         return None

@@ -4,7 +4,7 @@ import ctypes as C
 
 import numpy as np
 
-from .engine import SwdkError, lib as _lib
+from .engine import SwdkError, lib as _lib, torch_stream
 
 IN_DIM, HIDDEN, OUT_PHYS = 320, 256, 64
 
@@ -93,7 +93,7 @@ class MLP:
         """Fused inference on tile-image features straight to (c, half-width)
         per row (prop: (nrows, 2) float32), on torch's current stream."""
         import torch
-        st = C.c_void_p(torch.cuda.current_stream(prop.device).cuda_stream)
+        st = C.c_void_p(torch_stream(prop.device))
         self._check(_bind().swdk_mlp_propose(self._h, _p(x_tiles), nrows, kappa, _p(prop), st), "propose")
         return prop
 

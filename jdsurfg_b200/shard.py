@@ -28,6 +28,8 @@ NCCL all-gather into device tensors.
 """
 import numpy as np
 
+from .engine import torch_stream
+
 
 def column_block(ncol, world, rank):
     """[start, end) of rank's columns, the reference's allocate_tasks split."""
@@ -121,7 +123,7 @@ class ShardedSurfTime:
         blk = lambda a: None if a is None else a[:, c0:c1].contiguous()
         vs_b, vp_b, rho_b = blk(vs), blk(vp), blk(rho)
         if stream is None and vs.is_cuda:  # order the engine's work with torch's (the gather reads its outputs)
-            stream = torch.cuda.current_stream(vs.device).cuda_stream
+            stream = torch_stream(vs.device)
         if self.compute is not None:
             np_ = lambda a: None if a is None else a.cpu().numpy()
             r = self.compute(path, np_(vs_b), np_(vp_b), np_(rho_b))

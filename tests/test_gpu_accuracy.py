@@ -24,7 +24,10 @@ correct FP64 implementations disagree by that much.  A slot outside the
 tolerance passes only if the oracle's own U (km/s) and kernel (relative)
 move by comparable amounts under such changes (oracle_lib.kernel_spread):
 |dU| <= max(1e-6, 2 * U spread) and kernel error <= max(1e-5, 10 * kernel
-spread).  The number of exempted slots is printed.
+spread).  A group slot can also differ because its T(1 +- 0.005) roots,
+which the outputs do not show, round one REAL*4 ulp apart; such a slot
+passes if the oracle's U and kernel move as far under one ulp (2^-24) of
+its roots.  The numbers of exempted slots are printed.
 """
 import numpy as np
 import pytest
@@ -55,32 +58,43 @@ def _report(name, seed):
     scale = np.abs(ref["kernel"]).max(axis=1) + 1e-30
     kr = np.abs(g["kernel"] - ref["kernel"]).max(axis=1) / scale
     assert dc[ok].max() <= TOL_C, f"{name}: max |dc| {dc[ok].max():.3g}"
-    # kernels of slots whose roots differ by a REAL*4 ulp: the oracle at the GPU's root
+    # slots whose roots differ by a REAL*4 ulp: the oracle's group velocity
+    # and kernel at the GPU's root
     nsame_c = 0
-    for s, col in np.argwhere(ok & (kr > TOL_K) & (dc > 0)):
+    for s, col in np.argwhere(ok & ((kr > TOL_K) | (du > TOL_U)) & (dc > 0)):
         rel = g["vc"][s, col] / ref["vc"][s, col] - 1.0
         r2 = O.kernel_at(case, int(col), rel)
         kr[s, col] = np.abs(g["kernel"][s, :, col] - r2["kernel"][s, :, 0]).max() / scale[s, col]
+        du[s, col] = abs(g["vout"][s, col] - r2["vout"][s, 0])
         nsame_c += 1
     bad = ok & ((du > TOL_U) | (kr > TOL_K))
     bcols = np.nonzero(bad.any(axis=0))[0]
-    nexempt = 0
+    nexempt = nround = 0
     if len(bcols):
         ks, us = O.kernel_spread(case, bcols)
+        # the same under one REAL*4 ulp (2^-24) of the roots handed to the
+        # eigen routines: the group slots' T(1+-0.005) roots are not in the
+        # outputs, so a one-ulp difference there shows only through U
+        ks24, us24 = O.kernel_spread(case, bcols, rel=2.0 ** -24, steps=(-1, 1))
         for j, col in enumerate(bcols):
             for s in np.nonzero(bad[:, col])[0]:
-                print(f"{name} slot {s} column {cols[col]}: |dU| {du[s, col]:.3g} (oracle U spread {us[s, j]:.3g}), "
-                      f"kernel {kr[s, col]:.3g} (oracle kernel spread {ks[s, j]:.3g})")
-                assert du[s, col] <= max(TOL_U, 2.0 * us[s, j])
-                assert kr[s, col] <= max(TOL_K, 10.0 * ks[s, j])
-                nexempt += 1
+                print(f"{name} slot {s} column {cols[col]}: |dc| {dc[s, col]:.3g}, |dU| {du[s, col]:.3g} "
+                      f"(oracle U spread {us[s, j]:.3g}, {us24[s, j]:.3g} per ulp), kernel {kr[s, col]:.3g} "
+                      f"(oracle kernel spread {ks[s, j]:.3g}, {ks24[s, j]:.3g} per ulp)")
+                if du[s, col] <= max(TOL_U, 2.0 * us[s, j]) and kr[s, col] <= max(TOL_K, 10.0 * ks[s, j]):
+                    nexempt += 1
+                    continue
+                assert du[s, col] <= max(TOL_U, 2.0 * us24[s, j])
+                assert kr[s, col] <= max(TOL_K, 2.0 * ks24[s, j])
+                nround += 1
     rms = lambda x: float(np.sqrt(np.mean(x[ok] ** 2)))
     line = (f"{name}: {NCOL} columns x {ref['vc'].shape[0]} slots ({int(ok.sum())} with a root): "
             f"|dc| max {dc[ok].max():.3g} rms {rms(dc):.3g} km/s; |dU| max {du[ok].max():.3g} rms {rms(du):.3g} km/s; "
             f"kernel rel max {kr[ok].max():.3g} rms {rms(kr):.3g}; {nsame_c} kernels compared at the GPU's root "
-            f"(roots one REAL*4 ulp apart); {nexempt} slots exempted by the oracle's own conditioning")
+            f"(roots one REAL*4 ulp apart); {nexempt} slots exempted by the oracle's own conditioning, {nround} by "
+            f"its sensitivity to one REAL*4 ulp of the roots")
     print(line)
-    return nexempt, int(ok.sum())
+    return nexempt + nround, int(ok.sum())
 
 
 def test_accuracy_256x256x64_phase_and_group():
