@@ -568,8 +568,16 @@ __device__ __forceinline__ int ragged_find(const T* tab, int n, long long key, l
 // (chains in `order`, Rayleigh first, columns consecutive) whenever their
 // current chain is finished, so lanes stay busy while long chains run.
 // queue[0] is the next item; the launch covers the GPU once.
+// Dynamic shared memory of k_roots_queue and k_retry (128 threads): 55 KB,
+// above the 48 KB a launch gets without opting in; four blocks fit an SM's
+// 228 KB.
+constexpr size_t ROOTS_SMEM = 128 * (sizeof(ChainState) + sizeof(ChainParams) + sizeof(ChainIO));
+
 #ifndef SWDK_ROOTS_MINB
 #define SWDK_ROOTS_MINB 4  // 128 registers (64 B spill): roots 381 ms on the default workload; 5 blocks (96 registers) spill 660 B, 471 ms
+#endif
+#ifndef SWDK_RETRY_MINB
+#define SWDK_RETRY_MINB 2  // retries: 192 registers, no spill; one record per warp, fewer records than resident warps
 #endif
 #ifndef SWDK_EIGEN_MINB
 #define SWDK_EIGEN_MINB 3  // Rayleigh passes: 168 registers, no spill; eigen 171 ms on the default workload (4: 180 ms, 5: 227 ms)
@@ -594,18 +602,26 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
   double cbbuf[KMAX_CHAIN + 24];
   // the chain's state machine lives in shared memory, so the registers go to
   // the secular function: 96 registers, 5 blocks of 128 per SM
-  __shared__ ChainState sst[128];
+  // dynamic shared memory (ROOTS_SMEM): the chain states, and the chains'
+  // parameters and output addressing, which the state machine reads between
+  // evaluations instead of holding them in registers across them
+  extern __shared__ __align__(16) unsigned char roots_smem[];
+  ChainState* sst = reinterpret_cast<ChainState*>(roots_smem);
+  ChainParams* sprm = reinterpret_cast<ChainParams*>(sst + 128);
+  ChainIO* sio = reinterpret_cast<ChainIO*>(sprm + 128);
   __shared__ unsigned long long phase_ev[NPHASE_EV];
+  // evaluations, Rayleigh and Love layer evaluations, proposals used and
+  // refused: block totals, added at each chain's end (no registers held)
+  __shared__ unsigned long long blk_ev[5];
   if (threadIdx.x < NPHASE_EV) phase_ev[threadIdx.x] = 0ull;
+  if (threadIdx.x < 5) blk_ev[threadIdx.x] = 0ull;
   __syncthreads();
   ChainState& s = sst[threadIdx.x];
-  ChainParams P;
-  ChainIO io;
+  ChainParams& P = sprm[threadIdx.x];
+  ChainIO& io = sio[threadIdx.x];
   LayerView V;
-  ChainDesc cd;
   int col = 0, item_of = 0;
   bool have = false, exhausted = false;
-  unsigned long long ev_r = 0, ev_l = 0, lay_r = 0, lay_l = 0, pok = 0, pfail = 0;
   io.c = cbuf;
   io.cb = cbbuf;
   for (;;) {
@@ -618,6 +634,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         item_of = (int)item;
         // the item's model (a ragged batch) or the single model's arrays
         int mcol = ncol, lstride = rg.lstride;
+        ChainDesc cd;
         long long o_col = 0, o_lay = 0, o_root = 0, o_node = 0, o_dl = 0;
         if (rg.blocks) {
           const RBlock B = rg.blocks[ragged_find(rg.blocks, rg.nblocks, (long long)item, &RBlock::item0)];
@@ -674,12 +691,12 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
       if (need) break;
       // chain finished
       if (s.iterlim)
-        for (int i = 0; i < cd.nmode * cd.np; ++i)
+        for (int i = 0; i < P.nmode * P.kmax; ++i)
           if (io.st[(size_t)i * io.ostride] == ST_OK) io.st[(size_t)i * io.ostride] = ST_ITER_LIMIT;
       if (retry == RETRY_DEFERRED && s.ierr != 0) {
         // failed slots become single-period work items for k_retry
-        for (int m = 1; m <= cd.nmode; ++m)
-          for (int k = 1; k <= cd.np; ++k) {
+        for (int m = 1; m <= P.nmode; ++m)
+          for (int k = 1; k <= P.kmax; ++k) {
             const double v = out_at(io, m, k);
             if (v == 0.0 || !(v == v)) {
               const unsigned int r = atomicAdd(retry_count, 1u);
@@ -687,10 +704,10 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
             }
           }
       }
-      if (cd.iwave == 2) { ev_r += s.nevals; lay_r += (unsigned long long)s.nevals * V.L; }
-      else { ev_l += s.nevals; lay_l += (unsigned long long)s.nevals * V.L; }
-      pok += s.nprop_ok;
-      pfail += s.nprop_fail;
+      atomicAdd(&blk_ev[0], (unsigned long long)s.nevals);
+      atomicAdd(&blk_ev[P.iwave == 2 ? 1 : 2], (unsigned long long)s.nevals * V.L);
+      if (s.nprop_ok) atomicAdd(&blk_ev[3], (unsigned long long)s.nprop_ok);
+      if (s.nprop_fail) atomicAdd(&blk_ev[4], (unsigned long long)s.nprop_fail);
       have = false;
     }
     if (__ballot_sync(0xffffffffu, need) == 0u) break;
@@ -704,21 +721,7 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
   __syncthreads();
   if (threadIdx.x < NPHASE_EV && nevals && phase_ev[threadIdx.x])
     atomicAdd(nevals + EV_BASE + threadIdx.x, phase_ev[threadIdx.x]);
-  unsigned long long e = ev_r + ev_l;
-  for (int o = 16; o > 0; o >>= 1) {
-    e += __shfl_down_sync(0xffffffffu, e, o);
-    lay_r += __shfl_down_sync(0xffffffffu, lay_r, o);
-    lay_l += __shfl_down_sync(0xffffffffu, lay_l, o);
-    pok += __shfl_down_sync(0xffffffffu, pok, o);
-    pfail += __shfl_down_sync(0xffffffffu, pfail, o);
-  }
-  if ((threadIdx.x & 31) == 0 && nevals) {
-    atomicAdd(nevals, e);
-    atomicAdd(nevals + 1, lay_r);
-    atomicAdd(nevals + 2, lay_l);
-    atomicAdd(nevals + 3, pok);
-    atomicAdd(nevals + 4, pfail);
-  }
+  if (threadIdx.x < 5 && nevals && blk_ev[threadIdx.x]) atomicAdd(nevals + threadIdx.x, blk_ev[threadIdx.x]);
 }
 
 // One round of the getsol scan (surfdisp96.f:452-486) by a whole warp.  The
@@ -770,7 +773,7 @@ __device__ int retry_scan(ChainState& s, const ChainParams& P, const LayerView& 
 // lanes hold the same chain state and take the scan 32 points at a time
 // (retry_scan), the other requests (start point, refinement) are evaluated
 // by all lanes alike.
-__global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const int* __restrict__ order,
+__global__ void __launch_bounds__(128, SWDK_RETRY_MINB) k_retry(int ncol, const int* __restrict__ order,
                                                                const ChainDesc* __restrict__ chains,
                                                                const double* __restrict__ periods,
                                                                const float4* __restrict__ layR,
@@ -784,20 +787,27 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
                                                                unsigned long long* __restrict__ nevals, RaggedMap rg,
                                                                const float4* __restrict__ nodes,
                                                                const DepthLayer* __restrict__ dl) {
-  __shared__ ChainState sst[128];  // one copy of the warp's chain state per lane
+  // dynamic shared memory (ROOTS_SMEM): one copy of the warp's chain state,
+  // parameters and output addressing per lane
+  extern __shared__ __align__(16) unsigned char roots_smem[];
+  ChainState* sst = reinterpret_cast<ChainState*>(roots_smem);
+  ChainParams* sprm = reinterpret_cast<ChainParams*>(sst + 128);
+  ChainIO* sio = reinterpret_cast<ChainIO*>(sprm + 128);
+  __shared__ unsigned long long blk_ev[3];  // evaluations, Rayleigh and Love layer evaluations
+  if (threadIdx.x < 3) blk_ev[threadIdx.x] = 0ull;
+  __syncthreads();
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
   const unsigned int n = min(*retry_count, retry_cap);
   const int lane = threadIdx.x & 31;
-  unsigned long long ev_r = 0, lay_r = 0, lay_l = 0;
   for (;;) {
     unsigned int r = 0;
     if (lane == 0) r = atomicAdd(queue, 1u);
     r = __shfl_sync(0xffffffffu, r, 0);
     if (r >= n) break;
     ChainState& s = sst[threadIdx.x];
-    ChainParams P;
-    ChainIO io;
+    ChainParams& P = sprm[threadIdx.x];
+    ChainIO& io = sio[threadIdx.x];
     LayerView V;
     const int2 rec = retry_list[r];
     const int m = rec.y >> 16, k = rec.y & 0xffff;
@@ -862,23 +872,24 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_retry(int ncol, const 
     __syncwarp();
     if (lane == 0) {
       if (s.iterlim && st_at(io, m, k) != ST_NO_ROOT) st_at(io, m, k) = ST_ITER_LIMIT;
-      ev_r += nev;
-      if (cd.iwave == 2) lay_r += nev * V.L;
-      else lay_l += nev * V.L;
+      atomicAdd(&blk_ev[0], nev);
+      atomicAdd(&blk_ev[P.iwave == 2 ? 1 : 2], nev * V.L);
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    ev_r += __shfl_down_sync(0xffffffffu, ev_r, o);
-    lay_r += __shfl_down_sync(0xffffffffu, lay_r, o);
-    lay_l += __shfl_down_sync(0xffffffffu, lay_l, o);
-  }
-  if (lane == 0 && nevals && ev_r) {
-    atomicAdd(nevals, ev_r);
-    atomicAdd(nevals + 1, lay_r);
-    atomicAdd(nevals + 2, lay_l);
-    atomicAdd(nevals + EV_BASE + EV_RETRY, ev_r);
-  }
+  __syncthreads();
+  if (threadIdx.x < 3 && nevals && blk_ev[threadIdx.x]) atomicAdd(nevals + threadIdx.x, blk_ev[threadIdx.x]);
+  if (threadIdx.x == 0 && nevals && blk_ev[0]) atomicAdd(nevals + EV_BASE + EV_RETRY, blk_ev[0]);
 }
+
+// Opts k_roots_queue and k_retry in to ROOTS_SMEM on the current device and
+// returns k_roots_queue's resident blocks per SM.
+cudaError_t roots_occupancy(int* per) {
+  cudaError_t e = cudaFuncSetAttribute(k_roots_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROOTS_SMEM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_retry, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROOTS_SMEM);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_roots_queue, 128, ROOTS_SMEM);
+  return e;
+}
+
 
 // recip() on an array (its accuracy test)
 __global__ void k_recip(int n, const double* __restrict__ x, double* __restrict__ r) {
@@ -975,13 +986,14 @@ __device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax
 
   using Scratch = typename std::conditional<love, LoveScratch, RayScratch>::type;
   Scratch scr;  // up-pass checkpoints and the segment being consumed (per slot thread)
-  double kacc[NZMAX], kp[NZMAX];
+  double kp[NZMAX];  // one pass's node sums; the scaled sums accumulate in the output
   NodeSink sink;
   sink.kp = (path == 0) ? kp : nullptr;
   sink.crs = crs;
   sink.L = L;
   sink.nw = ci.nw;
-  const NodeSink nosink = {nullptr, crs, L, ci.nw};
+  sink.nz = nz;
+  const NodeSink nosink = {nullptr, crs, L, ci.nw, nz};
   for (int s = threadIdx.x; s < gn; s += blockDim.x) {
     const SlotDesc sd = slots[g0 + s];
     constexpr bool group = (WT == 1 || WT == 3);
@@ -1027,7 +1039,7 @@ __device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax
       }
     } else {
     // ---- get_1d_kernel: kernel1D (SurfaceWave.cpp:266-412) ----
-    for (int i = 0; i < nz; ++i) kacc[i] = 0.0;
+    double* kout = kernel + (size_t)sd.oslot * nz * ldo + col;  // node i at kout[i * ldo]
     if (!group) {
       const double omega = 2.0 * PI_F / sd.t, wvno = omega / c0;
       double ugr, norm;
@@ -1040,7 +1052,7 @@ __device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax
         tm = sqrt(1. + x * x);
       }
       const double s1 = 1.0 / (norm * tm * tm * tm);
-      for (int i = 0; i < nz; ++i) kacc[i] = kp[i] * s1;
+      for (int i = 0; i < nz; ++i) kout[(size_t)i * ldo] = kp[i] * s1;
       const double cs = c0 / tm;
       vc[oo] = cs;
       vout[oo] = cs;
@@ -1080,19 +1092,22 @@ __device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax
         } else {
           coef = tm * (f1 - f2 / dtt);
         }
+        // the sum over the passes, from 0, in the output
         if (coef != 0.0) {
           const double s1 = coef / norm;
-          for (int i = 0; i < nz; ++i) kacc[i] += kp[i] * s1;
+          for (int i = 0; i < nz; ++i) {
+            const double prev = (pass == 0) ? 0.0 : kout[(size_t)i * ldo];
+            kout[(size_t)i * ldo] = prev + kp[i] * s1;
+          }
+        } else if (pass == 0) {
+          for (int i = 0; i < nz; ++i) kout[(size_t)i * ldo] = 0.0;
         }
       }
       vc[oo] = cp / tm;
       vout[oo] = cg * tm;
     }
     // water / merged fluid nodes carry no kernel (SurfaceWave.cpp:495)
-    for (int i = 0; i < nz; ++i) {
-      const double v = (i < ci.nw) ? 0.0 : kacc[i];
-      kernel[((size_t)sd.oslot * nz + i) * ldo + col] = v;
-    }
+    for (int i = 0; i < ci.nw; ++i) kout[(size_t)i * ldo] = 0.0;
     }  // get_1d_kernel
   }
 }
@@ -1587,7 +1602,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
     int dev = 0, nsm = 0, per = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0));
+    CK(roots_occupancy(&per));
     ctx->roots_blocks = std::max(1, nsm * std::max(1, per));
   }
   const int nitems = (int)P.chains.size() * ncol;
@@ -1599,7 +1614,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaMemsetAsync(ctx->retry_ctr.p, 0, 2 * sizeof(unsigned int), st));
   unsigned int* rctr = ctx->retry_ctr.as<unsigned int>();
   ctx->launches += 2;
-  k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, 0, st>>>(
+  k_roots_queue<<<std::min(rblocks, (nitems + 127) / 128), 128, ROOTS_SMEM, st>>>(
       ncol, nitems, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(), ctx->layR.as<float4>(),
       ctx->layL.as<float4>(), ctx->info.as<ColInfo>(), ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, RETRY_DEFERRED,
       ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->queue.as<unsigned int>(),
@@ -1607,7 +1622,7 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       ctx->nevals.as<unsigned long long>(), RaggedMap{nullptr, nullptr, 0, Lmax},
       use_nodes ? ctx->nodes.as<float4>() : nullptr, ctx->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
-  k_retry<<<rblocks, 128, 0, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
+  k_retry<<<rblocks, 128, ROOTS_SMEM, st>>>(ncol, P.d_order.as<int>(), P.d_chains.as<ChainDesc>(), P.d_periods.as<double>(),
                                    ctx->layR.as<float4>(), ctx->layL.as<float4>(), ctx->info.as<ColInfo>(),
                                    ctx->cfg.refine, ctx->cfg.rtol, ctx->cfg.sngl, ctx->croot.as<double>(),
                                    ctx->cstat.as<int32_t>(), ctx->retry_list.as<int2>(), rctr, rcap, rctr + 1,
@@ -2377,7 +2392,7 @@ int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
   unsigned int* rctr = R->retry_ctr.as<unsigned int>();
   const long long grid = std::min<long long>(R->roots_blocks, (R->nitems + 127) / 128);
   R->launches += 2;
-  k_roots_queue<<<(unsigned)std::max(1LL, grid), 128, 0, st>>>(
+  k_roots_queue<<<(unsigned)std::max(1LL, grid), 128, ROOTS_SMEM, st>>>(
       0, (int)R->nitems, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(), R->layR.as<float4>(),
       R->layL.as<float4>(), R->info.as<ColInfo>(), cfg.refine, cfg.rtol, cfg.sngl, RETRY_DEFERRED,
       R->croot.as<double>(), R->cstat.as<int32_t>(), R->queue.as<unsigned int>(),
@@ -2385,7 +2400,7 @@ int ragged_enqueue(swdk_ragged* R, cudaStream_t st, bool timing) {
       R->nevals.as<unsigned long long>(), rg, use_nodes ? R->nodes.as<float4>() : nullptr,
       R->dltab.as<DepthLayer>());
   CK(cudaGetLastError());
-  k_retry<<<R->roots_blocks, 128, 0, st>>>(0, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(),
+  k_retry<<<R->roots_blocks, 128, ROOTS_SMEM, st>>>(0, nullptr, R->d_chains.as<ChainDesc>(), R->d_periods.as<double>(),
                                            R->layR.as<float4>(), R->layL.as<float4>(), R->info.as<ColInfo>(),
                                            cfg.refine, cfg.rtol, cfg.sngl, R->croot.as<double>(),
                                            R->cstat.as<int32_t>(), R->retry_list.as<int2>(), rctr, rcap, rctr + 1,
@@ -2603,7 +2618,8 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
   int dev = 0, nsm = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0);
+  if (e == cudaSuccess) e = roots_occupancy(&per);
+  if (e != cudaSuccess) return bail(SWDK_E_CUDA, std::string("ragged batch set-up: ") + cudaGetErrorString(e));
   R->roots_blocks = ctx->cfg.block_roots > 0 ? ctx->cfg.block_roots : std::max(1, nsm * std::max(1, per));
   *out = R;
   return SWDK_OK;
@@ -2673,7 +2689,7 @@ int swdk_autotune(swdk_ctx* ctx, int nx, int ny, int nz, const float* d_vs, cons
   int dev = 0, nsm = 0, per = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_roots_queue, 128, 0));
+  CK(roots_occupancy(&per));
   per = std::max(1, per);
   // candidates: resident blocks of the persistent root kernel, 1..per per SM
   // plus one oversubscribed grid (queue items then also spread over waves)

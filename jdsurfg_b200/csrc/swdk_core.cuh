@@ -153,25 +153,30 @@ struct LayerView {
   // times the wave's density factor (sphere(), surfdisp96.f:499-571)
   SWDK_HD float4 layer(int m) const {
     if (!nodes) return lay[idx(m)];
-    const DepthLayer& q = dl[m];
-    float ai, bi, ri;
     if (m == L - 1) {
-      const float4 n = nodes[(L + 3) / 4 - 1];
-      ai = n.x; bi = n.y; ri = n.z;
-    } else {
-      const int i = m >> 2;
-      const float4 n0 = nodes[i], n1 = nodes[i + 1];
-      const float w = (float)(2 * (m & 3) + 1);
-#ifdef __CUDA_ARCH__
-      ai = (float)__dadd_rn((double)n0.x, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.x, n0.x)), 0.125));
-      bi = (float)__dadd_rn((double)n0.y, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.y, n0.y)), 0.125));
-      ri = (float)__dadd_rn((double)n0.z, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.z, n0.z)), 0.125));
-#else
-      ai = (float)((double)n0.x + (double)(w * (n1.x - n0.x)) * 0.125);
-      bi = (float)((double)n0.y + (double)(w * (n1.y - n0.y)) * 0.125);
-      ri = (float)((double)n0.z + (double)(w * (n1.z - n0.z)) * 0.125);
-#endif
+      const float4 n = nodes[nnode() - 1];
+      return flatten(n.x, n.y, n.z, m);
     }
+    return from_nodes(nodes[m >> 2], nodes[(m >> 2) + 1], m);
+  }
+  SWDK_HD int nnode() const { return (L + 3) >> 2; }
+  // sublayer m < L-1 of node interval m/4 (nodes n0 above, n1 below)
+  SWDK_HD float4 from_nodes(const float4& n0, const float4& n1, int m) const {
+    const float w = (float)(2 * (m & 3) + 1);
+    float ai, bi, ri;
+#ifdef __CUDA_ARCH__
+    ai = (float)__dadd_rn((double)n0.x, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.x, n0.x)), 0.125));
+    bi = (float)__dadd_rn((double)n0.y, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.y, n0.y)), 0.125));
+    ri = (float)__dadd_rn((double)n0.z, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.z, n0.z)), 0.125));
+#else
+    ai = (float)((double)n0.x + (double)(w * (n1.x - n0.x)) * 0.125);
+    bi = (float)((double)n0.y + (double)(w * (n1.y - n0.y)) * 0.125);
+    ri = (float)((double)n0.z + (double)(w * (n1.z - n0.z)) * 0.125);
+#endif
+    return flatten(ai, bi, ri, m);
+  }
+  SWDK_HD float4 flatten(float ai, float bi, float ri, int m) const {
+    const DepthLayer& q = dl[m];
     float4 out;
     out.x = q.d;
 #ifdef __CUDA_ARCH__
@@ -184,6 +189,44 @@ struct LayerView {
     out.w = ri * (wave == 2 ? q.fR : q.fL);
 #endif
     return out;
+  }
+  // A walk over consecutive layers (DIR -1: upward, m decreasing; +1:
+  // downward) that loads ahead of use.  From the nodes it holds the current
+  // interval's two nodes and the next interval's far node, which is loaded
+  // one interval (four sublayers) before it is needed; from a table it holds
+  // the next layer, loaded one layer early.  Layers L-1 (the half-space)
+  // and below are not walked.
+  struct Walk {
+    float4 n0, n1, nn;
+    int i;
+  };
+  template <int DIR, bool NODES>
+  SWDK_HD void walk_start(Walk& w, int m) const {
+    if (!NODES) { w.nn = lay[idx(m)]; return; }
+    w.i = m >> 2;
+    w.n0 = nodes[w.i];
+    w.n1 = nodes[w.i + 1];
+    const int j = DIR < 0 ? w.i - 1 : w.i + 2;
+    if (j >= 0 && j < nnode()) w.nn = nodes[j];
+  }
+  // layer m of the walk: the call before was walk_start(m) or walk_layer(m - DIR)
+  template <int DIR, bool NODES>
+  SWDK_HD float4 walk_layer(Walk& w, int m) const {
+    if (!NODES) {
+      const float4 r = w.nn;
+      const int j = m + DIR;
+      if (j >= 0 && j < L) w.nn = lay[idx(j)];
+      return r;
+    }
+    const int i = m >> 2;
+    if (i != w.i) {
+      if (DIR < 0) { w.n1 = w.n0; w.n0 = w.nn; }
+      else { w.n0 = w.n1; w.n1 = w.nn; }
+      w.i = i;
+      const int j = DIR < 0 ? i - 1 : i + 2;
+      if (j >= 0 && j < nnode()) w.nn = nodes[j];
+    }
+    return from_nodes(w.n0, w.n1, m);
   }
   SWDK_HD float4 get(int m) const {  // m: reference (top-down, 0-based) index
     return lay[idx(m)];
@@ -481,6 +524,7 @@ SWDK_HD void apply_dunkin(const LayerCoef& k, double wvno2, double& e0, double& 
 // skips the search where no cut is possible (long periods).
 constexpr double SEC_TRUNC_Q = 30.0;
 
+template <bool NODES>
 SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
   if (!V.trunc) return V.L - 1;
   const double c = omega / wvno, bm = V.bmax;
@@ -488,8 +532,10 @@ SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
   if (!(u > 0.0) || wvno * (double)V.htot * sqrt(u) <= SEC_TRUNC_Q) return V.L - 1;
   const double wvno2 = wvno * wvno;
   double cum = 0.0;
+  LayerView::Walk wk;
+  V.walk_start<1, NODES>(wk, V.llw - 1);
   for (int m = V.llw - 1; m < V.L - 2; ++m) {
-    const float4 ly = V.layer(m);
+    const float4 ly = V.walk_layer<1, NODES>(wk, m);
     if (ly.z > 0.0f) {
       const double xkb = omega * recip((double)ly.z);
       const double x2 = wvno2 - xkb * xkb;
@@ -500,13 +546,13 @@ SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
   return V.L - 1;
 }
 
-template <int NORM>
+template <int NORM, bool NODES>
 SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   double omega = omga;
   if (omega < 1.0e-4) omega = 1.0e-4;
   const double wvno2 = wvno * wvno;
   const double iom = 1.0 / omega;
-  const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
+  const int hs = secular_depth<NODES>(V, wvno, omega);  // the layer taken as the half-space
   const float4 h = V.layer(hs);
   double xka = omega * recip((double)h.y), xkb = omega * recip((double)h.z);
   const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
@@ -523,11 +569,10 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   double e4 = wvno2 - ra * rb;
   const int mlo = V.llw - 1;
   int since = 0;
-  // the next layer's float4 is loaded one layer ahead of its use
-  float4 ly = V.layer(hs - 1 >= mlo ? hs - 1 : mlo);
+  LayerView::Walk wk;
+  if (hs - 1 >= mlo) V.walk_start<-1, NODES>(wk, hs - 1);
   for (int m = hs - 1; m >= mlo; --m) {
-    const float4 cur_ly = ly;
-    if (m > mlo) ly = V.layer(m - 1);
+    const float4 cur_ly = V.walk_layer<-1, NODES>(wk, m);
     const LayerCoef cur = layer_coef(cur_ly, wvno, wvno2, omega, iom);
     apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
     if (++since >= NORM || m == mlo) {
@@ -568,9 +613,9 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
 }
 
 // dltar1 with 1/b and 1/(rho b^2) from recip()
-template <int NORM>
+template <int NORM, bool NODES>
 SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
-  const int hs = secular_depth(V, wvno, omega);  // the layer taken as the half-space
+  const int hs = secular_depth<NODES>(V, wvno, omega);  // the layer taken as the half-space
   float4 h = V.layer(hs);
   double beta1 = h.z, rho1 = h.w;
   double xkb = omega * recip(beta1);
@@ -579,11 +624,10 @@ SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
   double e2 = 1.0 / (beta1 * beta1);
   int since = 0;
   const int mlo = V.llw - 1;
-  // the next layer's float4 is loaded one layer ahead of its use
-  float4 nx = V.layer(hs - 1 >= mlo ? hs - 1 : mlo);
+  LayerView::Walk wk;
+  if (hs - 1 >= mlo) V.walk_start<-1, NODES>(wk, hs - 1);
   for (int m = hs - 1; m >= mlo; --m) {
-    const float4 ly = nx;
-    if (m > mlo) nx = V.layer(m - 1);
+    const float4 ly = V.walk_layer<-1, NODES>(wk, m);
     beta1 = ly.z;
     rho1 = ly.w;
     const double dpth = ly.x;
@@ -628,8 +672,12 @@ SWDK_HD double secular(const LayerView& V, int iwave, double wvno, double omega)
 // production secular function: reciprocal-table variants; the reference
 // refinement keeps per-layer normalisation like surfdisp96
 SWDK_HD double secular_fast(const LayerView& V, int iwave, int refine, double wvno, double omega) {
-  if (refine == 0) return (iwave == 1) ? dltar1_fast<1>(V, wvno, omega) : dltar4_fast<1>(V, wvno, omega);
-  return (iwave == 1) ? dltar1_fast<4>(V, wvno, omega) : dltar4_fast<4>(V, wvno, omega);
+  if (V.nodes) {
+    if (refine == 0) return (iwave == 1) ? dltar1_fast<1, true>(V, wvno, omega) : dltar4_fast<1, true>(V, wvno, omega);
+    return (iwave == 1) ? dltar1_fast<4, true>(V, wvno, omega) : dltar4_fast<4, true>(V, wvno, omega);
+  }
+  if (refine == 0) return (iwave == 1) ? dltar1_fast<1, false>(V, wvno, omega) : dltar4_fast<1, false>(V, wvno, omega);
+  return (iwave == 1) ? dltar1_fast<4, false>(V, wvno, omega) : dltar4_fast<4, false>(V, wvno, omega);
 }
 
 // ---------------------------------------------------------------------------

@@ -83,35 +83,54 @@ SWDK_HD void make_love_layer(LoveLayer& y, double d, double zb, double zr, doubl
 //   w * (x_b fa(l) + x_a fa(l) dalpha/dbeta(n) + x_r fr(l) drho/dalpha(n) dalpha/dbeta(n))
 // with fa = vtp, fr = rtp; the pass's normaliser divides the sum afterwards.
 struct NodeSink {
-  double* kp;         // node accumulator [nz] (null: no kernels wanted)
+  double* kp;         // node sums [nz] (null: no kernels wanted)
   const float2* crs;  // (dalpha/dbeta, drho/dalpha) per node
-  int L, nw;
+  int L, nw, nz;
+  // The sweep visits the sublayers top-down, so the two nodes of the current
+  // node interval are the only ones still summing: they are held here and a
+  // node is stored once, when the sweep leaves it (the sums keep the order
+  // of a per-layer kp[n] += ...).
+  mutable int cur;          // node of s0 (-1: none yet)
+  mutable double s0, s1;    // running sums of nodes cur and cur + 1
+  SWDK_HD void start() const { cur = -1; s0 = 0.0; s1 = 0.0; }
+  SWDK_HD void to_node(int n) const {  // n >= cur: leave the nodes above n
+    if (n == cur) return;
+    if (cur >= 0) {
+      kp[cur] = s0;
+      if (n > cur + 1) kp[cur + 1] = s1;
+    }
+    s0 = (n == cur + 1) ? s1 : 0.0;
+    s1 = 0.0;
+    cur = n;
+  }
+  SWDK_HD void finish() const {
+    if (!kp || cur < 0) return;
+    kp[cur] = s0;
+    if (cur + 1 < nz) kp[cur + 1] = s1;
+  }
   SWDK_HD void add(int l, double fa, double fr, double xa, double xb, double xr) const {
     if (!kp) return;
-    int n0, n1 = -1;
-    double w0, w1 = 0.0;
     if (nw > 0 && l == 0) return;
     const int lp = (nw > 0) ? l - 1 : l;
-    if (l == L - 1) {
-      n0 = (lp >> 2) + nw;
-      w0 = 4.875;
-    } else {
-      const double t = (double)(2 * (lp & 3) + 1) / 8.0;
-      n0 = (lp >> 2) + nw;
-      w0 = 1.0 - t;
-      n1 = n0 + 1;
-      w1 = t;
-    }
+    const int n0 = (lp >> 2) + nw;
     const double xbf = xb * fa, xaf = xa * fa, xrf = xr * fr;
-    {
+    to_node(n0);
+    if (l == L - 1) {
       const float2 c = crs[n0];
       const double dadb = c.x, drda = c.y;
-      kp[n0] += w0 * (xbf + xaf * dadb + xrf * drda * dadb);
-    }
-    if (n1 >= 0) {
-      const float2 c = crs[n1];
-      const double dadb = c.x, drda = c.y;
-      kp[n1] += w1 * (xbf + xaf * dadb + xrf * drda * dadb);
+      s0 += 4.875 * (xbf + xaf * dadb + xrf * drda * dadb);
+    } else {
+      const double t = (double)(2 * (lp & 3) + 1) / 8.0;
+      {
+        const float2 c = crs[n0];
+        const double dadb = c.x, drda = c.y;
+        s0 += (1.0 - t) * (xbf + xaf * dadb + xrf * drda * dadb);
+      }
+      {
+        const float2 c = crs[n0 + 1];
+        const double dadb = c.x, drda = c.y;
+        s1 += t * (xbf + xaf * dadb + xrf * drda * dadb);
+      }
     }
   }
 };
@@ -540,7 +559,10 @@ constexpr double EIG_TRUNC_Q = 40.0;
 // recomputation repeats the up pass's arithmetic exactly, so the values are
 // the ones a full per-layer store would hold, with about 2 KB of scratch per
 // slot instead of 6 doubles per layer.
-constexpr int RAY_SEG = 16;
+#ifndef SWDK_RAY_SEG
+#define SWDK_RAY_SEG 16
+#endif
+constexpr int RAY_SEG = SWDK_RAY_SEG;
 constexpr int RAY_NCK = (LMAX + RAY_SEG - 1) / RAY_SEG;
 struct RayScratch {
   double ck[RAY_NCK][8];  // layer j*RAY_SEG: cd[5], exponent sum, exr, exi
@@ -599,6 +621,7 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
     if (m % RAY_SEG == 0) ray_keep(scr.ck[m / RAY_SEG], cd, exr, exi);
   }
   // ---- down + svfunc + energy, top-down ----
+  sink.start();
   const double* top = scr.ck[0];  // layer 0
   const double if1213 = -1.0 / top[1];
   const double exe0 = top[5];
@@ -654,6 +677,7 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
     sink.add(m, y.vtp, y.rtp, da, db, dr);
     u0 = u1;
   }
+  sink.finish();
   ugr = (wvno * acc.sumi1 + acc.sumi2) / (omega * acc.sumi0);
   norm = ugr * acc.sumi0;
 }
@@ -773,6 +797,7 @@ SWDK_HDI void love_pass(const LoveLayer* lay, int Lfull, double omega, double wv
   double sumi0 = 0.0, sumi1 = 0.0;
   double ext = 0.0;
   double uu = top0 * iumax, tt = 0.0;
+  sink.start();
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
   for (int k = 0; k < L; ++k) {
     const int j0 = k - k % RAY_SEG;
@@ -838,6 +863,7 @@ SWDK_HDI void love_pass(const LoveLayer* lay, int Lfull, double omega, double wv
     uu = nuu;
     tt = ntt;
   }
+  sink.finish();
   ugr = sumi1 / (c * sumi0);
   norm = sumi1;
 }

@@ -1889,6 +1889,16 @@ struct Opts {
 // change of their input.  0 (the default) leaves both exactly as the
 // reference.
 double g_cpert = 0.0;
+// A second probe: c1 and c2 of the group kernels (the roots at T(1 +- 0.005))
+// moved by g_ulp[0] and g_ulp[1] REAL*4 ulps, each on its own; 0 leaves them.
+int g_ulp[2] = {0, 0};
+
+double ulp_step(double c, int n) {
+  float f = (float)c;
+  for (; n > 0; --n) f = std::nextafter(f, HUGE_VALF);
+  for (; n < 0; ++n) f = std::nextafter(f, -HUGE_VALF);
+  return (double)f;
+}
 
 // kernel1D (SurfaceWave.cpp:266-412); kvs/kvp/krho are (nz, kmax) column-major
 void kernel1d(const float* vs, const float* vp, const float* rho, const float* dep, int nz, const Tables& T,
@@ -1966,6 +1976,8 @@ void kernel1d(const float* vs, const float* vp, const float* rho, const float* d
             c1[i] = c1[i] * (1.0 + g_cpert);
             c2[i] = c2[i] * (1.0 + g_cpert);
           }
+          if (g_ulp[0]) c1[i] = ulp_step(c1[i], g_ulp[0]);
+          if (g_ulp[1]) c2[i] = ulp_step(c2[i], g_ulp[1]);
           if (w == 1) {
             sregnpu_(TH, VP, VS, RH, rmax, &tt[i], &cp[i], vc + k, ur.data(), uz.data(), tr.data(), tz.data(),
                      &t1[i], &c1[i], &t2[i], &c2[i], dcdar.data(), dcdbr.data(), dcdhr.data(), dcdrr.data(),
@@ -2051,6 +2063,8 @@ extern "C" {
 
 // the conditioning probe of kernel1d (0 = off)
 void swdo_set_eigen_cpert(double rel) { g_cpert = rel; }
+// the group-root probe of kernel1d (0, 0 = off)
+void swdo_set_group_ulp(int u1, int u2) { g_ulp[0] = u1; g_ulp[1] = u2; }
 
 // get_1d_kernel (SurfaceWave.cpp:458-502) over ncol columns with OpenMP.
 //   vs: (ncol, nz) column-major float; vp_in/rho_in optional explicit node

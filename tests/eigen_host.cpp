@@ -21,6 +21,29 @@ struct LayerSink {
     db[l] = xb;
     dr[l] = xr;
   }
+  void start() const {}
+  void finish() const {}
+};
+
+// the node sums as a per-layer accumulation: kp[n] += w * (...) in layer
+// order, the arithmetic NodeSink keeps in registers
+struct TentSink {
+  double* kp;
+  const float2* crs;
+  int L, nw;
+  void start() const {}
+  void finish() const {}
+  void add(int l, double fa, double fr, double xa, double xb, double xr) const {
+    if (nw > 0 && l == 0) return;
+    const int lp = (nw > 0) ? l - 1 : l;
+    const int n0 = (lp >> 2) + nw;
+    const double xbf = xb * fa, xaf = xa * fa, xrf = xr * fr;
+    const double t = (double)(2 * (lp & 3) + 1) / 8.0;
+    const double w0 = (l == L - 1) ? 4.875 : 1.0 - t;
+    kp[n0] += w0 * (xbf + xaf * (double)crs[n0].x + xrf * (double)crs[n0].y * (double)crs[n0].x);
+    if (l != L - 1)
+      kp[n0 + 1] += t * (xbf + xaf * (double)crs[n0 + 1].x + xrf * (double)crs[n0 + 1].y * (double)crs[n0 + 1].x);
+  }
 };
 }  // namespace
 
@@ -76,6 +99,36 @@ extern "C" int eig_host_pass(int wave, int L, const float* thk, const float* vp,
     for (int i = 0; i < L; ++i) make_ray_layer(lay[i], zd[i], za[i], zb[i], zr[i], vtp[i], rtp[i]);
     RayScratch scr;
     rayleigh_pass(lay.data(), L, omega, wvno, scr, *ugr, *norm, sink, trunc_q);
+  }
+  return 0;
+}
+
+// The node sums of one pass through NodeSink (kp) and through TentSink
+// (kref) on the same flat layer model; nw fluid nodes merged into layer 0,
+// crs holds nz (dalpha/dbeta, drho/dalpha) pairs.
+extern "C" int eig_host_nodesums(int wave, int L, const float* thk, const float* vp, const float* vs,
+                                 const float* rho, int nw, int nz, const float* crs, double t, double c,
+                                 double trunc_q, double* kp, double* kref) {
+  if (L < 2 || L > LMAX || nz < 2) return -1;
+  const double omega = 2.0 * PI_F / t, wvno = omega / c;
+  std::vector<float2> cr(nz);
+  for (int i = 0; i < nz; ++i) { cr[i].x = crs[2 * i]; cr[i].y = crs[2 * i + 1]; }
+  for (int i = 0; i < nz; ++i) { kp[i] = 0.0; kref[i] = 0.0; }
+  NodeSink ns{kp, cr.data(), L, nw, nz};
+  TentSink ts{kref, cr.data(), L, nw};
+  double ugr, norm;
+  if (wave == 1) {
+    std::vector<LoveLayer> lay(L);
+    for (int i = 0; i < L; ++i) make_love_layer(lay[i], thk[i], vs[i], rho[i], 1.0, 1.0);
+    LoveScratch scr;
+    love_pass(lay.data(), L, omega, wvno, scr, ugr, norm, ns, trunc_q);
+    love_pass(lay.data(), L, omega, wvno, scr, ugr, norm, ts, trunc_q);
+  } else {
+    std::vector<RayLayer> lay(L);
+    for (int i = 0; i < L; ++i) make_ray_layer(lay[i], thk[i], vp[i], vs[i], rho[i], 1.0, 1.0);
+    RayScratch scr;
+    rayleigh_pass(lay.data(), L, omega, wvno, scr, ugr, norm, ns, trunc_q);
+    rayleigh_pass(lay.data(), L, omega, wvno, scr, ugr, norm, ts, trunc_q);
   }
   return 0;
 }

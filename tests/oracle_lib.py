@@ -217,6 +217,27 @@ def kernel_at(case, col, rel):
         lib().swdo_set_eigen_cpert(C.c_double(0.0))
 
 
+def group_root_spread(case, cols):
+    """Sensitivity of the oracle's group kernels to the REAL*4 rounding of
+    their hidden roots c1, c2 at T(1 +- 0.005): the largest kernel change
+    (relative to the slot's largest |kernel|) per (slot, column) when c1 or
+    c2 alone moves by one REAL*4 ulp either way.  sregnpu/slegnpu difference
+    the phase kernels at c1 and c2 over a 1 % period step, so a one-ulp
+    change of one of them moves the group kernel about 100 times as much as
+    the same change of c; phase slots do not move."""
+    base = get_1d_kernel(case, cols=cols)
+    scale = np.abs(base["kernel"]).max(axis=1) + 1e-30
+    ks = np.zeros_like(scale)
+    try:
+        for u in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+            lib().swdo_set_group_ulp(u[0], u[1])
+            r = get_1d_kernel(case, cols=cols)
+            ks = np.maximum(ks, np.abs(r["kernel"] - base["kernel"]).max(axis=1) / scale)
+    finally:
+        lib().swdo_set_group_ulp(0, 0)
+    return ks
+
+
 def map_spread(case, cols, rel=1e-15, steps=(-3, -1, 1, 3)):
     """The same conditioning probe for get_2d_map: the largest change of vout
     (km/s) per (slot, column) when the phase velocity handed to

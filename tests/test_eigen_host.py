@@ -124,3 +124,33 @@ def test_depth_truncation_changes_nothing_measurable(wave):
     print(f"truncated vs full: max rel diff {worst:.2e}, {cut} passes cut")
     assert worst <= 1e-12
     assert cut >= 3
+
+
+@pytest.mark.parametrize("wave", [2, 1], ids=["rayleigh", "love"])
+def test_node_sums_equal_per_layer_accumulation(wave):
+    """The kernel's node sums (NodeSink: the two nodes of the current
+    interval held while the sweep passes them, each stored once) equal a
+    per-layer kp[n] += w * (...) accumulation bit for bit, with and without
+    a merged fluid layer and with the depth truncation cutting the sweep."""
+    L_ = _lib()
+    L_.eig_host_nodesums.restype = C.c_int
+    rng = np.random.default_rng(5)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    nchecked = 0
+    for mi, (th, a, b, r) in enumerate(_models()[:3] + _models()[4:]):
+        L = len(th)
+        nw = 1 if mi == 3 else 0
+        nz = (L + 3) // 4 if nw == 0 else (L - 2) // 4 + 1 + nw
+        crs = f(rng.uniform(0.5, 2.0, 2 * nz))
+        cg, _, _ = O.surfdisp96(th, a, b, r, 0, wave, 1, 0, PERIODS, refine=1, rtol=1e-12, sngl=0)
+        for t, c in zip(PERIODS, cg):
+            if c == 0.0:
+                continue
+            for q in (0.0, 40.0):
+                kp, kref = np.zeros(nz), np.zeros(nz)
+                rc = L_.eig_host_nodesums(wave, L, _p(f(th)), _p(f(a)), _p(f(b)), _p(f(r)), nw, nz, _p(crs),
+                                          C.c_double(t), C.c_double(c), C.c_double(q), _p(kp), _p(kref))
+                assert rc == 0
+                np.testing.assert_array_equal(kp.view(np.int64), kref.view(np.int64))
+                nchecked += 1
+    assert nchecked >= 20

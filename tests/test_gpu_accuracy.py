@@ -25,9 +25,13 @@ tolerance passes only if the oracle's own U (km/s) and kernel (relative)
 move by comparable amounts under such changes (oracle_lib.kernel_spread):
 |dU| <= max(1e-6, 2 * U spread) and kernel error <= max(1e-5, 10 * kernel
 spread).  A group slot can also differ because its T(1 +- 0.005) roots,
-which the outputs do not show, round one REAL*4 ulp apart; such a slot
-passes if the oracle's U and kernel move as far under one ulp (2^-24) of
-its roots.  The numbers of exempted slots are printed.
+which the outputs do not show, round one REAL*4 ulp apart: sregnpu and
+slegnpu difference the phase kernels at those roots over a 1 % period step,
+so one ulp of either moves the group kernel by up to ~1e-4 of its largest
+value.  Such a slot passes if the oracle's U moves as far under one ulp
+(2^-24) of all its roots and its kernel as far under one ulp of all of them
+or of one hidden root alone (oracle_lib.group_root_spread).  The numbers of
+exempted slots are printed.
 """
 import numpy as np
 import pytest
@@ -72,20 +76,22 @@ def _report(name, seed):
     nexempt = nround = 0
     if len(bcols):
         ks, us = O.kernel_spread(case, bcols)
-        # the same under one REAL*4 ulp (2^-24) of the roots handed to the
-        # eigen routines: the group slots' T(1+-0.005) roots are not in the
-        # outputs, so a one-ulp difference there shows only through U
+        # the same under one REAL*4 ulp of the roots handed to the eigen
+        # routines: all of them (2^-24 relative), and the group slots' hidden
+        # T(1 +- 0.005) roots one at a time (they are not in the outputs)
         ks24, us24 = O.kernel_spread(case, bcols, rel=2.0 ** -24, steps=(-1, 1))
+        kg = O.group_root_spread(case, bcols)
         for j, col in enumerate(bcols):
             for s in np.nonzero(bad[:, col])[0]:
                 print(f"{name} slot {s} column {cols[col]}: |dc| {dc[s, col]:.3g}, |dU| {du[s, col]:.3g} "
                       f"(oracle U spread {us[s, j]:.3g}, {us24[s, j]:.3g} per ulp), kernel {kr[s, col]:.3g} "
-                      f"(oracle kernel spread {ks[s, j]:.3g}, {ks24[s, j]:.3g} per ulp)")
+                      f"(oracle kernel spread {ks[s, j]:.3g}, {ks24[s, j]:.3g} per ulp, {kg[s, j]:.3g} per ulp "
+                      f"of a hidden group root)")
                 if du[s, col] <= max(TOL_U, 2.0 * us[s, j]) and kr[s, col] <= max(TOL_K, 10.0 * ks[s, j]):
                     nexempt += 1
                     continue
                 assert du[s, col] <= max(TOL_U, 2.0 * us24[s, j])
-                assert kr[s, col] <= max(TOL_K, 2.0 * ks24[s, j])
+                assert kr[s, col] <= max(TOL_K, 2.0 * max(ks24[s, j], kg[s, j]))
                 nround += 1
     rms = lambda x: float(np.sqrt(np.mean(x[ok] ** 2)))
     line = (f"{name}: {NCOL} columns x {ref['vc'].shape[0]} slots ({int(ok.sum())} with a root): "

@@ -114,13 +114,14 @@ def test_ragged_48_model_batch_against_oracle_sampled():
                 r2 = O.kernel_at(sub, int(j), gg["vc"][s, j] / ref["vc"][s, j] - 1.0)
                 krs[s, j] = np.abs(gg["kernel"][s, :, j] - r2["kernel"][s, :, 0]).max() / scale[s, j]
             if krs[s, j] > TOL_K:
-                # or its sensitivity to one REAL*4 ulp of the roots (a group
-                # slot's T(1 +- 0.005) roots are not in the outputs)
+                # or its sensitivity to one REAL*4 ulp of the roots, all of
+                # them or a group slot's hidden T(1 +- 0.005) roots alone
                 ks, _ = O.kernel_spread(sub, np.array([j]))
                 ks24, _ = O.kernel_spread(sub, np.array([j]), rel=2.0 ** -24, steps=(-1, 1))
+                kg = O.group_root_spread(sub, np.array([j]))
                 print(f"model {i} slot {s}: kernel {krs[s, j]:.3g}, oracle spread {ks[s, 0]:.3g}, "
-                      f"{ks24[s, 0]:.3g} per ulp")
-                assert krs[s, j] <= max(10.0 * ks[s, 0], 2.0 * ks24[s, 0]), (i, s, krs[s, j])
+                      f"{ks24[s, 0]:.3g} per ulp, {kg[s, 0]:.3g} per ulp of a hidden group root")
+                assert krs[s, j] <= max(10.0 * ks[s, 0], 2.0 * max(ks24[s, 0], kg[s, 0])), (i, s, krs[s, j])
                 krs[s, j] = 0.0
         kr = krs[ok].max(initial=0.0)
         worst_k = max(worst_k, kr)

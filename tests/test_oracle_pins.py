@@ -8,6 +8,7 @@ import pytest
 from scipy.optimize import brentq
 
 import oracle_lib as O
+from jdsurfg_b200 import synth
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -224,3 +225,19 @@ def test_frechet_file_round_trip():
         assert np.array_equal(i0, i1) and np.array_equal(v0, v1)
         assert np.all(np.diff(i1) > 0) and np.all(np.abs(v1) > 0)
     assert len(back[1][1]) == 0
+
+
+def test_group_root_probe_moves_only_group_slots():
+    """oracle_lib.group_root_spread moves the hidden roots c1, c2 of the
+    group kernels (sregnpu/slegnpu) by one REAL*4 ulp: phase slots stay
+    exactly, group slots move, and the probe leaves the oracle unchanged."""
+    case = synth.make_config("tiny", seed=3)
+    cols = np.arange(2)
+    base = O.get_1d_kernel(case, cols=cols)
+    kg = O.group_root_spread(case, cols)
+    nt = kg.shape[0] // 4  # Rc, Rg, Lc, Lg, mode 0
+    ok = base["status"] != 1
+    assert np.all(kg[:nt][ok[:nt]] == 0.0) and np.all(kg[2 * nt:3 * nt][ok[2 * nt:3 * nt]] == 0.0)
+    assert np.all(kg[nt:2 * nt][ok[nt:2 * nt]] > 0.0) and np.all(kg[3 * nt:][ok[3 * nt:]] > 0.0)
+    again = O.get_1d_kernel(case, cols=cols)
+    np.testing.assert_array_equal(again["kernel"], base["kernel"])
