@@ -1749,8 +1749,11 @@ int ensure_kids(swdk_ctx* ctx) {
   return SWDK_OK;
 }
 
-bool use_split(const swdk_ctx* ctx, int path, int ncol) {
-  const int lim = ctx->cfg.split_cols == 0 ? SPLIT_MIN_COLS : ctx->cfg.split_cols;
+// split_cols 0: host-memory calls split (each half's copies overlap the
+// other half's compute); device calls do not (two concurrent persistent
+// root searches only contend: 577 vs 557 ms per step on the default workload)
+bool use_split(const swdk_ctx* ctx, int path, int ncol, bool host) {
+  const int lim = ctx->cfg.split_cols == 0 ? (host ? SPLIT_MIN_COLS : 0) : ctx->cfg.split_cols;
   return path != 2 && lim > 0 && ncol >= lim && ncol >= 2;
 }
 
@@ -1758,7 +1761,7 @@ bool use_split(const swdk_ctx* ctx, int path, int ncol) {
 int run_split(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
               const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status, cudaStream_t st) {
   const int ncol = nx * ny;
-  if (!use_split(ctx, path, ncol) || nx <= 0 || ny <= 0) {
+  if (!use_split(ctx, path, ncol, false) || nx <= 0 || ny <= 0) {
     ctx->last_split = false;
     return run_device(ctx, path, nx, ny, nz, d_vs, d_vp, d_rho, d_vc, d_vout, d_kernel, d_status, st);
   }
@@ -1833,7 +1836,7 @@ int run_host(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* vs, c
   int r = ensure_plans(ctx);
   if (r) return r;
   const int ncol = nx * ny;
-  if (!use_split(ctx, path, ncol)) {
+  if (!use_split(ctx, path, ncol, true)) {
     r = host_piece(ctx, ctx, path, ncol, 0, ncol, nz, vs, vp, rho, vc, vout, kernel, status);
     if (r) return r;
     CK(cudaStreamSynchronize(ctx->stream));

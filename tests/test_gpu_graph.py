@@ -85,13 +85,14 @@ def test_autotune_keeps_results():
 
 @pytest.mark.parametrize("path", ["kernel", "map"])
 def test_column_halves_equal_one_piece(path):
-    """Large calls run as two concurrent column halves on child contexts; the
-    results must be the bits of the one-piece call, for device and host calls."""
+    """Calls split as two concurrent column halves on child contexts
+    (split_cols 8192; by default only host-memory calls split) give the bits
+    of the one-piece call, for device and host calls."""
     import torch
     dev = torch.device("cuda", 0)
     a = synth.subset_columns(synth.make_config("production", seed=2024), np.arange(9000))
     outs = []
-    for split in (-1, 0):
+    for split in (-1, 8192):
         eng = Engine(device=0, split_cols=split)
         keep = learn.load_proposals(eng)
         eng.setup(a)
