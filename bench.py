@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--ncols", type=int, default=0, help="use only the first N columns (profiling)")
     ap.add_argument("--refine", default="tight", choices=["tight", "reference"])
     ap.add_argument("--split-cols", type=int, default=0,
-                    help="column count from which a call runs as two halves (0 default, -1 never; profiling)")
+                    help="column count from which a call runs as two concurrent halves (0, the default: never)")
     ap.add_argument("--roots-blocks", type=int, default=0, help="fixed root-search grid (0: default/autotuned)")
     ap.add_argument("--no-node-layers", action="store_true",
                     help="root search reads the full layer tables instead of rebuilding sublayers from the nodes")

@@ -78,10 +78,10 @@ typedef struct swdk_config {
   int block_roots; /* blocks of the persistent root kernel, 0 = occupancy
                       default (swdk_autotune sets it)                       */
   int split_cols;  /* calls with at least this many columns run as two
-                      concurrent column halves; 0 = host-memory calls of
-                      8192 columns or more (one half's copies overlap the
-                      other half's compute), device calls never; < 0 =
-                      never                                                 */
+                      concurrent column halves on child contexts; <= 0
+                      (default) = never.  Host-memory calls stream their
+                      outputs back behind the eigen stage's column chunks
+                      either way.                                           */
   int node_layers; /* 1 (default): the root search rebuilds each column's
                       flattened sublayers from its grid nodes and one
                       per-depth table (the same arithmetic as the layer

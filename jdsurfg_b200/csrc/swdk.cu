@@ -1118,8 +1118,9 @@ __global__ void __launch_bounds__(128, (WT >= 2) ? SWDK_EIGEN_MINB_LOVE : SWDK_E
                                                const SlotDesc* __restrict__ slots, int g0, int gn,
                                                const double* __restrict__ croot, const int32_t* __restrict__ cstat,
                                                int sphere, double* __restrict__ vc, double* __restrict__ vout,
-                                               double* __restrict__ kernel, int32_t* __restrict__ status, int ldo) {
-  eigen_column<WT, PATH>(blockIdx.x, ncol, nz, Lmax, lay0, info, chainrule, slots, g0, gn, croot, cstat, sphere, vc,
+                                               double* __restrict__ kernel, int32_t* __restrict__ status, int ldo,
+                                               int col0) {
+  eigen_column<WT, PATH>(col0 + (int)blockIdx.x, ncol, nz, Lmax, lay0, info, chainrule, slots, g0, gn, croot, cstat, sphere, vc,
                          vout, kernel, status, ldo);
 }
 
@@ -1334,6 +1335,10 @@ struct swdk_ctx {
   swdk_ctx* kids[2] = {nullptr, nullptr};
   cudaEvent_t evfork = nullptr, evjoin[2] = {nullptr, nullptr};
   bool last_split = false;
+  // host-memory calls: the copy stream of the chunked output copies and
+  // one event per chunk plus one for the end of the copies
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t evchunk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   // CUDA graph of one call (swdk_graph_capture / swdk_graph_launch)
   bool capturing = false;
   cudaGraph_t graph = nullptr;
@@ -1535,9 +1540,21 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st, const
 // ldi / ldo: row strides (in columns) of the input model and of the outputs,
 // >= nx*ny; -1 = nx*ny (dense).  A column block of a larger model runs with
 // the pointers offset to its first column and the large model's strides.
+// Host destination of a host-memory call's outputs: columns c0.. of
+// (rows, ld) arrays.
+struct HostOut {
+  double *vc, *vout, *kernel;
+  int32_t* status;
+  int ld, c0;
+};
+constexpr int HOST_CHUNKS = 4;  // eigen chunks of a host-memory call
+
+int launch_eigen(swdk_ctx* ctx, const Plan& P, int path, int ncol, int nz, int c0, int c1, double* d_vc,
+                 double* d_vout, double* d_kernel, int32_t* d_status, int ldo, cudaStream_t st);
+
 int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_vs, const float* d_vp,
                const float* d_rho, double* d_vc, double* d_vout, double* d_kernel, int32_t* d_status,
-               cudaStream_t st, int ldi = -1, int ldo = -1) {
+               cudaStream_t st, int ldi = -1, int ldo = -1, const HostOut* ho = nullptr) {
   const bool roots_only = (path == 2);
   if (roots_only) path = 0;
   if (nx <= 0 || ny <= 0 || !d_vs || (!roots_only && (!d_vc || !d_vout || (path == 0 && !d_kernel))))
@@ -1631,22 +1648,39 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
   CK(cudaGetLastError());
   if (timing) CK(cudaEventRecord(ctx->ev[2], st));
   if (!roots_only) {
-
-    using EigFn = void (*)(int, int, int, const float4*, const ColInfo*, const float2*, const SlotDesc*, int, int,
-                           const double*, const int32_t*, int, double*, double*, double*, int32_t*, int);
-    static const EigFn eig[4][2] = {{k_eigen<0, 0>, k_eigen<0, 1>}, {k_eigen<1, 0>, k_eigen<1, 1>},
-                                    {k_eigen<2, 0>, k_eigen<2, 1>}, {k_eigen<3, 0>, k_eigen<3, 1>}};
-    for (int g = 0; g < P.groups.n; ++g) {
-      const int g0 = P.groups.start[g], gn = P.groups.count[g];
-      const int wt = P.slots[g0].wtype;
-      const int et = std::min(128, ((gn + 31) / 32) * 32);
-      const size_t smem = (size_t)Lmax * (wt >= 2 ? sizeof(LoveLayer) : sizeof(RayLayer)) + (size_t)nz * sizeof(float2);
-      ctx->launches += 1;
-      eig[wt][path]<<<ncol, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
-                                            ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), g0, gn,
-                                            ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere, d_vc,
-                                            d_vout, d_kernel, d_status, ldo);
-      CK(cudaGetLastError());
+    if (!ho) {
+      r = launch_eigen(ctx, P, path, ncol, nz, 0, ncol, d_vc, d_vout, d_kernel, d_status, ldo, st);
+      if (r) return r;
+    } else {
+      // host-memory call: the eigen stage in column chunks, each chunk's
+      // outputs copied to the host on the copy stream while the next chunk
+      // computes
+      if (!ctx->cstream) CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+      for (int i = 0; i <= HOST_CHUNKS; ++i)
+        if (!ctx->evchunk[i]) CK(cudaEventCreateWithFlags(&ctx->evchunk[i], cudaEventDisableTiming));
+      const int kmax = P.kmax;
+      for (int h = 0; h < HOST_CHUNKS; ++h) {
+        const int a = (int)((long long)ncol * h / HOST_CHUNKS), b = (int)((long long)ncol * (h + 1) / HOST_CHUNKS);
+        if (b <= a) continue;
+        r = launch_eigen(ctx, P, path, ncol, nz, a, b, d_vc, d_vout, d_kernel, d_status, ldo, st);
+        if (r) return r;
+        CK(cudaEventRecord(ctx->evchunk[h], st));
+        CK(cudaStreamWaitEvent(ctx->cstream, ctx->evchunk[h], 0));
+        const size_t w = (size_t)(b - a);
+        const size_t hp = (size_t)ho->ld;
+        CK(cudaMemcpy2DAsync(ho->vc + ho->c0 + a, hp * sizeof(double), d_vc + a, (size_t)ldo * sizeof(double),
+                             w * sizeof(double), kmax, cudaMemcpyDeviceToHost, ctx->cstream));
+        CK(cudaMemcpy2DAsync(ho->vout + ho->c0 + a, hp * sizeof(double), d_vout + a, (size_t)ldo * sizeof(double),
+                             w * sizeof(double), kmax, cudaMemcpyDeviceToHost, ctx->cstream));
+        if (ho->status)
+          CK(cudaMemcpy2DAsync(ho->status + ho->c0 + a, hp * sizeof(int32_t), d_status + a,
+                               (size_t)ldo * sizeof(int32_t), w * sizeof(int32_t), kmax, cudaMemcpyDeviceToHost,
+                               ctx->cstream));
+        if (path == 0)
+          CK(cudaMemcpy2DAsync(ho->kernel + ho->c0 + a, hp * sizeof(double), d_kernel + a,
+                               (size_t)ldo * sizeof(double), w * sizeof(double), (size_t)kmax * nz,
+                               cudaMemcpyDeviceToHost, ctx->cstream));
+      }
     }
   }
   if (timing) {
@@ -1654,6 +1688,10 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
     CK(cudaMemcpyAsync(ctx->h_nevals, ctx->nevals.p, NCOUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(ctx->ev[4], st));
     ctx->stats_pending = true;
+  }
+  if (ho && !roots_only) {  // the call's stream waits for the output copies
+    CK(cudaEventRecord(ctx->evchunk[HOST_CHUNKS], ctx->cstream));
+    CK(cudaStreamWaitEvent(st, ctx->evchunk[HOST_CHUNKS], 0));
   }
   ctx->stats.nchains = (int)P.chains.size();
   ctx->stats.nslots = P.kmax;
@@ -1704,14 +1742,35 @@ void collect_stats(swdk_ctx* ctx) {
   cudaEventElapsedTime(&ctx->stats.ms_eigen, ctx->ev[2], ctx->ev[3]);
 }
 
+// the eigen stage over columns [c0, c1): one launch per wave-type slot group
+int launch_eigen(swdk_ctx* ctx, const Plan& P, int path, int ncol, int nz, int c0, int c1, double* d_vc,
+                 double* d_vout, double* d_kernel, int32_t* d_status, int ldo, cudaStream_t st) {
+  using EigFn = void (*)(int, int, int, const float4*, const ColInfo*, const float2*, const SlotDesc*, int, int,
+                         const double*, const int32_t*, int, double*, double*, double*, int32_t*, int, int);
+  static const EigFn eig[4][2] = {{k_eigen<0, 0>, k_eigen<0, 1>}, {k_eigen<1, 0>, k_eigen<1, 1>},
+                                  {k_eigen<2, 0>, k_eigen<2, 1>}, {k_eigen<3, 0>, k_eigen<3, 1>}};
+  const int Lmax = 4 * nz - 3;
+  for (int g = 0; g < P.groups.n; ++g) {
+    const int g0 = P.groups.start[g], gn = P.groups.count[g];
+    const int wt = P.slots[g0].wtype;
+    const int et = std::min(128, ((gn + 31) / 32) * 32);
+    const size_t smem = (size_t)Lmax * (wt >= 2 ? sizeof(LoveLayer) : sizeof(RayLayer)) + (size_t)nz * sizeof(float2);
+    ctx->launches += 1;
+    eig[wt][path]<<<c1 - c0, et, smem, st>>>(ncol, nz, Lmax, ctx->lay0.as<float4>(), ctx->info.as<ColInfo>(),
+                                             ctx->chainrule.as<float2>(), P.d_slots.as<SlotDesc>(), g0, gn,
+                                             ctx->croot.as<double>(), ctx->cstat.as<int32_t>(), ctx->cfg.sphere,
+                                             d_vc, d_vout, d_kernel, d_status, ldo, c0);
+    CK(cudaGetLastError());
+  }
+  return SWDK_OK;
+}
+
 void drop_graph(swdk_ctx* ctx) {
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   ctx->gexec = nullptr;
   ctx->graph = nullptr;
 }
-
-constexpr int SPLIT_MIN_COLS = 8192;  // calls with fewer columns run as one piece
 
 void drop_kids(swdk_ctx* ctx) {
   for (int i = 0; i < 2; ++i) {
@@ -1749,11 +1808,14 @@ int ensure_kids(swdk_ctx* ctx) {
   return SWDK_OK;
 }
 
-// split_cols 0: host-memory calls split (each half's copies overlap the
-// other half's compute); device calls do not (two concurrent persistent
-// root searches only contend: 577 vs 557 ms per step on the default workload)
+// split_cols 0 (default): no call splits.  Two concurrent persistent root
+// searches only contend (577 vs 557 ms per device step on the default
+// workload), and a host-memory call streams its outputs back behind the
+// eigen stage's column chunks instead (e2e 13.9 M slots/s unsplit, 13.7 M
+// split).
 bool use_split(const swdk_ctx* ctx, int path, int ncol, bool host) {
-  const int lim = ctx->cfg.split_cols == 0 ? (host ? SPLIT_MIN_COLS : 0) : ctx->cfg.split_cols;
+  (void)host;
+  const int lim = ctx->cfg.split_cols;
   return path != 2 && lim > 0 && ncol >= lim && ncol >= 2;
 }
 
@@ -1813,18 +1875,14 @@ int host_piece(swdk_ctx* ctx, swdk_ctx* k, int path, int ncol, int c0, int n, in
     CK(cudaMemcpy2DAsync(k->in_vp.p, fw, vp + c0, ncol * sizeof(float), fw, nz, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpy2DAsync(k->in_rho.p, fw, rho + c0, ncol * sizeof(float), fw, nz, cudaMemcpyHostToDevice, st));
   }
+  // the outputs stream back chunk by chunk behind the eigen stage
+  const HostOut ho{vc, vout, kernel, status, ncol, c0};
   r = run_device(k, path, n, 1, nz, k->in_vs.as<float>(), vp ? k->in_vp.as<float>() : nullptr,
                  vp ? k->in_rho.as<float>() : nullptr, k->out_vc.as<double>(), k->out_vout.as<double>(),
-                 path == 0 ? k->out_kernel.as<double>() : nullptr, k->out_status.as<int32_t>(), st);
+                 path == 0 ? k->out_kernel.as<double>() : nullptr, k->out_status.as<int32_t>(), st, -1, -1, &ho);
   if (r) return fail(ctx, r, k->err);
-  CK(cudaMemcpy2DAsync(vc + c0, ncol * sizeof(double), k->out_vc.p, dw, dw, kmax, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpy2DAsync(vout + c0, ncol * sizeof(double), k->out_vout.p, dw, dw, kmax, cudaMemcpyDeviceToHost, st));
-  if (status)
-    CK(cudaMemcpy2DAsync(status + c0, ncol * sizeof(int32_t), k->out_status.p, iw, iw, kmax, cudaMemcpyDeviceToHost,
-                         st));
-  if (path == 0)
-    CK(cudaMemcpy2DAsync(kernel + c0, ncol * sizeof(double), k->out_kernel.p, dw, dw, (size_t)kmax * nz,
-                         cudaMemcpyDeviceToHost, st));
+  (void)dw;
+  (void)iw;
   return SWDK_OK;
 }
 
@@ -1938,6 +1996,12 @@ void swdk_destroy(swdk_ctx* ctx) {
   drop_kids(ctx);
   for (int i = 0; i < 6; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  for (cudaEvent_t e : ctx->evchunk)
+    if (e) cudaEventDestroy(e);
+  if (ctx->cstream) {
+    cudaStreamSynchronize(ctx->cstream);
+    cudaStreamDestroy(ctx->cstream);
+  }
   if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

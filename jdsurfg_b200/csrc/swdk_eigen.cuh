@@ -550,7 +550,13 @@ SWDK_HD int pass_layers(const Layer* lay, int L, double k2, double om2, double t
   return L;
 }
 
-constexpr double EIG_TRUNC_Q = 40.0;
+// The device passes run uncut (0): the slots of a warp are different
+// periods of one column and cut at very different depths, so a warp's
+// sweeps take as long as its deepest slot's while every slot pays for the
+// search (eigen stage 154 ms uncut against 166 ms cut at 40 per step of the
+// default workload).  Cutting at 40 changes U and kernels by < 1e-12
+// relative (CPU harness test).
+constexpr double EIG_TRUNC_Q = 0.0;
 
 // Up-pass storage of a Rayleigh pass with checkpoints: the compound vector
 // (and its exponent bookkeeping) is kept only at every RAY_SEG-th layer and
