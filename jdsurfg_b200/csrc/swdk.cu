@@ -48,7 +48,7 @@ constexpr int EV_BASE = 5;
 struct ColInfo {
   double cc;    // surfdisp96 start value cc (surfdisp96.f:222)
   float betmx;  // largest flattened shear velocity
-  float htot;   // total flattened thickness of the finite layers
+  float pad_;
   int L;        // sublayers incl. half-space
   int llw;      // 2 if the top layer is fluid
   int nw;       // leading fluid grid nodes
@@ -185,9 +185,6 @@ __device__ void sd96_setup(int L, int sphere, float* d, float* a, float* b, cons
   cc1 = fmul(0.90f, cc1);
   ci.cc = (double)cc1;
   ci.betmx = betmx;
-  float ht = 0.0f;
-  for (int i = 0; i < L - 1; ++i) ht += d[i];
-  ci.htot = ht;
 }
 
 __device__ __forceinline__ bool finitef(float x) { return isfinite(x); }
@@ -447,9 +444,6 @@ __device__ __forceinline__ void roots_body(const ChainDesc cd, int ncol, const d
   V.wave = cd.iwave;
   V.L = ci.L;
   V.llw = ci.llw;
-  V.trunc = 0;
-  V.htot = ci.htot;
-  V.bmax = ci.betmx;
   ChainParams P;
   P.t = periods + cd.t_off;
   P.kmax = cd.np;
@@ -662,9 +656,6 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
         V.lstride = lstride;
         V.L = ci.L;
         V.llw = ci.llw;
-        V.trunc = (refine == 1);
-        V.htot = ci.htot;
-        V.bmax = ci.betmx;
         V.nodes = (nodes && ci.nw == 0) ? nodes + o_node + (size_t)col * ((lstride + 3) / 4) : nullptr;
         V.dl = dl + o_dl;
         V.wave = cd.iwave;
@@ -834,9 +825,6 @@ __global__ void __launch_bounds__(128, SWDK_RETRY_MINB) k_retry(int ncol, const 
     V.lstride = lstride;
     V.L = ci.L;
     V.llw = ci.llw;
-    V.trunc = (refine == 1);
-    V.htot = ci.htot;
-    V.bmax = ci.betmx;
     V.nodes = (nodes && ci.nw == 0) ? nodes + o_node + (size_t)col * ((lstride + 3) / 4) : nullptr;
     V.dl = dl + o_dl;
     V.wave = cd.iwave;

@@ -138,8 +138,6 @@ struct LayerView {
   int lstride;  // layer slots per column of the table (column-major layout)
   int L;    // layers including the half-space
   int llw;  // 2 when the top layer is fluid (surfdisp96.f:143-144)
-  int trunc;          // secular_fast may cut the depth (secular_depth)
-  float htot, bmax;   // total finite-layer thickness and largest shear velocity
   // node source (null: the layer table): the column's grid nodes
   // (vp, vs, rho, -) and the depth grid's flattening factors
   const float4* nodes;
@@ -512,56 +510,13 @@ SWDK_HD void apply_dunkin(const LayerCoef& k, double wvno2, double& e0, double& 
   e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
 }
 
-// Depth cut of one secular evaluation.  The period equation's value is the
-// propagated compound (Rayleigh) or Haskell (Love) vector at the surface;
-// in an evanescent layer its parts below the dominant one shrink by
-// exp(-2 Re(r_beta) d) relative to it, so below the depth where
-// sum(Re(r_beta) d) from the top exceeds SEC_TRUNC_Q the deeper structure
-// changes the value by less than exp(-2 SEC_TRUNC_Q) relative, far below
-// rounding: the evaluation then starts from the next layer as its
-// half-space.  Returns the index of the layer used as the half-space (L-1:
-// no cut).  A bound k H sqrt(1 - c^2/bmax^2) on the whole column's decay
-// skips the search where no cut is possible (long periods).
-constexpr double SEC_TRUNC_Q = 30.0;
-
-template <bool NODES>
-SWDK_HD int secular_depth(const LayerView& V, double wvno, double omega) {
-  if (!V.trunc) return V.L - 1;
-  const double c = omega / wvno, bm = V.bmax;
-  const double u = 1.0 - (c / bm) * (c / bm);
-  // A warp's lanes run their layer loops together, so a cut pays only when
-  // every lane evaluating with it can cut: the search is skipped unless all
-  // of them pass the bound (327.9 vs 334.5 ms of root search per step on
-  // the default workload; searching per lane regardless: 359 ms).
-  const bool can = (u > 0.0) && wvno * (double)V.htot * sqrt(u) > SEC_TRUNC_Q;
-#ifdef __CUDA_ARCH__
-  if (!__all_sync(__activemask(), can)) return V.L - 1;
-#else
-  if (!can) return V.L - 1;
-#endif
-  const double wvno2 = wvno * wvno;
-  double cum = 0.0;
-  LayerView::Walk wk;
-  V.walk_start<1, NODES>(wk, V.llw - 1);
-  for (int m = V.llw - 1; m < V.L - 2; ++m) {
-    const float4 ly = V.walk_layer<1, NODES>(wk, m);
-    if (ly.z > 0.0f) {
-      const double xkb = omega * recip((double)ly.z);
-      const double x2 = wvno2 - xkb * xkb;
-      if (x2 > 0.0) cum += x2 * rsqrt(x2) * (double)ly.x;
-    }
-    if (cum > SEC_TRUNC_Q) return m + 1;
-  }
-  return V.L - 1;
-}
-
 template <int NORM, bool NODES>
 SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   double omega = omga;
   if (omega < 1.0e-4) omega = 1.0e-4;
   const double wvno2 = wvno * wvno;
   const double iom = 1.0 / omega;
-  const int hs = secular_depth<NODES>(V, wvno, omega);  // the layer taken as the half-space
+  const int hs = V.L - 1;  // the half-space
   const float4 h = V.layer(hs);
   double xka = omega * recip((double)h.y), xkb = omega * recip((double)h.z);
   const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
@@ -579,11 +534,7 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
   const int mlo = V.llw - 1;
   int since = 0;
   LayerView::Walk wk;
-  if (hs - 1 >= mlo) V.walk_start<-1, NODES>(wk, hs - 1);
-  for (int m = hs - 1; m >= mlo; --m) {
-    const float4 cur_ly = V.walk_layer<-1, NODES>(wk, m);
-    const LayerCoef cur = layer_coef(cur_ly, wvno, wvno2, omega, iom);
-    apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
+  auto norm_e = [&](int m) {
     if (++since >= NORM || m == mlo) {
       since = 0;
       double t1 = fmax(fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))), fabs(e4));
@@ -595,6 +546,21 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
         e0 *= it1; e1 *= it1; e2 *= it1; e3 *= it1; e4 *= it1;
       }
     }
+  };
+  if (hs - 1 >= mlo) {
+    V.walk_start<-1, NODES>(wk, hs - 1);
+    LayerCoef cur = layer_coef(V.walk_layer<-1, NODES>(wk, hs - 1), wvno, wvno2, omega, iom);
+    int m = hs - 1;
+    for (; m > mlo; --m) {
+      // the next layer's coefficients do not depend on e: computed while
+      // this layer's product runs (root search 336 -> 327 ms per step)
+      const float4 nly = V.walk_layer<-1, NODES>(wk, m - 1);
+      apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
+      cur = layer_coef(nly, wvno, wvno2, omega, iom);
+      norm_e(m);
+    }
+    apply_dunkin(cur, wvno2, e0, e1, e2, e3, e4);
+    norm_e(m);
   }
   if (V.llw != 1) {
     const float4 ly = V.layer(0);
@@ -624,7 +590,7 @@ SWDK_HDI double dltar4_fast(const LayerView& V, double wvno, double omga) {
 // dltar1 with 1/b and 1/(rho b^2) from recip()
 template <int NORM, bool NODES>
 SWDK_HDI double dltar1_fast(const LayerView& V, double wvno, double omega) {
-  const int hs = secular_depth<NODES>(V, wvno, omega);  // the layer taken as the half-space
+  const int hs = V.L - 1;  // the half-space
   float4 h = V.layer(hs);
   double beta1 = h.z, rho1 = h.w;
   double xkb = omega * recip(beta1);
