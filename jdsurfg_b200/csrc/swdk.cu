@@ -2625,35 +2625,23 @@ int swdk_ragged_create(int n, swdk_ctx* const* ctxs, const swdk_call* calls, swd
       c->depth_dev = c->depth_d.p;
     }
   }
-  // root work blocks, the dearest items first so that the queue's tail is
-  // made of cheap ones: an item's cost is taken as layers x periods x modes,
-  // x2 for a group chain (two roots per period) and x4 for Rayleigh (its
-  // layer step costs about four of Love's)
-  {
-    struct Cand {
-      double cost;
-      int model, chain;
-    };
-    std::vector<Cand> cand;
+  // root work blocks: every model's Rayleigh chains, then the Love chains,
+  // model by model, so the items in flight share a few models' node arrays
+  // in L2 (ordering the blocks by cost across models instead measured 4 %
+  // slower on the 48-model batch)
+  for (int w = 2; w >= 1; --w)
     for (int i = 0; i < n; ++i) {
       const Plan& P = ctxs[i]->plan[ppath];
       for (int ci : P.order) {
-        const ChainDesc& cd = P.chains[ci];
-        const double cost = (double)(4 * calls[i].nz - 3) * cd.np * cd.nmode * (cd.igr > 0 ? 2.0 : 1.0) *
-                            (cd.iwave == 2 ? 4.0 : 1.0);
-        cand.push_back({cost, i, chain0[i] + ci});
+        if (P.chains[ci].iwave != w) continue;
+        RBlock B;
+        B.item0 = R->nitems;
+        B.model = i;
+        B.chain = chain0[i] + ci;
+        R->blocks.push_back(B);
+        R->nitems += R->models[i].ncol;
       }
     }
-    std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.cost > b.cost; });
-    for (const Cand& c : cand) {
-      RBlock B;
-      B.item0 = R->nitems;
-      B.model = c.model;
-      B.chain = c.chain;
-      R->blocks.push_back(B);
-      R->nitems += R->models[c.model].ncol;
-    }
-  }
   if (R->nitems >= 0x7fffffffLL) return bail(SWDK_E_LIMIT, "ragged batch: too many work items");
   auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
     cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
