@@ -568,13 +568,13 @@ __device__ __forceinline__ int ragged_find(const T* tab, int n, long long key, l
 constexpr size_t ROOTS_SMEM = 128 * (sizeof(ChainState) + sizeof(ChainParams) + sizeof(ChainIO));
 
 #ifndef SWDK_ROOTS_MINB
-#define SWDK_ROOTS_MINB 4  // 128 registers (64 B spill): roots 381 ms on the default workload; 5 blocks (96 registers) spill 660 B, 471 ms
+#define SWDK_ROOTS_MINB 4  // 127 registers, no spill (shared memory allows 4 blocks too); 3 blocks measured slower
 #endif
 #ifndef SWDK_RETRY_MINB
-#define SWDK_RETRY_MINB 2  // retries: 192 registers, no spill; one record per warp, fewer records than resident warps
+#define SWDK_RETRY_MINB 2  // retries: no spill; one record per warp, fewer records than resident warps
 #endif
 #ifndef SWDK_EIGEN_MINB
-#define SWDK_EIGEN_MINB 3  // Rayleigh passes: 168 registers, no spill; eigen 171 ms on the default workload (4: 180 ms, 5: 227 ms)
+#define SWDK_EIGEN_MINB 3  // Rayleigh passes: 168 registers, no spill (2: 183, 3: 171, 4: 180, 5: 227 ms of eigen per step)
 #endif
 #ifndef SWDK_EIGEN_MINB_LOVE
 #define SWDK_EIGEN_MINB_LOVE 5  // Love passes
@@ -594,8 +594,6 @@ __global__ void __launch_bounds__(128, SWDK_ROOTS_MINB) k_roots_queue(int ncol, 
                                                      const DepthLayer* __restrict__ dl) {
   double cbuf[KMAX_CHAIN];
   double cbbuf[KMAX_CHAIN + 24];
-  // the chain's state machine lives in shared memory, so the registers go to
-  // the secular function: 96 registers, 5 blocks of 128 per SM
   // dynamic shared memory (ROOTS_SMEM): the chain states, and the chains'
   // parameters and output addressing, which the state machine reads between
   // evaluations instead of holding them in registers across them
@@ -1323,10 +1321,9 @@ struct swdk_ctx {
   int last_ncol = 0, last_path = -1;
   // depth vector on the device (uploaded once per swdk_set_depth)
   const void* depth_dev = nullptr;
-  // large calls run as two column halves on two child contexts (own
-  // buffers and streams), forked from and joined back into the caller's
-  // stream, so each half's stage tails overlap the other half's work and,
-  // for host calls, the copies of one half overlap the other's compute
+  // with split_cols > 0, large calls run as two column halves on two child
+  // contexts (own buffers and streams), forked from and joined back into the
+  // caller's stream
   swdk_ctx* kids[2] = {nullptr, nullptr};
   cudaEvent_t evfork = nullptr, evjoin[2] = {nullptr, nullptr};
   bool last_split = false;

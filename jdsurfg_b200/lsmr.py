@@ -28,17 +28,40 @@ from .engine import SwdkError, lib
 
 class DeviceCSR:
     """m x n matrix as device CSR (torch tensors): rowptr int64 (m+1),
-    indices int32, values float32."""
+    indices int32, values float32.
 
-    def __init__(self, rowptr, indices, values, m, n):
+    deterministic=True (the default) keeps the transposed matrix too (built
+    once on the device, a column's entries in row order), so A^T y is a row
+    product like A x: the same sums in the same order on every call.  With
+    False, A^T y scatters with FP64 atomics (the reference's myaprod_csr uses
+    an OpenMP atomic the same way) and its last bits vary between calls."""
+
+    def __init__(self, rowptr, indices, values, m, n, deterministic=True):
         self.rowptr, self.indices, self.values, self.m, self.n = rowptr, indices, values, m, n
         L = lib()
         L.swdk_aprod_csr.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]
+        self.t = self.transpose() if deterministic else None
+
+    def transpose(self):
+        """The n x m transpose as device CSR, each row (a column of A) with its
+        entries in increasing row order."""
+        import torch
+        dev = self.rowptr.device
+        counts = torch.diff(self.rowptr)
+        rows = torch.repeat_interleave(torch.arange(self.m, dtype=torch.int32, device=dev), counts)
+        perm = torch.argsort(self.indices, stable=True)
+        colptr = torch.zeros(self.n + 1, dtype=torch.int64, device=dev)
+        colptr[1:] = torch.cumsum(torch.bincount(self.indices, minlength=self.n), 0)
+        return DeviceCSR(colptr, rows[perm].contiguous(), self.values[perm].contiguous(), self.n, self.m,
+                         deterministic=False)
 
     def aprod(self, mode, x, y):
         """mode 1: y += A x; mode 2: x += A^T y (x, y FP64 device tensors)."""
         import torch
+        if mode == 2 and self.t is not None:
+            self.t.aprod(1, y, x)
+            return
         st = torch.cuda.current_stream(x.device).cuda_stream
         rc = lib().swdk_aprod_csr(mode, self.m, self.n, self.rowptr.data_ptr(), self.indices.data_ptr(),
                                   self.values.data_ptr(), x.data_ptr(), y.data_ptr(), st)

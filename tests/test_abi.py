@@ -45,6 +45,8 @@ def test_config_defaults_and_arg_checks():
     cfg = Config()
     assert lib.swdk_config_default(C.byref(cfg)) == 0
     assert cfg.refine == 1 and cfg.sngl == 1 and cfg.sphere == 1 and abs(cfg.rtol - 1e-10) < 1e-20
+    # node-rebuilt layers on; no call splits into column halves unless asked
+    assert cfg.node_layers == 1 and cfg.split_cols == 0 and cfg.block_roots == 0
     assert lib.swdk_config_default(None) == -1
     assert lib.swdk_create(None, None) == -1
     assert lib.swdk_kmax(None) == 0

@@ -17,13 +17,14 @@ def _problem(m, n, density, seed):
     return A, b
 
 
-def _device(A):
+def _device(A, deterministic=True):
     import torch
     from jdsurfg_b200.lsmr import DeviceCSR
     d = torch.device("cuda", 0)
     return DeviceCSR(torch.from_numpy(A.indptr.astype(np.int64)).to(d),
                      torch.from_numpy(A.indices.astype(np.int32)).to(d),
-                     torch.from_numpy(A.data.astype(np.float32)).to(d), A.shape[0], A.shape[1])
+                     torch.from_numpy(A.data.astype(np.float32)).to(d), A.shape[0], A.shape[1],
+                     deterministic=deterministic)
 
 
 def test_csr_products_match_scipy():
@@ -41,6 +42,30 @@ def test_csr_products_match_scipy():
     xd = torch.from_numpy(x0.copy()).cuda()
     D.aprod(2, xd, torch.from_numpy(y0).cuda())
     assert np.allclose(xd.cpu().numpy(), x0 + A.T @ y0, rtol=1e-11, atol=1e-11)
+    # the scattering product (FP64 atomics) agrees to rounding
+    xa = torch.from_numpy(x0.copy()).cuda()
+    _device(A, deterministic=False).aprod(2, xa, torch.from_numpy(y0).cuda())
+    assert np.allclose(xa.cpu().numpy(), xd.cpu().numpy(), rtol=1e-12, atol=1e-12)
+
+
+def test_transpose_product_is_deterministic_and_matches_row_order():
+    """A^T y through the device transpose: the same bits on every call, and
+    the transpose holds A's entries column by column in row order."""
+    import torch
+    A, _ = _problem(4000, 1500, 0.02, 5)
+    D = _device(A)
+    T = A.T.tocsr()
+    T.sort_indices()
+    assert np.array_equal(D.t.rowptr.cpu().numpy(), T.indptr)
+    assert np.array_equal(D.t.indices.cpu().numpy(), T.indices)
+    assert np.array_equal(D.t.values.cpu().numpy(), T.data.astype(np.float32))
+    y = torch.from_numpy(np.random.default_rng(6).standard_normal(4000)).cuda()
+    outs = []
+    for _ in range(3):
+        x = torch.zeros(1500, dtype=torch.float64, device="cuda")
+        D.aprod(2, x, y)
+        outs.append(x.cpu().numpy())
+    assert all(np.array_equal(outs[0].view(np.int64), o.view(np.int64)) for o in outs[1:])
 
 
 @pytest.mark.parametrize("damp", [0.0, 0.3])
