@@ -412,7 +412,8 @@ def run_lsmr(args, torch, dev, rank, world, pg):
                 "data": "synthetic Frechet-shaped CSR (bench.py lsmr_matrix)",
                 "config": {"workload": "lsmr", "rows": A.m, "cols": A.n, "nonzeros": nnz, "iteration_limit": K,
                            "iterations_per_step": its_step,
-                           "damp": 0.1, "products": "libswdk k_aprod1 on A and on its device transpose",
+                           "damp": 0.1, "solver": "swdk_lsmr_solve: products of A and of its device transpose, "
+                                                  "norms and scalar recurrences on the device",
                            "l2": "inputs (1.3 GB of CSR per product) larger than L2"},
                 "clocks": clk,
                 "e2e": {"value": world / e2e_s, "unit": LSMR_UNIT, "h2d_bytes_per_step": int(A.m * 8),
@@ -420,8 +421,9 @@ def run_lsmr(args, torch, dev, rank, world, pg):
                 "gpu_launches": None,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                              "traffic": None, "bytes_per_iteration": per_it,
-                             "note": "per iteration two SpMV over the 165 M nonzeros plus host scalar recurrences "
-                                     "(three device-to-host norm reads)"},
+                             "note": "per iteration two SpMV over the 165 M nonzeros, four fixed-grid norm "
+                                     "reductions and the one-thread recurrences; the host reads the state every "
+                                     "16 iterations"},
                 "cpu_baseline": cb, "istop": info["istop"], "itn": info["itn"]}
         print(json.dumps(line), flush=True)
     if pg:

@@ -356,6 +356,31 @@ int swdk_frechet_records_device(int64_t m, int32_t m_header, int32_t n, const in
 int swdk_aprod_csr(int mode, int64_t m, int64_t n, const int64_t* d_rowptr, const int32_t* d_indices,
                    const float* d_values, double* d_x, double* d_y, void* stream);
 
+/* LSMR on the device (replaces the solve of csr_matrix::lsmr_solver,
+ * src/shared/csr_matrix.cpp, running src/shared/lsmrModule_csr.f90):
+ * min ||A x - b||^2 + damp^2 ||x||^2 by Fong & Saunders' iteration with FP64
+ * device vectors and every scalar recurrence on the device; the host reads
+ * the state back every 16 iterations.  A (m x n) and its transpose (n x m,
+ * each row a column of A with its entries in row order) are device CSR with
+ * int64 row pointers, int32 indices and FP32 values, owned by the caller and
+ * kept alive while the handle is used.  d_b (m) and d_x (n) are FP64 device
+ * vectors.  istop as in the reference module: 1 ||r|| small, 2 ||A^T r||
+ * small, 3 cond(A) above conlim, 4-6 the same at machine precision, 7 the
+ * iteration limit; 0 when b or A^T b is zero (x = 0).  Local
+ * reorthogonalization is not implemented.  The solve is the same bits on
+ * every run. */
+typedef struct swdk_lsmr swdk_lsmr;
+typedef struct swdk_lsmr_info {
+  int istop, itn;
+  double normA, condA, normr, normAr, normx;
+} swdk_lsmr_info;
+int swdk_lsmr_create(int device, int64_t m, int64_t n, const int64_t* d_rowptr, const int32_t* d_indices,
+                     const float* d_values, const int64_t* d_trowptr, const int32_t* d_tindices,
+                     const float* d_tvalues, swdk_lsmr** out);
+int swdk_lsmr_solve(swdk_lsmr* solver, const double* d_b, double* d_x, double damp, double atol, double btol,
+                    double conlim, int itnlim, swdk_lsmr_info* info, void* stream);
+void swdk_lsmr_destroy(swdk_lsmr* solver);
+
 /* Statistics of the last get_1d_kernel / get_2d_map / surfdisp96 call. */
 int swdk_get_stats(swdk_ctx* ctx, swdk_stats* out);
 

@@ -17,6 +17,7 @@ SOURCES = {
     "swdk.cu": ([], ["swdk_core.cuh", "swdk_eigen.cuh"]),
     "swdk_mlp.cu": ([], []),
     "swdk_fmst.cu": (["-fmad=false"], ["swdk_fmst_march.cuh"]),
+    "swdk_lsmr.cu": ([], []),
 }
 OUT = os.path.join(HERE, "libswdk.so")
 

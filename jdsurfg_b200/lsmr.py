@@ -4,9 +4,12 @@ The reference solves the damped least-squares system of every inversion
 iteration with LSMR (csr_matrix::lsmr_solver, src/shared/csr_matrix.cpp,
 running src/shared/lsmrModule_csr.f90 in FP32 with OpenMP matrix products).
 Here the matrix stays on the device as the CSR rows swdk_frechet_csr_device
-produced (FP32 values, int32 columns, int64 row pointers); the two products
-per iteration are libswdk's k_aprod1/k_aprod2 (swdk_aprod_csr), the vectors
-are FP64 device tensors, and the scalar recurrences run on the host.
+produced (FP32 values, int32 columns, int64 row pointers), with its
+transpose built once on the device; the vectors are FP64.  lsmr() runs the
+whole iteration in libswdk (swdk_lsmr_solve: row-kernel products of A and
+of its transpose, fixed-grid norms, the scalar recurrences in device
+memory), so the solve is the same bits on every run; lsmr_stepwise() is the
+same iteration driven step by step from the host.
 
 The iteration follows Fong & Saunders, "LSMR: An iterative algorithm for
 sparse least-squares problems", SIAM J. Sci. Comput. 33 (2011): Golub-Kahan
@@ -23,7 +26,7 @@ Local reorthogonalization (the reference's localSize) is not implemented.
 import ctypes as C
 import math
 
-from .engine import SwdkError, lib
+from .engine import SwdkError, lib, torch_stream
 
 
 class DeviceCSR:
@@ -42,6 +45,23 @@ class DeviceCSR:
         L.swdk_aprod_csr.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]
         self.t = self.transpose() if deterministic else None
+
+    def solver(self):
+        """The matrix's swdk_lsmr handle (its work vectors), created on first
+        use and kept for the matrix's lifetime."""
+        if getattr(self, "_solver", None) is None:
+            import weakref
+            L = _bind()
+            h = C.c_void_p()
+            t = self.t
+            rc = L.swdk_lsmr_create(self.rowptr.device.index, self.m, self.n, self.rowptr.data_ptr(),
+                                    self.indices.data_ptr(), self.values.data_ptr(), t.rowptr.data_ptr(),
+                                    t.indices.data_ptr(), t.values.data_ptr(), C.byref(h))
+            if rc != 0:
+                raise SwdkError(f"swdk_lsmr_create failed ({rc})")
+            self._solver = h
+            weakref.finalize(self, L.swdk_lsmr_destroy, h)
+        return self._solver
 
     def transpose(self):
         """The n x m transpose as device CSR, each row (a column of A) with its
@@ -69,10 +89,55 @@ class DeviceCSR:
             raise SwdkError(f"swdk_aprod_csr failed ({rc})")
 
 
+class _Info(C.Structure):
+    _fields_ = [("istop", C.c_int), ("itn", C.c_int), ("normA", C.c_double), ("condA", C.c_double),
+                ("normr", C.c_double), ("normAr", C.c_double), ("normx", C.c_double)]
+
+
+def _bind():
+    L = lib()
+    if not getattr(L, "_lsmr_bound", False):
+        vp = C.c_void_p
+        L.swdk_lsmr_create.argtypes = [C.c_int, C.c_int64, C.c_int64, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]
+        L.swdk_lsmr_solve.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                      C.POINTER(_Info), vp]
+        L.swdk_lsmr_destroy.argtypes = [vp]
+        L.swdk_lsmr_destroy.restype = None
+        L._lsmr_bound = True
+    return L
+
+
 def lsmr(A, b, damp=0.0, atol=1e-6, btol=1e-6, conlim=1e8, itnlim=None):
-    """Solve min ||A x - b||^2 + damp^2 ||x||^2.  A: DeviceCSR; b: FP64 device
-    tensor (m).  Returns x (device) and dict(istop, itn, normA, condA, normr,
-    normAr, normx)."""
+    """Solve min ||A x - b||^2 + damp^2 ||x||^2.  A: DeviceCSR with its
+    transpose (deterministic=True); b: FP64 device tensor (m).  The whole
+    iteration runs on the device (swdk_lsmr_solve: the scalar recurrences in
+    device memory, the host reading them every 16 iterations), on torch's
+    current stream.  Returns x (device) and dict(istop, itn, normA, condA,
+    normr, normAr, normx)."""
+    import torch
+    if A.t is None:
+        return lsmr_stepwise(A, b, damp, atol, btol, conlim, itnlim)
+    L = _bind()
+    m, n = A.m, A.n
+    itnlim = min(m, n) if itnlim is None else itnlim
+    x = torch.empty(n, dtype=torch.float64, device=b.device)
+    b = b.contiguous()
+    info = _Info()
+    st = C.c_void_p(torch_stream(b.device))
+    rc = L.swdk_lsmr_solve(A.solver(), C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), damp, atol, btol, conlim,
+                           itnlim, C.byref(info), st)
+    if rc != 0:
+        raise SwdkError(f"swdk_lsmr_solve failed ({rc})")
+    return x, dict(istop=info.istop, itn=info.itn, normA=info.normA, condA=info.condA, normr=info.normr,
+                   normAr=info.normAr, normx=info.normx)
+
+
+def lsmr_stepwise(A, b, damp=0.0, atol=1e-6, btol=1e-6, conlim=1e8, itnlim=None):
+    """The same iteration step by step from the host: the two products by
+    libswdk, the vector updates as torch operations and the scalar
+    recurrences in Python (two norm reads per iteration).  Kept as the
+    readable statement of what swdk_lsmr_solve does on the device; used
+    when A has no transpose."""
     import torch
     m, n = A.m, A.n
     dev = b.device

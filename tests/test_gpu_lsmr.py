@@ -86,3 +86,33 @@ def test_lsmr_matches_scipy(damp):
     xs = x.cpu().numpy()
     g = A.T @ (A @ xs - b) + damp ** 2 * xs
     assert np.linalg.norm(g) <= 1e-6 * np.linalg.norm(A.T @ b)
+
+
+def test_device_solve_matches_stepwise_and_is_deterministic():
+    """swdk_lsmr_solve (everything on the device) against the host-driven
+    iteration with the same formulas: the same stop, the same iteration
+    count, the solutions within 1e-10; and the same bits on a second run."""
+    import torch
+    from jdsurfg_b200.lsmr import lsmr, lsmr_stepwise
+    A, b = _problem(3000, 1400, 0.02, 8)
+    D = _device(A)
+    bd = torch.from_numpy(b).cuda()
+    x1, i1 = lsmr(D, bd, damp=0.05, atol=1e-9, btol=1e-9, itnlim=200)
+    x2, i2 = lsmr(D, bd, damp=0.05, atol=1e-9, btol=1e-9, itnlim=200)
+    xs, isw = lsmr_stepwise(D, bd, damp=0.05, atol=1e-9, btol=1e-9, itnlim=200)
+    a1, a2, as_ = x1.cpu().numpy(), x2.cpu().numpy(), xs.cpu().numpy()
+    assert np.array_equal(a1.view(np.int64), a2.view(np.int64)) and i1 == i2
+    assert i1["istop"] == isw["istop"] and abs(i1["itn"] - isw["itn"]) <= 1
+    assert np.linalg.norm(a1 - as_) <= 1e-10 * np.linalg.norm(as_)
+    assert abs(i1["normr"] - isw["normr"]) <= 1e-10 * max(1.0, isw["normr"])
+
+
+def test_device_solve_iteration_limit_and_zero_rhs():
+    import torch
+    from jdsurfg_b200.lsmr import lsmr
+    A, b = _problem(2000, 900, 0.02, 9)
+    D = _device(A)
+    x, info = lsmr(D, torch.from_numpy(b).cuda(), atol=0.0, btol=0.0, conlim=0.0, itnlim=5)
+    assert info["istop"] == 7 and info["itn"] == 5
+    x0, i0 = lsmr(D, torch.zeros(2000, dtype=torch.float64, device="cuda"))
+    assert i0["istop"] == 0 and i0["itn"] == 0 and float(x0.abs().max()) == 0.0
