@@ -287,7 +287,7 @@ def run_reference(args):
                 "ms_per_step": 1e3 * int(pairs["rcv_ptr"][-1]) / cb["value"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_survey)",
-                "config": fmst_config(s, pairs), "cpu_baseline": cb,
+                "config": dict(fmst_config(s, pairs), l2="flushed between steps (256 MiB write)"), "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": FMST_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -539,8 +539,8 @@ def run_fmst(args, torch, dev, rank, world, pg):
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py make_survey)",
-                "config": dict(fmst_config(s, pairs), l2="flushed between steps (256 MiB write)",
-                               max_band=info["max_band"], receivers_ok=ok),
+                "config": dict(fmst_config(s, pairs), l2="flushed between steps (256 MiB write)"),
+                "detail": {"max_band": info["max_band"], "receivers_ok": ok},
                 "clocks": clk,
                 "e2e": {"value": world * nrcv / e2e_s, "unit": FMST_UNIT,
                         "h2d_bytes_per_step": int(case["vs"].nbytes), "d2h_bytes_per_step": int(nrcv * 4),
@@ -966,9 +966,10 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator, jdsurfg_b200/synth.py); no public dataset exists for this path",
-                "config": dict(case_desc(args, case, kmax), timed_as="eager calls" if args.no_graph else
-                               "CUDA-graph replays of one get_1d_kernel_device call",
-                               roots_blocks_autotuned=roots_blocks), "clocks": clk, "e2e": e2e,
+                "config": case_desc(args, case, kmax),
+                "timing": {"timed_as": "eager calls" if args.no_graph else
+                           "CUDA-graph replays of one get_1d_kernel_device call",
+                           "roots_blocks_autotuned": roots_blocks}, "clocks": clk, "e2e": e2e,
                 "gpu_launches": int(acc["kernel_launches"]), "roofline": roofline, "cpu_baseline": cb,
                 "plain": plain,
                 "detail": {"secular_evals_per_step": evals / args.steps,
