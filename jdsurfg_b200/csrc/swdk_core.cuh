@@ -163,9 +163,14 @@ struct LayerView {
     const float w = (float)(2 * (m & 3) + 1);
     float ai, bi, ri;
 #ifdef __CUDA_ARCH__
-    ai = (float)__dadd_rn((double)n0.x, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.x, n0.x)), 0.125));
-    bi = (float)__dadd_rn((double)n0.y, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.y, n0.y)), 0.125));
-    ri = (float)__dadd_rn((double)n0.z, __dmul_rn((double)__fmul_rn(w, __fsub_rn(n1.z, n0.z)), 0.125));
+    // The preparation forms v0 + d/8 (d = w (v1 - v0) in REAL*4) in double
+    // and rounds it to REAL*4.  d/8 is exact in REAL*4 (a power-of-two
+    // scaling of a normal number), so that is the correctly rounded REAL*4
+    // sum of v0 and d/8, which one IEEE single-precision addition also
+    // gives: the same bits without FP64 conversions in the layer walk.
+    ai = __fadd_rn(n0.x, __fmul_rn(0.125f, __fmul_rn(w, __fsub_rn(n1.x, n0.x))));
+    bi = __fadd_rn(n0.y, __fmul_rn(0.125f, __fmul_rn(w, __fsub_rn(n1.y, n0.y))));
+    ri = __fadd_rn(n0.z, __fmul_rn(0.125f, __fmul_rn(w, __fsub_rn(n1.z, n0.z))));
 #else
     ai = (float)((double)n0.x + (double)(w * (n1.x - n0.x)) * 0.125);
     bi = (float)((double)n0.y + (double)(w * (n1.y - n0.y)) * 0.125);
@@ -669,41 +674,45 @@ enum Phase : int {
 
 struct ChainParams {
   const double* t;  // periods of the chain
-  int kmax;         // periods
-  int nmode;        // modes 1..nmode (surfdisp96 "mode")
-  int igr;          // 0 phase; >0 numerical group velocity (surfdisp96.f:241-248)
-  int iwave;        // 1 Love, 2 Rayleigh
-  int refine;       // 0 reference nevill, 1 Brent
   double rtol;      // Brent bracket tolerance (relative)
-  int sngl;         // REAL*4 output like the reference
   double cc;        // start value 0.95*0.90*c_R(slowest layer), surfdisp96.f:206-226
   float betmx;      // largest shear velocity of the flattened model
-  int retry;        // surfdisp()'s single-period retries (surfdisp.cpp:94-109): RETRY_*
+  int16_t kmax;     // periods (<= KMAX_CHAIN)
+  int16_t nmode;    // modes 1..nmode (surfdisp96 "mode")
+  int8_t igr;       // 0 phase; >0 numerical group velocity (surfdisp96.f:241-248)
+  int8_t iwave;     // 1 Love, 2 Rayleigh
+  int8_t refine;    // 0 reference nevill, 1 Brent
+  int8_t sngl;      // REAL*4 output like the reference
+  int8_t retry;     // surfdisp()'s single-period retries (surfdisp.cpp:94-109): RETRY_*
 };
 
+// The chain state, parameters and output addressing of the root kernels live
+// in shared memory (one of each per lane, 352 bytes together), which is what
+// lets five 128-thread blocks share an SM; integer fields are as narrow as
+// their ranges allow (periods <= KMAX_CHAIN, scan steps <= SCAN_CAP + 32,
+// Brent steps <= 201, Neville points <= 10).
 struct ChainState {
-  int phase, next;
   double last;    // value of the last requested secular evaluation
   double creq;    // requested phase velocity
   double omega;   // 2 pi / t1 of the current root
   // surfdisp96 locals
-  int iq, k, ift, ierr;
   double t1;
-  float t1a, t1b;
   double c1, c2, clow, cm, del1, del2, del1st;
-  int ifirst, idir, gpass;
   // refinement
   double c3, del3, ra_, fa, rb_, fb, rc_, fc, rd, re;
-  int nev, nctrl, m;
-  int nscan;
   // learned proposals
   double plo, phi, fplo, c1s, del1s;
-  int pm, nprop_ok, nprop_fail;
   // retries
-  int sub, rq_m, rq_k, sub_ierr;
   double sub_out;
-  int iterlim;
-  long long nevals;
+  float t1a, t1b;
+  int nevals;
+  int16_t phase, next;
+  int16_t iq, k, ift;
+  int16_t nctrl, nscan;
+  int16_t pm, nprop_ok, nprop_fail;
+  int16_t rq_m, rq_k, iterlim;
+  int8_t ierr, ifirst, idir, gpass;
+  int8_t nev, m, sub;
 };
 
 // Output callback: slot (mode iq, period k) gets value v; the caller owns
