@@ -576,12 +576,11 @@ struct RayScratch {
   double seg[RAY_SEG][6];  // the segment being consumed: cd[5], exponent sum
 };
 
-// one step of the up pass (sregn96.f90:401-489): the compound vector cd of
-// layer m from that of layer m+1 (cp, in place), with its exponent sum
-SWDK_HD void ray_up_step(const RayLayer& y, const SlotK& s, double* cd, double& exr, int& exi) {
-  const int iw = (y.zb > 0.0) ? 0 : 1;
-  LVars v;
-  vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
+// one step of the up pass (sregn96.f90:401-489) after vars_lean of its
+// layer: the compound vector cd of layer m from that of layer m+1 (in
+// place), with its exponent sum
+SWDK_HD void ray_up_apply(const LVars& v, const RayLayer& y, int iw, const SlotK& s, double* cd, double& exr,
+                          int& exi) {
   double ee[5];
   dnka_apply(v, y, iw, s, cd, ee);
   double t1 = 0.0;
@@ -605,12 +604,22 @@ SWDK_HD void ray_keep(double* dst, const double* cd, double exr, int exi) {
 // column's layer records lay[0..L-1] (top-down, lay[L-1] the half-space),
 // depth-truncated by pass_layers.  Returns ugr (flat) and norm = ugr*sumi0;
 // the raw layer kernels go to the sink as the top-down sweep produces them.
+//
+// One loop runs the up pass (layers L-2 .. 0, keeping checkpoints), then
+// the top-down sweep (layers 0 .. L-1), which at the first layer of each
+// segment recomputes the segment's compound vectors from its checkpoint by
+// further up steps.  Every step evaluates its layer's variables (vars_lean:
+// square roots, exponentials or sines and cosines) at one place in the
+// code, so the kernel holds one copy of that code instead of three (the
+// Rayleigh eigen kernel waited on instruction fetch about as often as on
+// its FP64 results).  The steps and their arithmetic are those of separate
+// up, recompute and down loops.
 template <class Sink>
 SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double wvno, RayScratch& scr, double& ugr,
                             double& norm, const Sink& sink, double trunc_q = EIG_TRUNC_Q) {
   const SlotK s = slot_consts(omega, wvno);
   const int L = pass_layers(lay, Lfull, s.k2, s.om2, trunc_q);
-  // ---- up (sregn96.f90:401-489), checkpoints only ----
+  // ---- up (sregn96.f90:401-489) start: the half-space ----
   double cd[6];
   {
     const RayLayer& y = lay[L - 1];
@@ -621,48 +630,68 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
   int exi = 0;
   ray_keep(scr.hs, cd, exr, exi);
   if ((L - 1) % RAY_SEG == 0) ray_keep(scr.ck[(L - 1) / RAY_SEG], cd, exr, exi);
-#pragma unroll 1  // a layer recursion: unrolling only grows the code
-  for (int m = L - 2; m >= 0; --m) {
-    ray_up_step(lay[m], s, cd, exr, exi);
-    if (m % RAY_SEG == 0) ray_keep(scr.ck[m / RAY_SEG], cd, exr, exi);
-  }
-  // ---- down + svfunc + energy, top-down ----
-  sink.start();
-  const double* top = scr.ck[0];  // layer 0
-  const double if1213 = -1.0 / top[1];
-  const double exe0 = top[5];
-  Eig4 u0;
-  u0.ur = top[2] / top[1];
-  u0.uz = 1.0; u0.tz = 0.0; u0.tr = 0.0;
-  if (lay[0].zb <= 0.0) { u0.ur = 0.0; u0.tr = 0.0; }  // fluid top (jwat)
+  // ---- down + svfunc + energy state ----
+  double if1213 = 0.0, exe0 = 0.0;
+  Eig4 u0 = {0.0, 0.0, 0.0, 0.0};
   double vv[4] = {1.0, 0.0, 0.0, 0.0};
   double dxr = 0.0;
   int dxi = 0;
   EnergyAcc acc = {0.0, 0.0, 0.0, 0.0};
   const double c = omega * s.ik;
+  int up = L - 2;        // layer of the next up-pass step (< 0: the up pass is done)
+  int dn = 0;            // layer of the next down step
+  int sl = -1, sj0 = -1;  // segment recomputation: its next layer sl while sl > sj0
+  bool down = false;
+  auto begin_down = [&]() {
+    sink.start();
+    const double* top = scr.ck[0];  // layer 0
+    if1213 = -1.0 / top[1];
+    exe0 = top[5];
+    u0.ur = top[2] / top[1];
+    u0.uz = 1.0; u0.tz = 0.0; u0.tr = 0.0;
+    if (lay[0].zb <= 0.0) { u0.ur = 0.0; u0.tr = 0.0; }  // fluid top (jwat)
+    down = true;
+  };
+  if (up < 0) begin_down();
 #pragma unroll 1  // a layer recursion: unrolling only grows the code
-  for (int m = 0; m < L; ++m) {
-    const int j0 = m - m % RAY_SEG;  // first layer of m's segment
-    if (m == j0 && m < L - 1) {
-      // cd of layers j0+1 .. t from the checkpoint at t
-      const int t = (j0 + RAY_SEG < L - 1) ? j0 + RAY_SEG : L - 1;
-      const double* src = (t == L - 1) ? scr.hs : scr.ck[t / RAY_SEG];
-      double w[6];
-      for (int i = 0; i < 6; ++i) w[i] = src[i];
-      double rexr = src[6];
-      int rexi = (int)src[7];
-      for (int i = 0; i < 6; ++i) scr.seg[t - j0 - 1][i] = w[i];
-#pragma unroll 1
-      for (int l = t - 1; l > j0; --l) {
-        ray_up_step(lay[l], s, w, rexr, rexi);
-        for (int i = 0; i < 6; ++i) scr.seg[l - j0 - 1][i] = w[i];
+  for (;;) {
+    int lm;
+    bool upstep;
+    if (!down) {
+      lm = up;
+      upstep = true;
+    } else {
+      const int j0 = dn - dn % RAY_SEG;  // first layer of dn's segment
+      if (sl <= sj0 && dn == j0 && dn < L - 1 && sj0 != j0) {
+        // cd of layers j0+1 .. t from the checkpoint at t
+        const int t = (j0 + RAY_SEG < L - 1) ? j0 + RAY_SEG : L - 1;
+        const double* src = (t == L - 1) ? scr.hs : scr.ck[t / RAY_SEG];
+        for (int i = 0; i < 6; ++i) cd[i] = src[i];
+        exr = src[6];
+        exi = (int)src[7];
+        for (int i = 0; i < 6; ++i) scr.seg[t - j0 - 1][i] = cd[i];
+        sj0 = j0;
+        sl = t - 1;
       }
+      upstep = sl > sj0;
+      lm = upstep ? sl : dn;
     }
-    const RayLayer& y = lay[m];
+    const RayLayer& y = lay[lm];
     const int iw = (y.zb > 0.0) ? 0 : 1;
-    const bool half = (m == L - 1);
     LVars v;
     vars_lean(s.k2 - s.om2 * y.ia2, s.k2 - s.om2 * y.ib2, y.d, iw, v);
+    if (upstep) {
+      ray_up_apply(v, y, iw, s, cd, exr, exi);
+      if (!down) {
+        if (up % RAY_SEG == 0) ray_keep(scr.ck[up / RAY_SEG], cd, exr, exi);
+        if (--up < 0) begin_down();
+      } else {
+        for (int i = 0; i < 6; ++i) scr.seg[sl - sj0 - 1][i] = cd[i];
+        --sl;
+      }
+      continue;
+    }
+    const bool half = (dn == L - 1);
     Eig4 u1 = u0;
     if (!half) {
       double a0[4];
@@ -675,13 +704,14 @@ SWDK_HDI void rayleigh_pass(const RayLayer* lay, int Lfull, double omega, double
       dxr = dxr + v.pex;
       dxi += e;
       const double exa1 = dxr + (double)dxi * LN2;
-      const double* cd1 = scr.seg[m - j0];  // layer m + 1
+      const double* cd1 = scr.seg[dn - (dn - dn % RAY_SEG)];  // layer dn + 1
       u1 = eigen_at(cd1, vv, exa1 + cd1[5] - exe0, if1213);
     }
     double da, db, dr;
     energy_lean(y, v, iw, half, u0, u1, s, c, acc, da, db, dr);
-    sink.add(m, y.vtp, y.rtp, da, db, dr);
+    sink.add(dn, y.vtp, y.rtp, da, db, dr);
     u0 = u1;
+    if (++dn >= L) break;
   }
   sink.finish();
   ugr = (wvno * acc.sumi1 + acc.sumi2) / (omega * acc.sumi0);
