@@ -571,7 +571,7 @@ constexpr size_t ROOTS_SMEM = 128 * (sizeof(ChainState) + sizeof(ChainParams) + 
 #define SWDK_ROOTS_MINB 4  // 127 registers, no spill (shared memory allows 4 blocks too); 3 blocks measured slower
 #endif
 #ifndef SWDK_RETRY_MINB
-#define SWDK_RETRY_MINB 2  // retries: no spill; one record per warp, fewer records than resident warps
+#define SWDK_RETRY_MINB 3  // retries, one record per warp: 168 registers (48 B of spill loads); 2 blocks (202 registers) measured 8 ms per step slower, 4 (128 registers, more spill) the same as 3
 #endif
 #ifndef SWDK_EIGEN_MINB
 #define SWDK_EIGEN_MINB 3  // Rayleigh passes: 168 registers, no spill (2: 183, 3: 171, 4: 180, 5: 227 ms of eigen per step)
@@ -917,7 +917,7 @@ __device__ __forceinline__ double flat2sphere(double t, double c, int love, int 
 // one block's work: column col of a model with ncol columns (its arrays
 // passed at the model's offsets)
 template <int WT, int PATH>
-__device__ __forceinline__ void eigen_column(int col, int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
+__device__ __noinline__ void eigen_column(int col, int ncol, int nz, int Lmax, const float4* __restrict__ lay0,
                                              const ColInfo* __restrict__ info, const float2* __restrict__ chainrule,
                                              const SlotDesc* __restrict__ slots, int g0, int gn,
                                              const double* __restrict__ croot, const int32_t* __restrict__ cstat,
