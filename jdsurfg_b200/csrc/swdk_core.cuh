@@ -669,7 +669,7 @@ enum Phase : int {
   PH_CHAIN_START, PH_PERIOD_START, PH_GS_START, PH_GS_FIRST, PH_SCAN, PH_SCAN_GOT, PH_REFINE_START,
   PH_NEV_A, PH_NEV_TOP, PH_NEV_BODY_GOT, PH_NEV_BODY, PH_NEV_HALF_GOT, PH_NEV_NEV_GOT, PH_BRENT_STEP,
   PH_BRENT_GOT, PH_REFINE_DONE, PH_GS_OK, PH_GS_FAIL, PH_PERIOD_OUT, PH_FAIL, PH_MODE_END, PH_CHAIN_END,
-  PH_RETRY_NEXT, PH_PROP_LO, PH_PROP_HI, PH_PROP_CHECK, PH_PROP_DOWN, PH_PROP_DOWN_GOT, PH_PROP_C1_GOT, PH_DONE
+  PH_RETRY_NEXT, PH_PROP_LO, PH_PROP_HI, PH_PROP_CHECK, PH_PROP_DOWN, PH_PROP_DOWN_GOT, PH_PROP_C1_GOT, PH_FIRST_NEXT, PH_FIRST_GOT, PH_DONE
 };
 
 struct ChainParams {
@@ -710,6 +710,7 @@ struct ChainState {
   int16_t iq, k, ift;
   int16_t nctrl, nscan;
   int16_t pm, nprop_ok, nprop_fail;
+  int16_t pj;  // first-period proposal: grid index of the last coarse point checked
   int16_t rq_m, rq_k, iterlim;
   int8_t ierr, ifirst, idir, gpass;
   int8_t nev, m, sub;
@@ -796,6 +797,34 @@ SWDK_HD bool proposal_cell(const ChainState& s, const ChainParams& P, const Chai
   return s.c1 + (double)(m + 1) * DC < (double)P.betmx + DC;
 }
 
+// The first period of a Rayleigh chain's first mode scans from cc, on
+// average about 90 grid steps below the root.  There the proposal is the
+// network's absolute estimate c* (no previous root to anchor it), and the
+// stretch [c1, g_m] below its cell is checked at every FIRST_STRIDE-th grid
+// point instead of being skipped: each checked point must keep the
+// polarity of f(c1); the first that does not ends the check, and the
+// reference's scan resumes one grid step at a time from the checked point
+// below it, so it reaches the first sign change of the plain scan.  This
+// holds unless the first two roots lie inside one coarse interval (and the
+// estimate lies above both): the fundamental and first higher Rayleigh
+// modes are at least 0.05 km/s apart at 1-2 s on the default and 0.2 km/s
+// on the production grid, above the coarse interval of 0.02 km/s.  Love
+// chains keep the plain scan: their first two modes come as close as
+// 0.001 km/s at short periods.
+constexpr int FIRST_STRIDE = 4;
+
+SWDK_HD bool first_cell(const ChainState& s, const ChainParams& P, const ChainIO& io, int& m) {
+  if (!io.prop || s.sub || P.igr > 0 || P.refine != 1 || P.iwave != 2 || s.k != 1 || s.iq != 1 || s.gpass != 0 ||
+      s.ifirst != 1 || s.del1st == 0.0)
+    return false;
+  const float2 pr = io.prop[0];  // (mode 1, period 1)
+  if (!(pr.y > 0.0f) || !(pr.y <= 0.25f)) return false;
+  const double x = ((double)pr.x - s.c1) / DC;
+  if (!(x >= 4.0 * FIRST_STRIDE) || !(x < 1.0e4)) return false;
+  m = (int)floor(x);
+  return s.c1 + (double)(m + 1) * DC < (double)P.betmx + DC;
+}
+
 // grid point c1 + j*dc, accumulated like the scan does
 SWDK_HD double scan_grid(double c1, int j) {
   double c = c1;
@@ -858,6 +887,7 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
           s.clow = s.cm;
         }
         s.gpass = 0;
+        s.pj = -1;  // the first-period jump is tried once per period (a fallback rescans from c1)
         s.phase = PH_GS_START;
         int m;
         if (proposal_cell(s, P, io, m)) {
@@ -947,6 +977,50 @@ SWDK_HDI bool chain_advance(ChainState& s, const ChainParams& P, const ChainIO& 
         if (s.ifirst == 1) s.idir = 1;
         else if (plmn >= 0.0) s.idir = 1;
         else s.idir = -1;
+        s.phase = PH_SCAN;
+        int m;
+        if (s.pj == -1 && first_cell(s, P, io, m)) {  // the first period: checked jump to the learned cell
+          s.c1s = s.c1;
+          s.del1s = s.del1st;
+          s.pm = m;
+          s.pj = 0;
+          s.plo = s.c1;
+          s.fplo = s.del1;
+          s.phase = PH_FIRST_NEXT;
+        }
+        break;
+      }
+      case PH_FIRST_NEXT: {  // next coarse point below the cell, or the cell
+        if (s.pj + FIRST_STRIDE < s.pm) {
+          double c = s.plo;
+          for (int i = 0; i < FIRST_STRIDE; ++i) c = c + DC;
+          s.phi = c;
+          SWDK_REQ(c, PH_FIRST_GOT);
+        }
+        // every checked point kept the polarity: the cell [g_m, g_m+1]
+        double c = s.plo;
+        for (int i = s.pj; i < s.pm; ++i) c = c + DC;
+        s.plo = c;
+        s.phi = c + DC;
+        s.idir = 1;
+        s.nscan = s.pm;
+        s.phase = PH_PROP_LO;
+        break;
+      }
+      case PH_FIRST_GOT: {
+        if (dsign1(s.last) == dsign1(s.del1s)) {
+          s.plo = s.phi;
+          s.fplo = s.last;
+          s.pj = s.pj + FIRST_STRIDE;
+          s.phase = PH_FIRST_NEXT;
+          break;
+        }
+        // a sign change in (plo, phi]: the reference's scan from plo
+        s.nprop_fail++;
+        s.c1 = s.plo;
+        s.del1 = s.fplo;
+        s.idir = 1;
+        s.nscan = s.pj;
         s.phase = PH_SCAN;
         break;
       }
@@ -1196,6 +1270,7 @@ SWDK_HD int eval_phase(const ChainState& s) {
     case PH_SCAN_GOT: return (s.k == 1 && s.gpass == 0) ? EV_SCAN_FIRST : EV_SCAN;
     case PH_PROP_HI:
     case PH_PROP_CHECK: return EV_CELL;
+    case PH_FIRST_GOT: return EV_SCAN_FIRST;
     case PH_PROP_DOWN_GOT:
     case PH_PROP_C1_GOT: return EV_WALK;
     default: return EV_REFINE;
