@@ -351,52 +351,66 @@ __global__ void k_depth_table(int nz, const float* __restrict__ depth, int spher
 }
 
 // ---------------------------------------------------------------------------
-// proposal-network rows: row = slot * ncol + col; one warp per row, a lane
-// writes 8 consecutive columns (16 bytes)
+// proposal-network rows: row = slot * ncol + col; a half-warp per row:
+// lane h < 8 loads nodes 8h .. 8h+7 once and writes their four components
+// (four 16-byte chunks of 8 columns), lanes 8 .. 15 write the period
+// features and the zero padding
 //   x[0:64) vs, [64:128) vp, [128:192) rho, [192:256) thickness,
 //   x[256] log(T)/log(100), x[257] (mode-1)/2, zero to 320
 // tiled = 0: row-major (n, 320); tiled = 1: the 128-row tile images
 // swdk_mlp_propose reads (128-byte swizzled K-major, 81920 bytes per tile)
 // ---------------------------------------------------------------------------
+static_assert(FEAT_NODES == 64 && FEAT_DIM == 320, "k_features packs 64 nodes x 4 components + 64 columns");
+__device__ __forceinline__ void feat_store(__nv_bfloat16* x, int tiled, int w, int c0, const float* v, bool inr) {
+  uint32_t pk[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const __nv_bfloat162 b2 = __floats2bfloat162_rn(inr ? v[2 * e] : 0.0f, inr ? v[2 * e + 1] : 0.0f);
+    pk[e] = *reinterpret_cast<const uint32_t*>(&b2);
+  }
+  uint8_t* dst;
+  if (tiled) {
+    const int t = w >> 7, r = w & 127, kb = c0 >> 6, j = (c0 & 63) >> 3;
+    dst = reinterpret_cast<uint8_t*>(x) + (size_t)t * (128 * FEAT_DIM * 2) + kb * (128 * 128) + r * 128 +
+          ((j ^ (r & 7)) << 4);
+  } else {
+    dst = reinterpret_cast<uint8_t*>(x + (size_t)w * FEAT_DIM + c0);
+  }
+  *reinterpret_cast<uint4*>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+}
+
 __global__ void k_features(int64_t row0, int nrows, int ncol, int64_t rowmax, const float4* __restrict__ slotfeat,
                            const float4* __restrict__ nodefeat, const int64_t* __restrict__ rowlist,
                            __nv_bfloat16* __restrict__ x, int tiled) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), h = threadIdx.x & 15;
   if (w >= nrows) return;
   const int64_t row = rowlist ? rowlist[w] : row0 + w;
   const bool inr = row >= 0 && row < rowmax;
   const int s = inr ? (int)(row / ncol) : 0, col = inr ? (int)(row % ncol) : 0;
-  const float4 sf = slotfeat[s];
-  const float4* nf = nodefeat + (size_t)col * FEAT_NODES;
-  for (int q = lane; q < FEAT_DIM / 8; q += 32) {
-    float v[8];
-    const int c0 = q * 8;
-    if (c0 < 4 * FEAT_NODES) {
-      const int comp = c0 / FEAT_NODES, n0 = c0 % FEAT_NODES;
+  float v[8];
+  if (h < 8) {
+    const float4* nf = nodefeat + (size_t)col * FEAT_NODES + 8 * h;
+    float4 n[8];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const float4 n = nf[n0 + e];
-        v[e] = comp == 0 ? n.x : comp == 1 ? n.y : comp == 2 ? n.z : n.w;
-      }
-    } else {
+    for (int e = 0; e < 8; ++e) n[e] = nf[e];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) v[e] = (c0 + e == 256) ? sf.x : (c0 + e == 257) ? sf.y : 0.0f;
-    }
-    uint32_t pk[4];
+    for (int e = 0; e < 8; ++e) v[e] = n[e].x;
+    feat_store(x, tiled, w, 8 * h, v, inr);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const __nv_bfloat162 b2 = __floats2bfloat162_rn(inr ? v[2 * e] : 0.0f, inr ? v[2 * e + 1] : 0.0f);
-      pk[e] = *reinterpret_cast<const uint32_t*>(&b2);
-    }
-    uint8_t* dst;
-    if (tiled) {
-      const int t = w >> 7, r = w & 127, kb = c0 >> 6, j = (c0 & 63) >> 3;
-      dst = reinterpret_cast<uint8_t*>(x) + (size_t)t * (128 * FEAT_DIM * 2) + kb * (128 * 128) + r * 128 +
-            ((j ^ (r & 7)) << 4);
-    } else {
-      dst = reinterpret_cast<uint8_t*>(x + (size_t)w * FEAT_DIM + c0);
-    }
-    *reinterpret_cast<uint4*>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    for (int e = 0; e < 8; ++e) v[e] = n[e].y;
+    feat_store(x, tiled, w, FEAT_NODES + 8 * h, v, inr);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = n[e].z;
+    feat_store(x, tiled, w, 2 * FEAT_NODES + 8 * h, v, inr);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = n[e].w;
+    feat_store(x, tiled, w, 3 * FEAT_NODES + 8 * h, v, inr);
+  } else {
+    const float4 sf = slotfeat[s];
+    const int c0 = 4 * FEAT_NODES + 8 * (h - 8);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = (c0 + e == 256) ? sf.x : (c0 + e == 257) ? sf.y : 0.0f;
+    feat_store(x, tiled, w, c0, v, inr);
   }
 }
 
@@ -1517,7 +1531,7 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st, const
     for (int64_t a = r0; a < r1; a += PROP_CHUNK) {
       const int n = (int)std::min<int64_t>(PROP_CHUNK, r1 - a);
       ctx->launches += 2;
-      k_features<<<(n + 7) / 8, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(), nodefeat, nullptr,
+      k_features<<<(n + 15) / 16, 256, 0, st>>>(a, n, ncol, nrows, P.d_rootfeat.as<float4>(), nodefeat, nullptr,
                                               ctx->pfeat.as<__nv_bfloat16>(), 1);
       CK(cudaGetLastError());
       int r = swdk_mlp_propose(ctx->net[w], ctx->pfeat.p, n, ctx->kappa[w], prop + a, st);
@@ -2243,7 +2257,7 @@ int swdk_training_rows(swdk_ctx* ctx, const int64_t* d_rows, int n, void* d_x, f
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
   const Plan& P = ctx->plan[0];
   const int64_t rowmax = (int64_t)P.nroot * ctx->last_ncol;
-  k_features<<<(n + 7) / 8, 256, 0, st>>>(0, n, ctx->last_ncol, rowmax, P.d_rootfeat.as<float4>(),
+  k_features<<<(n + 15) / 16, 256, 0, st>>>(0, n, ctx->last_ncol, rowmax, P.d_rootfeat.as<float4>(),
                                           ctx->nodefeat.as<float4>(), d_rows, (__nv_bfloat16*)d_x, 0);
   CK(cudaGetLastError());
   if (d_y) {
