@@ -257,10 +257,21 @@ int swdk_gemm_bf16_tn(int M, int N, int K, const void* d_a, const void* d_b, flo
 /* Attach proposal networks (either may be NULL); kappa_* scales the
  * predicted sigma into the bracket half-width of that wave type.  From the
  * second period of a mode on, the bracket is centred on the previous
- * period's root plus the predicted change, c(k-1) + mu(k) - mu(k-1); the
- * first period keeps the plain scan.  NULL/NULL disables proposals.  The
- * networks must outlive their use by this context. */
+ * period's root plus the predicted change, c(k-1) + mu(k) - mu(k-1).  The
+ * first period of a Rayleigh chain's first mode jumps to the cell of the
+ * network's own estimate, the stretch below it checked at every fourth
+ * point of the scan grid; the first period of Love chains and of higher
+ * modes keeps the plain scan.  NULL/NULL disables proposals.  The networks
+ * must outlive their use by this context. */
 int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double kappa_rayleigh, double kappa_love);
+
+/* Testing aid (no counterpart in the reference): every proposed phase
+ * velocity is moved by shift_km_s (|shift| <= 10) before the search; 0, the
+ * default, leaves the network's proposals as they are.  A constant shift
+ * leaves the anchored brackets of later periods unchanged and moves only
+ * the first-period jump, whose roots must not move.  Drops a captured
+ * graph. */
+int swdk_set_proposal_shift(swdk_ctx* ctx, double shift_km_s);
 
 /* Training support: root search only (all root chains of get_1d_kernel)
  * on device models, then per-slot metadata, the roots and their status, and

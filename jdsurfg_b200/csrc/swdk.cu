@@ -414,6 +414,13 @@ __global__ void k_features(int64_t row0, int nrows, int ncol, int64_t rowmax, co
   }
 }
 
+// swdk_set_proposal_shift: every proposed phase velocity (rows with a
+// bracket, half-width > 0) moved by shift km/s
+__global__ void k_shift_prop(int n, float2* __restrict__ prop, float shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && prop[i].y > 0.0f) prop[i].x += shift;
+}
+
 // training targets of chosen rows: y = c_flat - FEAT_C0
 __global__ void k_targets(int n, int64_t rowmax, const int64_t* __restrict__ rows, const double* __restrict__ croot,
                           float* __restrict__ y) {
@@ -1330,6 +1337,7 @@ struct swdk_ctx {
   // learned bracket proposals
   swdk_mlp* net[2] = {nullptr, nullptr};  // 0: Rayleigh, 1: Love
   double kappa[2] = {4.0, 4.0};
+  double prop_shift = 0.0;  // swdk_set_proposal_shift (testing aid)
   DevBuf nodefeat, pfeat, prop;
   DevBuf retry_list, retry_ctr;  // deferred retries: records and {count, queue}
   int last_ncol = 0, last_path = -1;
@@ -1536,6 +1544,11 @@ int run_proposals(swdk_ctx* ctx, const Plan& P, int ncol, cudaStream_t st, const
       CK(cudaGetLastError());
       int r = swdk_mlp_propose(ctx->net[w], ctx->pfeat.p, n, ctx->kappa[w], prop + a, st);
       if (r) return fail(ctx, r, std::string("proposal inference: ") + swdk_mlp_last_error(ctx->net[w]));
+      if (ctx->prop_shift != 0.0) {
+        ctx->launches += 1;
+        k_shift_prop<<<(n + 255) / 256, 256, 0, st>>>(n, prop + a, (float)ctx->prop_shift);
+        CK(cudaGetLastError());
+      }
     }
   }
   return SWDK_OK;
@@ -1819,6 +1832,7 @@ int ensure_kids(swdk_ctx* ctx) {
     k->net[1] = ctx->net[1];
     k->kappa[0] = ctx->kappa[0];
     k->kappa[1] = ctx->kappa[1];
+    k->prop_shift = ctx->prop_shift;
     ctx->kids[i] = k;
     CK(cudaEventCreateWithFlags(&ctx->evjoin[i], cudaEventDisableTiming));
   }
@@ -2211,6 +2225,14 @@ int swdk_set_proposal(swdk_ctx* ctx, swdk_mlp* rayleigh, swdk_mlp* love, double 
   ctx->net[1] = love;
   ctx->kappa[0] = kappa_rayleigh;
   ctx->kappa[1] = kappa_love;
+  return SWDK_OK;
+}
+
+int swdk_set_proposal_shift(swdk_ctx* ctx, double shift_km_s) {
+  if (!ctx || !(fabs(shift_km_s) <= 10.0)) return fail(ctx, SWDK_E_ARG, "bad arguments");
+  drop_graph(ctx);
+  drop_kids(ctx);
+  ctx->prop_shift = shift_km_s;
   return SWDK_OK;
 }
 

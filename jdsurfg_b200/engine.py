@@ -84,6 +84,7 @@ def lib():
                                                vp, vp, vp]
         L.swdk_get_stats.argtypes = [vp, C.POINTER(Stats)]
         L.swdk_set_proposal.argtypes = [vp, vp, vp, C.c_double, C.c_double]
+        L.swdk_set_proposal_shift.argtypes = [vp, C.c_double]
         L.swdk_roots_device.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
         L.swdk_root_slots.argtypes = [vp, C.POINTER(C.c_int), vp, vp, vp]
         L.swdk_last_roots.argtypes = [vp, vp, vp]
@@ -266,6 +267,11 @@ class Engine:
         hr = rayleigh._h if rayleigh is not None else None
         hl = love._h if love is not None else None
         self._check(lib().swdk_set_proposal(self._h, hr, hl, kappa_rayleigh, kappa_love), "swdk_set_proposal")
+
+    def set_proposal_shift(self, shift_km_s):
+        """Testing aid: move every proposed phase velocity by shift_km_s
+        (only the first period's jump moves; the roots must not)."""
+        self._check(lib().swdk_set_proposal_shift(self._h, float(shift_km_s)), "swdk_set_proposal_shift")
 
     def roots_device(self, nx, ny, nz, vs, vp=None, rho=None, stream=None):
         """Root search of every get_1d_kernel root slot on device models."""

@@ -88,3 +88,32 @@ def test_training_rows_and_targets():
     # out-of-range rows give zero features and targets
     assert np.all(xr[4:] == 0.0) and np.all(yr[4:] == 0.0)
     eng.close()
+
+
+@pytest.mark.parametrize("shift", [0.15, -0.15, 0.03, -0.6])
+def test_shifted_first_period_proposals_keep_the_roots(shift):
+    """A constant shift of every proposed phase velocity leaves the anchored
+    brackets of later periods (c(k-1) + mu(k) - mu(k-1)) as they are and
+    moves only the first period's jump: above the root, a checked point
+    finds the sign change and the scan resumes from the checked point below
+    it; below the root, the scan goes on up from the cell.  The roots, and
+    so status, U and kernels, stay the plain scan's bits."""
+    case = synth.subset_columns(synth.make_config("large", seed=2024), np.arange(1024))
+    plain, _ = _run(case)
+    base, sb = _run(case, nets_dir=learn.WEIGHTS)
+    eng = Engine(device=0, refine="tight")
+    keep = learn.load_proposals(eng, learn.WEIGHTS)
+    eng.set_proposal_shift(shift)
+    eng.setup(case)
+    out = eng.get_1d_kernel(case["vs"], case["vp"], case["rho"], nx=case["nx"], ny=case["ny"])
+    st = eng.stats()
+    eng.close()
+    del keep
+    for k in ("vc", "vout", "status", "kernel"):
+        np.testing.assert_array_equal(out[k], plain[k], err_msg=k)
+    # the shift did move the first-period search
+    print(f"shift {shift:+.2f} km/s: secular evaluations {sb['secular_evals']} -> {st['secular_evals']}, "
+          f"proposals fell back {sb['proposals_rejected']} -> {st['proposals_rejected']}")
+    assert st["secular_evals"] != sb["secular_evals"]
+    if shift >= 0.15:
+        assert st["proposals_rejected"] > sb["proposals_rejected"]
