@@ -1318,7 +1318,8 @@ int nt_of(const double* col, int ntmax) {
 #define SWDK_HOST_CHUNKS 16
 #endif
 // eigen chunks of a host-memory call (e2e on the default workload: 4 chunks
-// 14.9, 8 chunks 15.25, 16 chunks 15.33 M slots/s; device time 15.4)
+// 14.9, 8 chunks 15.25, 16 chunks 15.33 M slots/s with device time 15.4;
+// with the faster eigen stage 16 chunks 17.29, 32 chunks 16.72 M slots/s)
 constexpr int HOST_CHUNKS = SWDK_HOST_CHUNKS;
 
 struct swdk_ctx {
