@@ -1354,6 +1354,10 @@ struct swdk_ctx {
   // one event per chunk plus one for the end of the copies
   cudaStream_t cstream = nullptr;
   cudaEvent_t evchunk[HOST_CHUNKS + 1] = {};
+  // host-memory calls: two streams the eigen chunks alternate on, and
+  // their fork/join events
+  cudaStream_t estream[2] = {};
+  cudaEvent_t evefork = nullptr, evejoin[2] = {};
   // CUDA graph of one call (swdk_graph_capture / swdk_graph_launch)
   bool capturing = false;
   cudaGraph_t graph = nullptr;
@@ -1677,6 +1681,11 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       if (!ctx->cstream) CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
       for (int i = 0; i <= HOST_CHUNKS; ++i)
         if (!ctx->evchunk[i]) CK(cudaEventCreateWithFlags(&ctx->evchunk[i], cudaEventDisableTiming));
+      for (int i = 0; i < 2; ++i) {
+        if (!ctx->estream[i]) CK(cudaStreamCreateWithFlags(&ctx->estream[i], cudaStreamNonBlocking));
+        if (!ctx->evejoin[i]) CK(cudaEventCreateWithFlags(&ctx->evejoin[i], cudaEventDisableTiming));
+      }
+      if (!ctx->evefork) CK(cudaEventCreateWithFlags(&ctx->evefork, cudaEventDisableTiming));
       const int kmax = P.kmax;
       auto chunk = [&](int h, int& a, int& b) {
         a = (int)((long long)ncol * h / HOST_CHUNKS);
@@ -1684,14 +1693,23 @@ int run_device(swdk_ctx* ctx, int path, int nx, int ny, int nz, const float* d_v
       };
       // every chunk is queued before the first copy is issued: a copy to
       // pageable host memory returns only when done, and the chunks behind
-      // it must already be on the device by then
+      // it must already be on the device by then.  The chunks alternate
+      // between two streams, so one chunk's blocks fill the SMs that the
+      // other's last wave leaves idle (the outputs are disjoint columns).
+      CK(cudaEventRecord(ctx->evefork, st));
+      for (int i = 0; i < 2; ++i) CK(cudaStreamWaitEvent(ctx->estream[i], ctx->evefork, 0));
       for (int h = 0; h < HOST_CHUNKS; ++h) {
         int a, b;
         chunk(h, a, b);
         if (b <= a) continue;
-        r = launch_eigen(ctx, P, path, ncol, nz, a, b, d_vc, d_vout, d_kernel, d_status, ldo, st);
+        cudaStream_t es = ctx->estream[h & 1];
+        r = launch_eigen(ctx, P, path, ncol, nz, a, b, d_vc, d_vout, d_kernel, d_status, ldo, es);
         if (r) return r;
-        CK(cudaEventRecord(ctx->evchunk[h], st));
+        CK(cudaEventRecord(ctx->evchunk[h], es));
+      }
+      for (int i = 0; i < 2; ++i) {
+        CK(cudaEventRecord(ctx->evejoin[i], ctx->estream[i]));
+        CK(cudaStreamWaitEvent(st, ctx->evejoin[i], 0));
       }
       for (int h = 0; h < HOST_CHUNKS; ++h) {
         int a, b;
@@ -2035,6 +2053,14 @@ void swdk_destroy(swdk_ctx* ctx) {
     cudaStreamSynchronize(ctx->cstream);
     cudaStreamDestroy(ctx->cstream);
   }
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->estream[i]) {
+      cudaStreamSynchronize(ctx->estream[i]);
+      cudaStreamDestroy(ctx->estream[i]);
+    }
+    if (ctx->evejoin[i]) cudaEventDestroy(ctx->evejoin[i]);
+  }
+  if (ctx->evefork) cudaEventDestroy(ctx->evefork);
   if (ctx->h_nevals) cudaFreeHost(ctx->h_nevals);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
