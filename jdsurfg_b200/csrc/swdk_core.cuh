@@ -687,10 +687,10 @@ struct ChainParams {
 };
 
 // The chain state, parameters and output addressing of the root kernels live
-// in shared memory (one of each per lane, 352 bytes together), which is what
-// lets five 128-thread blocks share an SM; integer fields are as narrow as
-// their ranges allow (periods <= KMAX_CHAIN, scan steps <= SCAN_CAP + 32,
-// Brent steps <= 201, Neville points <= 10).
+// in shared memory (one of each per lane, 352 bytes together, 45 KB per
+// 128-thread block); integer fields are as narrow as their ranges allow
+// (periods <= KMAX_CHAIN, scan steps <= SCAN_CAP + 32, Brent steps <= 201,
+// Neville points <= 10).
 struct ChainState {
   double last;    // value of the last requested secular evaluation
   double creq;    // requested phase velocity
@@ -810,7 +810,9 @@ SWDK_HD bool proposal_cell(const ChainState& s, const ChainParams& P, const Chai
 // modes are at least 0.05 km/s apart at 1-2 s on the default and 0.2 km/s
 // on the production grid, above the coarse interval of 0.02 km/s.  Love
 // chains keep the plain scan: their first two modes come as close as
-// 0.001 km/s at short periods.
+// 0.001 km/s at short periods; so do higher Rayleigh modes, whose first
+// period scans up from the mode below (modes 1 and 2 as close as
+// 0.0002 km/s).
 constexpr int FIRST_STRIDE = 4;
 
 SWDK_HD bool first_cell(const ChainState& s, const ChainParams& P, const ChainIO& io, int& m) {
