@@ -119,3 +119,33 @@ def test_love_roots_of_the_reference_test_model(T):
     assert ierr == 0
     cp = _first_root(lambda x: _love_D(x, T, thk, b, r), b.min() * (1 + 1e-9), 0.99999 * b[-1], 0.004)
     assert abs(cp - c[0]) < 1e-11, (T, cp, c[0])
+
+
+def _nth_root(D, lo, hi, step, n):
+    x0, f0 = lo, D(lo)
+    x, found = lo + step, 0
+    while x < hi:
+        f = D(x)
+        if np.sign(f) != np.sign(f0):
+            found += 1
+            if found == n:
+                return brentq(D, x0, x, xtol=1e-13, rtol=1e-15)
+        x0, f0 = x, f
+        x += step
+    raise AssertionError("no root")
+
+
+@pytest.mark.parametrize("T", [2.0, 5.0, 10.0])
+@pytest.mark.parametrize("iwave", [1, 2])
+def test_first_overtone_of_the_reference_test_model(T, iwave):
+    """surfdisp96's second mode (its scan continued from the mode below) is
+    the propagator's second root."""
+    (thk, a, b, r), (thk32, a32, b32, r32) = _model()
+    c, ierr, _ = O.surfdisp96(thk32, a32, b32, r32, 0, iwave, 2, 0, np.array([T]), refine=1, rtol=1e-12, sngl=0)
+    assert ierr == 0
+    if iwave == 2:
+        D, lo = (lambda x: _rayleigh_D(x, T, thk, a, b, r)), 0.8 * b.min()
+    else:
+        D, lo = (lambda x: _love_D(x, T, thk, b, r)), b.min() * (1 + 1e-9)
+    cp = _nth_root(D, lo, 0.99999 * b[-1], 0.002, 2)
+    assert abs(cp - c[0]) < 1e-11, (T, iwave, cp, c[0])
