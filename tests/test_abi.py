@@ -50,6 +50,11 @@ def test_config_defaults_and_arg_checks():
     assert lib.swdk_config_default(None) == -1
     assert lib.swdk_create(None, None) == -1
     assert lib.swdk_kmax(None) == 0
+    # proposals: a null context is refused before any CUDA call
+    lib.swdk_set_proposal_shift.argtypes = [C.c_void_p, C.c_double]
+    assert lib.swdk_set_proposal_shift(None, 0.1) == -1
+    lib.swdk_set_proposal.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double]
+    assert lib.swdk_set_proposal(None, None, None, 1.0, 1.0) == -1
 
 
 def test_fmst_entry_points_check_arguments_without_gpu():
